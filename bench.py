@@ -1,0 +1,357 @@
+#!/usr/bin/env python3
+"""Benchmark: BN254 G1 multi-scalar multiplication on B200.
+
+Default workload (one step = one MSM): BN254 G1, n = 2^24 points P_i = k_i*G
+(k_i uniform in [1, r)), scalars uniform in Fr given in Montgomery form, all
+synthetic from the library's seeded generator.  `value` is device time per
+MSM with inputs resident in HBM (CUDA events on the launching stream);
+`e2e` is the same MSM through the drop-in C ABI call
+(zkmetal_bn254_msm_fr) from pinned host buffers, host<->device copies
+included.  With --gpus N (torchrun, one process per GPU) a step is one MSM of
+N*2^24 points split into point-range shards: each rank computes its shard's
+partial sum and the N partial points are all-gathered (NCCL) and added.
+
+--impl reference times the reference's own CPU Pippenger
+(bn254_pippenger_msm, compiled from the reference sources into oracle/_ref)
+on the host cores for the same metric.
+"""
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+# the reference C oracle parallelises with OpenMP; give it every host thread
+os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count() or 1))
+
+CANON_PRODUCTS_PER_POINT = {"bn254": 23936, "bls12_381": 52800}
+METRIC = "BN254 G1 MSM ms @2^24 (uniform Fr, Montgomery scalars)"
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+# --------------------------------------------------------------- clocks
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.idx = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.idx), "--query-gpu=" + self.FIELDS, "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for name, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(name)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# --------------------------------------------------------------- CPU (reference) timing
+def reference_cpu_msm_ms(n_sample, points_b, scalars_mont_b, repeats=1):
+    """Time the reference C Pippenger on host cores; returns (ms per run, threads, kind)."""
+    from oracle import lib as olib
+    from oracle import build as obuild
+    obuild.build_cmsm()
+    if not os.path.exists(olib.REF_LIB):
+        try:
+            obuild.build_all()
+        except Exception:
+            pass
+    kind = "reference" if os.path.exists(olib.REF_LIB) else "port"
+    orc = olib.RefOracle() if kind == "reference" else olib.COracle()
+    sc_int = orc.fr_from_mont("bn254", scalars_mont_b, n_sample)  # conversion timed separately (not here)
+    times = []
+    for _ in range(repeats):
+        t0 = time.perf_counter()
+        orc.msm_jacobian("bn254", points_b, sc_int, n_sample) if kind == "reference" else \
+            orc.msm("bn254", points_b, sc_int, n_sample)
+        times.append((time.perf_counter() - t0) * 1e3)
+    from oracle.pyref import _ref_window_bits
+    wb = _ref_window_bits(n_sample)
+    windows = (256 + wb - 1) // wb  # the reference runs one OpenMP task per window
+    threads = min(int(os.environ.get("OMP_NUM_THREADS", "1")), windows)
+    return statistics.median(times), threads, kind
+
+
+def host_inputs(n, seed, index0=0):
+    """Synthetic inputs in host memory (bases from the device generator when a
+    GPU is present; they are plain input data for the CPU run)."""
+    import torch
+    from zkmetal_b200 import MetalMSM
+    from zkmetal_b200 import lib as zl
+    e = MetalMSM()
+    p = torch.empty(n * 64, dtype=torch.uint8, device="cuda")
+    s = torch.empty(n * 32, dtype=torch.uint8, device="cuda")
+    torch.cuda.synchronize()
+    assert zl.lib().zkmsm_gen_bases(e.handle, 0, seed, index0, n, p.data_ptr()) == 0
+    assert zl.lib().zkmsm_gen_scalars(e.handle, 0, seed, index0, n, 0, 1, s.data_ptr()) == 0
+    torch.cuda.synchronize()
+    pb, sb = p.cpu().numpy().tobytes(), s.cpu().numpy().tobytes()
+    e.close()
+    return pb, sb
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    n_full = 1 << args.log2n
+    n_sample = min(n_full, 1 << args.cpu_log2n)
+    pb, sb = host_inputs(n_sample, args.seed)
+    scale = n_full / n_sample
+    ms_all = []
+    for i in range(args.warmup + args.steps):
+        ms, threads, kind = reference_cpu_msm_ms(n_sample, pb, sb)
+        if i >= args.warmup:
+            ms_all.append(ms * scale)
+    v = statistics.mean(ms_all)
+    sample = "one %d-point BN254 MSM per step (reference C Pippenger, %d OpenMP threads), time x%g to 2^%d" % (
+        n_sample, threads, scale, args.log2n)
+    line = {"metric": METRIC, "value": round(v, 3), "unit": "ms", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(v, 3), "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u64", "data": "synthetic", "impl": "reference",
+            "config": {"workload": "bn254_g1_msm", "n": n_full, "scalars": "uniform Fr (Montgomery form)",
+                       "bases": "k_i*G, k_i uniform in [1,r)"},
+            "cpu_baseline": {"value": round(v, 3), "unit": "ms", "cores": threads, "kind": kind, "sample": sample},
+            "e2e": {"value": round(v, 3), "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# --------------------------------------------------------------- GPU arm
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+    from zkmetal_b200 import MetalMSM
+    from zkmetal_b200 import lib as zl
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    L = zl.lib()
+    n = 1 << args.log2n
+    eng = MetalMSM()
+    if args.window:
+        assert L.zkmsm_engine_set_tuning(eng.handle, args.window, args.chunk, -1) == 0
+    # inputs: this rank's shard [rank*n, (rank+1)*n) of the N*n-point MSM
+    pts = torch.empty(n * 64, dtype=torch.uint8, device="cuda")
+    sc = torch.empty(n * 32, dtype=torch.uint8, device="cuda")
+    res = torch.empty(3 * 32, dtype=torch.uint8, device="cuda")
+    torch.cuda.synchronize()
+    t0 = time.time()
+    assert L.zkmsm_gen_bases(eng.handle, 0, args.seed, rank * n, n, pts.data_ptr()) == 0
+    assert L.zkmsm_gen_scalars(eng.handle, 0, args.seed, rank * n, n, 0 if args.dist == "uniform" else 1, 1,
+                               sc.data_ptr()) == 0
+    log("rank %d: inputs generated in %.1f s" % (rank, time.time() - t0))
+    stream = torch.cuda.current_stream()
+    gathered = torch.empty(world * 96, dtype=torch.uint8, device="cuda")
+    final = torch.empty(96, dtype=torch.uint8, device="cuda")
+
+    def step():
+        st = L.zkmsm_msm_device_async(eng.handle, 0, pts.data_ptr(), None, sc.data_ptr(), 1, n, res.data_ptr(),
+                                      stream.cuda_stream)
+        assert st == 0, zl.last_error()
+        if world > 1:
+            dist.all_gather_into_tensor(gathered, res)
+            assert L.zkmsm_sum_results_device(0, gathered.data_ptr(), world, final.data_ptr(),
+                                              stream.cuda_stream) == 0
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    L.zkmsm_engine_profile(eng.handle, 1)
+    ms5 = (ctypes.c_double * 5)()
+    calls = ctypes.c_uint64()
+    L.zkmsm_engine_phase_times(eng.handle, ms5, ctypes.byref(calls), 1)
+    launches0 = L.zkmsm_engine_launch_count(eng.handle)
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(0.3)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(args.steps):
+        step()
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1) / args.steps
+    clk = clocks.stop()
+    launches = L.zkmsm_engine_launch_count(eng.handle) - launches0 + (args.steps if world > 1 else 0)
+    L.zkmsm_engine_phase_times(eng.handle, ms5, ctypes.byref(calls), 1)
+    L.zkmsm_engine_profile(eng.handle, 0)
+    phases = [ms5[i] / max(1, calls.value) for i in range(5)]
+    if world > 1:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+
+    # ---- end to end through the drop-in C ABI from pinned host buffers
+    e2e_ms = None
+    if not args.no_e2e:
+        hp = torch.empty(n * 64, dtype=torch.uint8, pin_memory=True)
+        hs = torch.empty(n * 32, dtype=torch.uint8, pin_memory=True)
+        hp.copy_(pts.cpu())
+        hs.copy_(sc.cpu())
+        rx, ry, rz = (ctypes.create_string_buffer(32) for _ in range(3))
+        out_all = torch.empty(world * 96, dtype=torch.uint8)
+        times = []
+        for i in range(args.warmup + args.e2e_steps):
+            if world > 1:
+                dist.barrier()
+            t0 = time.perf_counter()
+            st = L.zkmetal_bn254_msm_fr(eng.handle, hp.data_ptr(), hs.data_ptr(), n, rx, ry, rz)
+            assert st == 0, zl.last_error()
+            if world > 1:
+                mine = torch.frombuffer(bytearray(rx.raw + ry.raw + rz.raw), dtype=torch.uint8).cuda()
+                g = torch.empty(world * 96, dtype=torch.uint8, device="cuda")
+                dist.all_gather_into_tensor(g, mine)
+                out_all.copy_(g.cpu())
+                fin = ctypes.create_string_buffer(96)
+                assert L.zkmsm_sum_results(0, out_all.numpy().ctypes.data, world, fin) == 0
+            dt = (time.perf_counter() - t0) * 1e3
+            if i >= args.warmup:
+                times.append(dt)
+        e2e_ms = statistics.mean(times)
+        if world > 1:
+            t = torch.tensor([e2e_ms], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            e2e_ms = float(t.item())
+
+    # ---- roofline of the dominant kernel (level-1 bucket accumulation)
+    prod_s = ctypes.c_double()
+    bn_mul = ctypes.c_double()
+    assert L.zkmsm_measure_peaks(ctypes.byref(prod_s), ctypes.byref(bn_mul), None) == 0
+    peak = prod_s.value / 1e9
+    acc_ms = phases[1]
+    achieved = CANON_PRODUCTS_PER_POINT["bn254"] * n / (acc_ms * 1e-3) / 1e9 if acc_ms > 0 else None
+    msm_achieved = CANON_PRODUCTS_PER_POINT["bn254"] * n / (ms * 1e-3) / 1e9
+    traffic = None
+    prof_json = os.path.join(ROOT, "profiles", "acc_l1_bn254_traffic.json")
+    if os.path.exists(prof_json):
+        try:
+            with open(prof_json) as f:
+                pj = json.load(f)
+            traffic = pj.get("dram_bytes_per_launch_at_2p24")
+        except Exception:
+            traffic = None
+
+    if rank != 0:
+        if world > 1:
+            dist.barrier()
+            dist.destroy_process_group()
+        return 0
+    line = {
+        "metric": METRIC, "value": round(ms, 3), "unit": "ms", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": False, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+        "config": {"workload": "bn254_g1_msm", "n": n * world, "n_per_gpu": n, "dist": args.dist,
+                   "scalars": "Fr in Montgomery form", "bases": "k_i*G, k_i uniform in [1,r)",
+                   "parallelism": "point-range shards + all-gather of %d partial points" % world,
+                   "l2": "inputs larger than L2 (%.2f GB per step per GPU)" % (n * 96 / 1e9)},
+        "points_per_s": round(n * world / (ms * 1e-3)),
+        "phase_ms": {"prep_sort": round(phases[0], 3), "acc_level1": round(phases[1], 3),
+                     "acc_levels2+": round(phases[2], 3), "bucket_reduce": round(phases[3], 3),
+                     "window_combine": round(phases[4], 3)},
+        "roofline": {"bound": "int-mul", "achieved": round(achieved, 1) if achieved else None,
+                     "peak": round(peak, 1), "unit": "G word-products/s",
+                     "frac": round(achieved / peak, 4) if achieved else None, "traffic": traffic,
+                     "kernel": "k_acc_l1 (bucket accumulation)",
+                     "peak_source": "measured live: mad.lo.cc+madc.hi pairs, all SMs (zkmsm_measure_peaks)",
+                     "msm_achieved": round(msm_achieved, 1), "msm_frac": round(msm_achieved / peak, 4),
+                     "bn254_fe_mul_per_s": round(bn_mul.value / 1e9, 2)},
+        "e2e": {"value": round(e2e_ms, 3) if e2e_ms else None, "unit": "ms", "h2d_bytes_per_step": n * 96,
+                "d2h_bytes_per_step": 96},
+        "gpu_launches": int(launches),
+        "clocks": clk,
+    }
+    if not args.no_cpu_baseline and world == 1:
+        n_sample = min(n, 1 << args.cpu_log2n)
+        pb = pts[:n_sample * 64].cpu().numpy().tobytes()
+        sb = sc[:n_sample * 32].cpu().numpy().tobytes()
+        cms, threads, kind = reference_cpu_msm_ms(n_sample, pb, sb)
+        scale = n / n_sample
+        line["cpu_baseline"] = {
+            "value": round(cms * scale, 1), "unit": "ms", "cores": threads, "kind": kind,
+            "sample": "one %d-point BN254 MSM (first shard of the same inputs), reference C Pippenger, "
+                      "%d OpenMP threads, time x%g to 2^%d" % (n_sample, threads, scale, args.log2n)}
+    print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--log2n", type=int, default=24)
+    ap.add_argument("--dist", choices=["uniform", "witness"], default="uniform")
+    ap.add_argument("--seed", type=int, default=0x5EED0001)
+    ap.add_argument("--window", type=int, default=0)
+    ap.add_argument("--chunk", type=int, default=0)
+    ap.add_argument("--cpu-log2n", type=int, default=22)
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

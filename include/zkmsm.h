@@ -1,0 +1,219 @@
+/* zkmsm.h -- C ABI of the B200 (sm_100a) multi-scalar multiplication library.
+ *
+ * Drop-in for the MSM part of zkMetal's C FFI.  Every entry point below that
+ * exists in the reference keeps its name, argument order, byte layouts,
+ * status codes and error behaviour; the citation next to each names the
+ * reference declaration it replaces (paths inside the zkMetal tree).  Entry
+ * points the reference does not have are marked NEW.
+ *
+ * Layouts (as in Sources/zkMetal-ffi/include/zkmetal.h:1-12):
+ *   BN254       field element 32 B = 8 x u32 little endian, Montgomery form
+ *               (R = 2^256); affine point 64 B (x, y); identity = all zero.
+ *   BLS12-381   field element 48 B = 12 x u32 LE Montgomery (R = 2^384);
+ *               affine point 96 B.
+ *   scalars     32 B = 8 x u32 LE.  "_msm" entry points take integers
+ *               (standard form, need not be reduced mod r, zkmetal.h:6);
+ *               NEW "_fr" entry points take Montgomery-form Fr (s * 2^256 mod r).
+ *   results     Jacobian (X, Y, Z), Montgomery form, each one field element.
+ *               The library always returns Z = 1 (R mod p) for a finite point
+ *               and (1, 1, 0) for the identity, so X and Y are the affine
+ *               coordinates.
+ *
+ * Threading (zkMetal_ffi.swift:22-35, MSM/MSMEngine.swift:33-58): an engine
+ * is not thread-safe; use one engine per thread.  The "_auto" functions share
+ * one lazily created engine guarded by a mutex.
+ */
+#ifndef ZKMSM_H
+#define ZKMSM_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes: zkmetal.h:28-34 ------------------------------------ */
+typedef int32_t ZkMetalStatus;
+#define ZKMETAL_SUCCESS 0
+#define ZKMETAL_ERR_NO_GPU -1
+#define ZKMETAL_ERR_INVALID_INPUT -2
+#define ZKMETAL_ERR_GPU_ERROR -3
+#define ZKMETAL_ERR_ALLOC_FAILED -4
+/* NEW: a served request was refused by admission control or cancelled */
+#define ZKMETAL_ERR_BUSY -5
+
+/* ---- engine lifecycle: zkmetal.h:40, 55-60 ------------------------------ */
+typedef void* ZkMetalMSMEngine;
+
+/* replaces zkmetal_msm_engine_create (zkmetal.h:57) */
+ZkMetalStatus zkmetal_msm_engine_create(ZkMetalMSMEngine* out);
+/* replaces zkmetal_msm_engine_destroy (zkmetal.h:60) */
+void zkmetal_msm_engine_destroy(ZkMetalMSMEngine engine);
+
+/* ---- BN254 G1 MSM: zkmetal.h:117-147 ------------------------------------ */
+
+/* replaces zkmetal_bn254_msm (zkmetal.h:129-137); n_points == 0 -> INVALID_INPUT */
+ZkMetalStatus zkmetal_bn254_msm(ZkMetalMSMEngine engine, const uint8_t* points, const uint8_t* scalars,
+                                uint32_t n_points, uint8_t* result_x, uint8_t* result_y, uint8_t* result_z);
+
+/* replaces zkmetal_bn254_msm_auto (zkmetal.h:140-147) */
+ZkMetalStatus zkmetal_bn254_msm_auto(const uint8_t* points, const uint8_t* scalars, uint32_t n_points,
+                                     uint8_t* result_x, uint8_t* result_y, uint8_t* result_z);
+
+/* replaces zkmetal_bn254_msm_u8 / _u16 / _u32 (zkmetal.h:446-471): 1, 2 or 4
+ * byte little-endian scalars, zero-extended */
+ZkMetalStatus zkmetal_bn254_msm_u8(ZkMetalMSMEngine engine, const uint8_t* points, const uint8_t* scalars,
+                                   uint32_t n_points, uint8_t* result_x, uint8_t* result_y, uint8_t* result_z);
+ZkMetalStatus zkmetal_bn254_msm_u16(ZkMetalMSMEngine engine, const uint8_t* points, const uint8_t* scalars,
+                                    uint32_t n_points, uint8_t* result_x, uint8_t* result_y, uint8_t* result_z);
+ZkMetalStatus zkmetal_bn254_msm_u32(ZkMetalMSMEngine engine, const uint8_t* points, const uint8_t* scalars,
+                                    uint32_t n_points, uint8_t* result_x, uint8_t* result_y, uint8_t* result_z);
+/* replaces zkmetal_bn254_msm_u8_auto / _u16_auto / _u32_auto (zkmetal.h:473-484) */
+ZkMetalStatus zkmetal_bn254_msm_u8_auto(const uint8_t* points, const uint8_t* scalars, uint32_t n_points,
+                                        uint8_t* result_x, uint8_t* result_y, uint8_t* result_z);
+ZkMetalStatus zkmetal_bn254_msm_u16_auto(const uint8_t* points, const uint8_t* scalars, uint32_t n_points,
+                                         uint8_t* result_x, uint8_t* result_y, uint8_t* result_z);
+ZkMetalStatus zkmetal_bn254_msm_u32_auto(const uint8_t* points, const uint8_t* scalars, uint32_t n_points,
+                                         uint8_t* result_x, uint8_t* result_y, uint8_t* result_z);
+
+/* replaces zkmetal_bn254_msm_batch (zkmetal.h:499-506): MSM i uses the next
+ * counts[i] points and scalars; results[i] = 96 B (X, Y, Z); counts[i] == 0
+ * writes 96 zero bytes (zkMetal_ffi.swift:1260-1264); n_msms == 0 ->
+ * INVALID_INPUT.  Unlike the reference, all MSMs run in one batched launch
+ * sequence instead of one after another. */
+ZkMetalStatus zkmetal_bn254_msm_batch(ZkMetalMSMEngine engine, const uint8_t* all_points,
+                                      const uint8_t* all_scalars, const uint32_t* counts, uint32_t n_msms,
+                                      uint8_t* results);
+/* replaces zkmetal_bn254_msm_batch_auto (zkmetal.h:509-515) */
+ZkMetalStatus zkmetal_bn254_msm_batch_auto(const uint8_t* all_points, const uint8_t* all_scalars,
+                                           const uint32_t* counts, uint32_t n_msms, uint8_t* results);
+
+/* NEW: BN254 with Montgomery-form Fr scalars (the conversion the reference
+ * does on the CPU in bn254_fr_batch_to_limbs, NeonFieldOps/bn254_msm.c:1537,
+ * runs inside the GPU scalar-preparation kernel) */
+ZkMetalStatus zkmetal_bn254_msm_fr(ZkMetalMSMEngine engine, const uint8_t* points, const uint8_t* scalars_mont,
+                                   uint32_t n_points, uint8_t* result_x, uint8_t* result_y, uint8_t* result_z);
+
+/* ---- BLS12-381 G1 MSM ---------------------------------------------------
+ * NEW symbols: the reference FFI has none.  They replace the Swift API
+ * BLS12381MSM.msm / msmFr (MSM/BLS12381MSMEngine.swift:260, 517) and the C
+ * g1 Pippenger (NeonFieldOps/bls12_381_ops.c:1141).  Points 96 B, results
+ * 48 B per coordinate. */
+ZkMetalStatus zkmetal_bls12_381_g1_msm(ZkMetalMSMEngine engine, const uint8_t* points, const uint8_t* scalars,
+                                       uint32_t n_points, uint8_t* result_x, uint8_t* result_y,
+                                       uint8_t* result_z);
+ZkMetalStatus zkmetal_bls12_381_g1_msm_fr(ZkMetalMSMEngine engine, const uint8_t* points,
+                                          const uint8_t* scalars_mont, uint32_t n_points, uint8_t* result_x,
+                                          uint8_t* result_y, uint8_t* result_z);
+ZkMetalStatus zkmetal_bls12_381_g1_msm_batch(ZkMetalMSMEngine engine, const uint8_t* all_points,
+                                             const uint8_t* all_scalars, const uint32_t* counts,
+                                             uint32_t n_msms, uint8_t* results);
+
+/* ---- misc: zkmetal.h:520-530 --------------------------------------------- */
+/* replaces zkmetal_set_shader_dir (zkmetal.h:524): accepted and ignored (no shaders) */
+void zkmetal_set_shader_dir(const char* path);
+/* replaces zkmetal_gpu_available (zkmetal.h:527): 1 if a CUDA device of compute capability 10.x is visible */
+int32_t zkmetal_gpu_available(void);
+/* replaces zkmetal_version (zkmetal.h:530) */
+const char* zkmetal_version(void);
+
+/* ==== NEW: device-resident data, batching, serving ======================= */
+
+/* Curve selector for the entry points below. */
+#define ZKMSM_BN254 0
+#define ZKMSM_BLS12_381 1
+/* Scalar encoding */
+#define ZKMSM_SCALAR_INT 0
+#define ZKMSM_SCALAR_MONT 1
+
+/* Text of the last error raised on the calling thread ("" if none). */
+const char* zkmsm_last_error(void);
+
+/* MSM on device buffers (CUDA pointers): d_points n affine points, d_scalars
+ * n x 32 B; result (3 field elements, Jacobian layout above) copied to HOST
+ * memory `result`.  `stream` is a cudaStream_t (0 = the engine's stream). */
+ZkMetalStatus zkmsm_msm_device(ZkMetalMSMEngine engine, int curve, const void* d_points, const void* d_scalars,
+                               int scalar_fmt, uint32_t n_points, uint8_t* result, void* stream);
+
+/* Enqueue-only variant for pipelined callers: all buffers are device
+ * pointers; d_phi (the endomorphism image of the bases, n affine points) may
+ * be NULL, in which case it is computed into engine scratch on the stream.
+ * The result (3 field elements) is written to DEVICE memory d_result.  The
+ * call returns without waiting; order other work on the same stream. */
+ZkMetalStatus zkmsm_msm_device_async(ZkMetalMSMEngine engine, int curve, const void* d_points, const void* d_phi,
+                                     const void* d_scalars, int scalar_fmt, uint32_t n_points, void* d_result,
+                                     void* stream);
+
+/* A base table kept resident in HBM (a commitment key), with its
+ * endomorphism image precomputed once.  points: HOST pointer unless
+ * points_on_device != 0. */
+typedef void* ZkMsmTable;
+ZkMetalStatus zkmsm_table_create(ZkMetalMSMEngine engine, int curve, const void* points, uint64_t n_points,
+                                 int points_on_device, ZkMsmTable* out);
+void zkmsm_table_destroy(ZkMsmTable table);
+/* Device pointer of the table's affine points (for reading back / tests). */
+const void* zkmsm_table_device_points(ZkMsmTable table);
+
+/* Batched commitments over a resident table: MSM i = sum_j s_ij * T[j] for
+ * j < counts[i] (a prefix of the table).  scalars: concatenated 32 B scalars
+ * (HOST unless scalars_on_device), results: n_msms x 3 field elements (HOST).
+ * All MSMs run as one batch captured in a CUDA graph (replayed when the same
+ * shape repeats); window width and chunking come from the autotuner. */
+ZkMetalStatus zkmsm_batch_commit(ZkMetalMSMEngine engine, ZkMsmTable table, const void* scalars,
+                                 int scalars_on_device, int scalar_fmt, const uint32_t* counts, uint32_t n_msms,
+                                 uint8_t* results);
+
+/* Tuning overrides (0 = automatic): window bits, chunk length, GLV on/off. */
+ZkMetalStatus zkmsm_engine_set_tuning(ZkMetalMSMEngine engine, int window_bits, int chunk, int glv);
+
+/* Synthetic inputs on the device (seeded, counter based):
+ * bases[i] = k_i * G with k_i uniform in [1, r); scalars uniform in Fr
+ * (dist 0) or witness-like (dist 1: 40% 0, 20% 1, 25% < 2^32, 15% uniform). */
+ZkMetalStatus zkmsm_gen_bases(ZkMetalMSMEngine engine, int curve, uint64_t seed, uint64_t index0, uint64_t n,
+                              void* d_out);
+ZkMetalStatus zkmsm_gen_scalars(ZkMetalMSMEngine engine, int curve, uint64_t seed, uint64_t index0,
+                                uint64_t n, int dist, int scalar_fmt, void* d_out);
+
+/* Per-phase device time: enable/disable recording CUDA events around the
+ * pipeline phases of every MSM this engine enqueues; read (after waiting for
+ * the recorded work) the cumulative milliseconds of phases
+ * 0 scalar preparation + bucket sort, 1 first accumulation level, 2 later
+ * accumulation levels, 3 bucket reduction, 4 window combine, and the number
+ * of MSM batches recorded. */
+ZkMetalStatus zkmsm_engine_profile(ZkMetalMSMEngine engine, int enable);
+ZkMetalStatus zkmsm_engine_phase_times(ZkMetalMSMEngine engine, double* ms5, uint64_t* calls, int reset);
+
+/* The execution plan (window widths, bucket layout, chunking of the segmented
+ * sums, reduction tree) the engine would use for a batch, as JSON text in
+ * buf.  Pure host computation: no device is touched. */
+ZkMetalStatus zkmsm_plan_describe(int curve, const uint32_t* counts, uint32_t n_msms, int scalar_fmt,
+                                  int window_bits, int chunk, int glv, int scalar_bits, char* buf, uint64_t buflen);
+
+/* Kernels launched so far by this engine (cumulative). */
+uint64_t zkmsm_engine_launch_count(ZkMetalMSMEngine engine);
+
+/* Roofline denominators measured on device 0: 32x32->64-bit word products per
+ * second (one low + one high multiply-add) with every SM occupied, and the
+ * Montgomery multiplications per second of this library's BN254 and
+ * BLS12-381 field code (either output pointer may be NULL). */
+ZkMetalStatus zkmsm_measure_peaks(double* products_per_s, double* bn254_mul_per_s, double* bls381_mul_per_s);
+
+/* Sum `count` results (each 3 field elements in the result layout above) into
+ * one; used to combine the partial MSMs of point-range shards. */
+ZkMetalStatus zkmsm_sum_results(int curve, const uint8_t* results, uint32_t count, uint8_t* out);
+/* Same on device buffers, enqueued on `stream` (cudaStream_t) without waiting. */
+ZkMetalStatus zkmsm_sum_results_device(int curve, const void* d_results, uint32_t count, void* d_out, void* stream);
+
+/* Device memory helpers for callers without a CUDA runtime of their own. */
+void* zkmsm_device_alloc(uint64_t bytes);
+void zkmsm_device_free(void* p);
+ZkMetalStatus zkmsm_memcpy_h2d(void* d_dst, const void* src, uint64_t bytes);
+ZkMetalStatus zkmsm_memcpy_d2h(void* dst, const void* d_src, uint64_t bytes);
+ZkMetalStatus zkmsm_device_sync(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* ZKMSM_H */

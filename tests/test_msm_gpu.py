@@ -1,0 +1,299 @@
+"""Parity of the CUDA MSM with the oracle, through the C ABI (GPU required).
+
+Shapes follow the reference tests (Tests/zkMetalTests/MSMTests.swift:7-108:
+5*G, n = 1..64 against a naive sum, scalar 0 / 1, determinism across runs
+and engines, on-curve; DASTests.swift:8-150: the BLS12-381 469*G answers),
+plus what the reference never checks on its GPU path: large n against the
+compiled reference C Pippenger, skewed (witness-like) scalars, duplicate and
+cancelling bases, identity bases, unreduced and maximal scalars, every
+tuning knob giving the same result, and the batch entry points.
+Bar: bit-exact affine results."""
+import ctypes
+import json
+import os
+import random
+
+import numpy as np
+import pytest
+import torch
+
+from oracle import pyref as R
+from tests.gpu_helpers import (CURVE_ID, check, gen_inputs, jac_to_affine_bytes, msm_device, np_bytes, oracle_msm,
+                               to_host)
+from zkmetal_b200 import BLS12381MSM, CommitmentTable, MetalMSM, MSMError, multiMSM
+from zkmetal_b200 import lib as zl
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "msm_golden.json")
+ENGINES = {"bn254": MetalMSM, "bls12_381": BLS12381MSM}
+
+
+@pytest.fixture(scope="module")
+def eng():
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    return {"bn254": MetalMSM(), "bls12_381": BLS12381MSM()}
+
+
+def aff(C, res):
+    return jac_to_affine_bytes(C, res.x + res.y + res.z)
+
+
+def test_gpu_available(eng):
+    assert zl.lib().zkmetal_gpu_available() == 1
+
+
+@pytest.mark.parametrize("curve", ["bn254", "bls12_381"])
+def test_5G(eng, curve):
+    C = R.CURVES[curve]
+    G = (C.gx, C.gy)
+    r = eng[curve].msm(C.enc_affine(G), R.pack_scalars_int([5]))
+    assert aff(C, r) == C.enc_affine(R.scalar_mul(C, G, 5))
+
+
+with open(GOLDEN) as _f:
+    _G = json.load(_f)
+
+
+@pytest.mark.parametrize("case", _G["cases"], ids=lambda c: "%s-%d-%d-%s" % (c["curve"], c["seed"], c["n"], c["dist"]))
+def test_golden_cases(eng, case):
+    C = R.CURVES[case["curve"]]
+    pts = R.make_bases(C, case["seed"], case["n"])
+    sc = R.make_scalars(C, case["seed"], case["n"], case["dist"])
+    want = bytes.fromhex(case["result_affine"])
+    e = eng[case["curve"]]
+    assert aff(C, e.msm(R.pack_points(C, pts), R.pack_scalars_int(sc))) == want
+    assert aff(C, e.msmFr(R.pack_points(C, pts), R.pack_scalars_mont(C, sc))) == want
+
+
+@pytest.mark.parametrize("kat", _G["kat"], ids=lambda k: "%s-%s" % (k["curve"], k["name"]))
+def test_golden_kats(eng, kat):
+    C = R.CURVES[kat["curve"]]
+    pb = b"".join(bytes.fromhex(p) for p in kat["points"])
+    r = eng[kat["curve"]].msm(pb, R.pack_scalars_int(kat["scalars"]))
+    assert aff(C, r) == bytes.fromhex(kat["result_affine"])
+
+
+@pytest.mark.parametrize("curve", ["bn254", "bls12_381"])
+def test_prefixes_vs_naive(eng, curve):
+    """MSMTests.swift:56-62 shape: n in {1, 2, 4, ..., 64} against naive sums."""
+    C = R.CURVES[curve]
+    pts = R.make_bases(C, 31, 64)
+    sc = [random.Random(31).getrandbits(256) for _ in range(64)]
+    for n in (1, 2, 4, 8, 16, 32, 64):
+        want = C.enc_affine(R.naive_msm(C, pts[:n], sc[:n]))
+        assert aff(C, eng[curve].msm(R.pack_points(C, pts[:n]), R.pack_scalars_int(sc[:n]))) == want, n
+
+
+@pytest.mark.parametrize("curve", ["bn254", "bls12_381"])
+def test_edge_cases(eng, curve):
+    C = R.CURVES[curve]
+    G = (C.gx, C.gy)
+    P = R.scalar_mul(C, G, 987654321)
+    Q = R.aff_neg(C, P)
+    cases = [
+        ([P, P, P], [3, 3, 3]),                         # duplicate bases in one bucket (doubling path)
+        ([P, Q], [9, 9]),                               # cancel to the identity
+        ([P, Q, P], [9, 9, 2]),
+        ([None, P, None], [5, 7, 11]),                  # identity bases (0, 0)
+        ([P, G], [0, 0]),                               # all-zero scalars
+        ([P, G], [1, 1]),
+        ([P, G, P], [C.r - 1, C.r, C.r + 5]),           # unreduced integer scalars
+        ([P, G], [(1 << 256) - 1, (1 << 255)]),
+        ([G] * 40, [1] * 40),                           # one hot bucket
+    ]
+    for pts, sc in cases:
+        want = C.enc_affine(R.naive_msm(C, pts, sc))
+        got = aff(C, eng[curve].msm(R.pack_points(C, pts), R.pack_scalars_int(sc)))
+        assert got == want, (pts, sc)
+
+
+def test_invalid_inputs(eng):
+    e = eng["bn254"]
+    with pytest.raises(MSMError) as ei:
+        e.msm(b"", b"")
+    assert ei.value.case == "invalidInput"
+    with pytest.raises(MSMError):
+        e.msm(bytes(64 * 2), bytes(32))
+    buf = ctypes.create_string_buffer(96)
+    assert zl.lib().zkmetal_bn254_msm(e.handle, buf, buf, 0, buf, buf, buf) == zl.ERR_INVALID_INPUT
+    assert zl.lib().zkmetal_bn254_msm_batch(e.handle, buf, buf, buf, 0, buf) == zl.ERR_INVALID_INPUT
+
+
+@pytest.mark.parametrize("curve", ["bn254", "bls12_381"])
+def test_generator_matches_restatement(eng, curve):
+    C = R.CURVES[curve]
+    n = 12
+    for dist in ("uniform", "witness"):
+        for fmt in (zl.SCALAR_INT, zl.SCALAR_MONT):
+            p, s = gen_inputs(eng[curve], curve, 5, n, dist, fmt)
+            assert to_host(p) == R.pack_points(C, R.make_bases(C, 5, n))
+            sc = R.make_scalars(C, 5, n, dist)
+            want = R.pack_scalars_mont(C, sc) if fmt == zl.SCALAR_MONT else R.pack_scalars_int(sc)
+            assert to_host(s) == want
+
+
+@pytest.mark.parametrize("curve,n,dist", [("bn254", 4096, "uniform"), ("bn254", 4096, "witness"),
+                                          ("bn254", 1 << 16, "uniform"), ("bn254", 1 << 16, "witness"),
+                                          ("bls12_381", 4096, "uniform"), ("bls12_381", 1 << 16, "witness"),
+                                          ("bls12_381", 1 << 16, "uniform")])
+def test_vs_reference_c(eng, oracles, curve, n, dist):
+    ref, cm = oracles
+    orc = ref if ref is not None else cm
+    C = R.CURVES[curve]
+    p, s = gen_inputs(eng[curve], curve, 100 + n, n, dist, zl.SCALAR_MONT)
+    got = jac_to_affine_bytes(C, msm_device(eng[curve], curve, p, s, zl.SCALAR_MONT, n))
+    want = oracle_msm(orc, curve, to_host(p), to_host(s), n, zl.SCALAR_MONT)
+    assert got == want
+
+
+@pytest.mark.parametrize("curve", ["bn254", "bls12_381"])
+def test_tuning_invariance(eng, oracles, curve):
+    """Window width, chunk length and GLV on/off change the schedule, never the result."""
+    ref, cm = oracles
+    orc = ref if ref is not None else cm
+    C = R.CURVES[curve]
+    n = 3000
+    p, s = gen_inputs(eng[curve], curve, 77, n, "witness", zl.SCALAR_INT)
+    e = eng[curve]
+    L = zl.lib()
+    results = set()
+    try:
+        for c, k, glv in [(0, 0, -1), (6, 8, 1), (11, 33, 1), (16, 128, 1), (21, 16, 1), (9, 8, 0), (13, 64, 0)]:
+            check(L.zkmsm_engine_set_tuning(e.handle, c, k, glv))
+            results.add(msm_device(e, curve, p, s, zl.SCALAR_INT, n))
+    finally:
+        check(L.zkmsm_engine_set_tuning(e.handle, 0, 0, -1))
+    assert len(results) == 1
+    assert jac_to_affine_bytes(C, results.pop()) == oracle_msm(orc, curve, to_host(p), to_host(s), n, zl.SCALAR_INT)
+
+
+@pytest.mark.parametrize("curve", ["bn254", "bls12_381"])
+def test_determinism_across_runs_and_engines(eng, curve):
+    C = R.CURVES[curve]
+    n = 32768
+    p, s = gen_inputs(eng[curve], curve, 9, n, "uniform", zl.SCALAR_MONT)
+    r1 = msm_device(eng[curve], curve, p, s, zl.SCALAR_MONT, n)
+    r2 = msm_device(eng[curve], curve, p, s, zl.SCALAR_MONT, n)
+    other = ENGINES[curve]()
+    r3 = msm_device(other, curve, p, s, zl.SCALAR_MONT, n)
+    other.close()
+    assert r1 == r2 == r3
+    assert C.on_curve(C.dec_affine(jac_to_affine_bytes(C, r1)))
+
+
+def test_small_scalar_variants(eng):
+    C = R.BN254
+    e = eng["bn254"]
+    L = zl.lib()
+    n = 200
+    pts = R.make_bases(C, 41, n)
+    pb = np_bytes(R.pack_points(C, pts))
+    rng = random.Random(41)
+    for width, fn in ((1, L.zkmetal_bn254_msm_u8), (2, L.zkmetal_bn254_msm_u16), (4, L.zkmetal_bn254_msm_u32)):
+        sc = [rng.getrandbits(8 * width) for _ in range(n)]
+        sb = np_bytes(b"".join(v.to_bytes(width, "little") for v in sc))
+        rx, ry, rz = (ctypes.create_string_buffer(32) for _ in range(3))
+        check(fn(e.handle, pb.ctypes.data, sb.ctypes.data, n, rx, ry, rz))
+        assert jac_to_affine_bytes(C, rx.raw + ry.raw + rz.raw) == C.enc_affine(R.naive_msm(C, pts, sc))
+
+
+@pytest.mark.parametrize("curve", ["bn254", "bls12_381"])
+def test_batch_entry_point_matches_plain(eng, curve):
+    """zkmetal_*_msm_batch: concatenated inputs, count 0 -> 96/144 zero bytes
+    (zkMetal_ffi.swift:1260-1264); each result equals its own plain call."""
+    C = R.CURVES[curve]
+    e = eng[curve]
+    counts = [5, 0, 300, 1, 64]
+    total = sum(counts)
+    pts = R.make_bases(C, 51, total)
+    sc = R.make_scalars(C, 51, total, "witness")
+    pb, sb = np_bytes(R.pack_points(C, pts)), np_bytes(R.pack_scalars_int(sc))
+    cnt = np.array(counts, dtype=np.uint32)
+    out = ctypes.create_string_buffer(len(counts) * 3 * C.fp_bytes)
+    fn = zl.lib().zkmetal_bn254_msm_batch if curve == "bn254" else zl.lib().zkmetal_bls12_381_g1_msm_batch
+    check(fn(e.handle, pb.ctypes.data, sb.ctypes.data, cnt.ctypes.data, len(counts), out))
+    f3 = 3 * C.fp_bytes
+    off = 0
+    for i, c in enumerate(counts):
+        got = out.raw[i * f3:(i + 1) * f3]
+        if c == 0:
+            assert got == bytes(f3)
+        else:
+            plain = e.msm(R.pack_points(C, pts[off:off + c]), R.pack_scalars_int(sc[off:off + c]))
+            assert got == plain.x + plain.y + plain.z
+            assert jac_to_affine_bytes(C, got) == C.enc_affine(R.naive_msm(C, pts[off:off + c], sc[off:off + c]))
+        off += c
+
+
+@pytest.mark.parametrize("curve", ["bn254", "bls12_381"])
+def test_resident_table_batch_commit(eng, curve):
+    """Many uneven MSMs over prefixes of one resident table, bit-exact against
+    separate plain calls (the batched-commitments pattern)."""
+    C = R.CURVES[curve]
+    e = eng[curve]
+    T = 1 << 14
+    p, _ = gen_inputs(e, curve, 61, T, "uniform", zl.SCALAR_MONT)
+    rng = random.Random(61)
+    counts = [int(2 ** rng.uniform(4, 14)) for _ in range(9)] + [T, 1, 0]
+    _, s = gen_inputs(e, curve, 62, sum(counts), "uniform", zl.SCALAR_MONT)
+    table = CommitmentTable(e, p.data_ptr(), on_device=True, n=T)
+    try:
+        res = table.batch_commit(s.data_ptr(), counts, fmt=zl.SCALAR_MONT, on_device=True)
+        res2 = table.batch_commit(s.data_ptr(), counts, fmt=zl.SCALAR_MONT, on_device=True)
+    finally:
+        table.close()
+    off = 0
+    for i, c in enumerate(counts):
+        got = res[i].x + res[i].y + res[i].z
+        assert got == res2[i].x + res2[i].y + res2[i].z
+        if c == 0:
+            assert got == bytes(3 * C.fp_bytes)
+        else:
+            sub = s[off * 32:(off + c) * 32]
+            assert got == msm_device(e, curve, p, sub, zl.SCALAR_MONT, c), i
+        off += c
+
+
+def test_multi_msm_matches_single(eng):
+    C = R.BN254
+    e = eng["bn254"]
+    n = 100
+    pts = R.make_bases(C, 71, n)
+    sets = [R.make_scalars(C, 71 + k, n, "uniform") for k in range(3)]
+    res = multiMSM(e, R.pack_points(C, pts), [R.pack_scalars_int(s) for s in sets])
+    for r, s in zip(res, sets):
+        single = e.msm(R.pack_points(C, pts), R.pack_scalars_int(s))
+        assert (r.x, r.y, r.z) == (single.x, single.y, single.z)
+
+
+@pytest.mark.slow
+@pytest.mark.parametrize("curve,dist", [("bn254", "uniform"), ("bn254", "witness"), ("bls12_381", "uniform")])
+def test_2_20_vs_reference_c(eng, oracles, curve, dist):
+    ref, cm = oracles
+    orc = ref if ref is not None else cm
+    C = R.CURVES[curve]
+    n = 1 << 20
+    p, s = gen_inputs(eng[curve], curve, 2020, n, dist, zl.SCALAR_MONT)
+    got = jac_to_affine_bytes(C, msm_device(eng[curve], curve, p, s, zl.SCALAR_MONT, n))
+    assert got == oracle_msm(orc, curve, to_host(p), to_host(s), n, zl.SCALAR_MONT)
+
+
+@pytest.mark.slow
+@pytest.mark.parametrize("dist", ["uniform", "witness"])
+def test_2_24_split_linearity(eng, oracles, dist):
+    """Full-size property check: MSM over 2^24 points equals the sum of the
+    MSMs over its two halves (different window widths are chosen for n and
+    n/2, so the two sides follow different schedules)."""
+    _, cm = oracles
+    C = R.BN254
+    n = 1 << 24
+    e = eng["bn254"]
+    p, s = gen_inputs(e, "bn254", 2424, n, dist, zl.SCALAR_MONT)
+    full = jac_to_affine_bytes(C, msm_device(e, "bn254", p, s, zl.SCALAR_MONT, n))
+    h = n // 2
+    a = jac_to_affine_bytes(C, msm_device(e, "bn254", p[:h * 64], s[:h * 32], zl.SCALAR_MONT, h))
+    b = jac_to_affine_bytes(C, msm_device(e, "bn254", p[h * 64:], s[h * 32:], zl.SCALAR_MONT, h))
+    assert full == cm.affine_add("bn254", a, b)
+    assert C.on_curve(C.dec_affine(full))

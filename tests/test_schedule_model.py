@@ -1,0 +1,230 @@
+"""CPU model of the device schedule, driven by the library's real host plan.
+
+The plan (window widths, bucket layout, segmented-sum chunking, reduction
+tree) comes from the C++ planner through zkmsm_plan_describe.  The kernels'
+index logic -- histogram, exclusive scan, counting-sort scatter (in a
+shuffled order, as atomics allow), chunked segmented sums with their partial
+slots, the multi-level partial passes, the weighted reduction tree and the
+Horner combine -- is replayed here with integers mod r standing in for group
+elements (P_i -> p_i, phi(P) -> lambda*p).  Every index is checked against the
+sizes the engine allocates from the same plan, every bucket must be written
+at most once, and the result must equal sum s_i p_i mod r.  No GPU needed.
+"""
+import ctypes
+import json
+import random
+
+import pytest
+
+from oracle import pyref as R
+from zkmetal_b200 import lib as zl
+
+
+def plan(curve, counts, fmt=0, window=0, chunk=0, glv=-1, bits=0):
+    L = zl.lib()
+    arr = (ctypes.c_uint32 * len(counts))(*counts)
+    buf = ctypes.create_string_buffer(1 << 22)
+    st = L.zkmsm_plan_describe(curve, arr, len(counts), fmt, window, chunk, glv, bits, buf, len(buf))
+    assert st == 0, zl.last_error()
+    return json.loads(buf.value.decode())
+
+
+def halves(C, s, glv):
+    """Device prepare_scalar: integer mod r, then GLV split with signs."""
+    s %= C.r
+    if not glv:
+        return [(s, 0)]
+    k1, k2 = R.glv_split(C, s)
+    return [(abs(k1), int(k1 < 0)), (abs(k2), int(k2 < 0))]
+
+
+def digits(k, c, nwin):
+    half = 1 << (c - 1)
+    carry = 0
+    for w in range(nwin):
+        v = ((k >> (c * w)) & ((1 << c) - 1)) + carry
+        if v > half:
+            yield w, (1 << c) - v, 1
+            carry = 1
+        else:
+            yield w, v, 0
+            carry = 0
+
+
+def excl_scan(a):
+    out, run = [], 0
+    for v in a:
+        out.append(run)
+        run += v
+    return out, run
+
+
+def run_model(C, pl, bases, scalars, seed=0):
+    r = C.r
+    lam = C.lam
+    rng = random.Random(seed)
+    descs = pl["descs"]
+    G = pl["nbuckets"]
+    # 1-3: histogram, scan, scatter
+    entries = []
+    for d in descs:
+        soff, n, boff, c, nwin, glv, bucket_off, fmt, win_off = d
+        B = 1 << (c - 1)
+        for i in range(n):
+            for j, (k, hneg) in enumerate(halves(C, scalars[soff + i], glv)):
+                for w, a, dneg in digits(k, c, nwin):
+                    if a:
+                        gb = bucket_off + w * B + (a - 1)
+                        assert gb < G
+                        entries.append((gb, (boff + i) | (j << 30) | ((hneg ^ dneg) << 31)))
+    assert len(entries) <= pl["entry_bound"]
+    rng.shuffle(entries)  # atomics give any order within a bucket
+    entries.sort(key=lambda e: e[0])
+    keys = [e[0] for e in entries]
+    vals = [e[1] for e in entries]
+
+    def point(v):
+        idx = v & 0x3FFFFFFF
+        x = bases[idx] * (lam if (v >> 30) & 1 else 1) % r
+        return (-x) % r if v >> 31 else x
+
+    buckets = [0] * G
+    written = [False] * G
+
+    def write_bucket(k, x):
+        assert not written[k], "bucket %d written twice" % k
+        written[k] = True
+        buckets[k] = x % r
+
+    cur_keys, cur_vals = keys, None
+    M = len(keys)
+    for lvl, (K, T, Mbound) in enumerate(pl["acc"]):
+        assert M <= Mbound
+        cnt = []
+        for t in range(T):
+            start = t * K
+            if start >= M:
+                cnt.append(0)
+                continue
+            end = min(start + K, M)
+            k0, k1 = cur_keys[start], cur_keys[end - 1]
+            cb = int(start > 0 and cur_keys[start - 1] == k0)
+            ca = int(end < M and cur_keys[end] == k1)
+            cnt.append((cb | ca) if k0 == k1 else cb + ca)
+        pos, total = excl_scan(cnt)
+        if lvl + 1 < len(pl["acc"]):
+            assert total <= pl["acc"][lvl + 1][2], "partial slots exceed the next level's bound"
+        else:
+            assert total == 0, "last level must complete every bucket"
+        pkeys = [None] * total
+        pvals = [None] * total
+        for t in range(T):
+            start = t * K
+            if start >= M:
+                continue
+            end = min(start + K, M)
+            cur = cur_keys[start]
+            cont_before = start > 0 and cur_keys[start - 1] == cur
+            first_run = True
+            slot = pos[t]
+            acc = 0
+            for i in range(start, end):
+                k = cur_keys[i]
+                if k != cur:
+                    if first_run and cont_before:
+                        pkeys[slot], pvals[slot] = cur, acc
+                        slot += 1
+                    else:
+                        write_bucket(cur, acc)
+                    acc, cur, first_run = 0, k, False
+                acc += point(vals[i]) if lvl == 0 else cur_vals[i]
+            cont_after = end < M and cur_keys[end] == cur
+            if (first_run and cont_before) or cont_after:
+                assert slot < total
+                pkeys[slot], pvals[slot] = cur, acc
+                slot += 1
+            else:
+                write_bucket(cur, acc)
+            assert slot == pos[t] + cnt[t], "slot count disagrees with the chunk count pass"
+        cur_keys, cur_vals, M = pkeys, pvals, total
+    assert M == 0
+    # bucket reduction tree
+    L, log2L = pl["red_L"], pl["red_log2L"]
+    inS, inW = buckets, None
+    for lvl, tasks in enumerate(pl["red"]):
+        nout = sum(t[3] for t in tasks)
+        outS, outW = [None] * nout, [None] * nout
+        for (in_off, n_in, out_off, n_out) in tasks:
+            for local in range(n_out):
+                g = out_off + local
+                c0 = in_off + local * L
+                cnt = min(L, n_in - local * L)
+                run = x = 0
+                for s in range(cnt - 1, 0, -1):
+                    run += inS[c0 + s]
+                    x += run
+                run += inS[c0]
+                outS[g] = run % r
+                x = x * (1 << (lvl * log2L))
+                if inW is not None:
+                    x += sum(inW[c0 + s] for s in range(cnt))
+                outW[g] = x % r
+        inS, inW = outS, outW
+    results = []
+    for d in descs:
+        soff, n, boff, c, nwin, glv, bucket_off, fmt, win_off = d
+        acc = 0
+        for w in range(nwin - 1, -1, -1):
+            acc = acc * (1 << c) + inS[win_off + w] + inW[win_off + w]
+        results.append(acc % r if n else 0)
+    return results
+
+
+CASES = [
+    # curve, counts, dist, window, chunk, glv, bits
+    ("bn254", [700], "uniform", 0, 0, -1, 0),
+    ("bn254", [700], "witness", 0, 8, -1, 0),
+    ("bn254", [2000], "witness", 6, 8, -1, 0),        # hot buckets -> several partial levels
+    ("bn254", [300, 0, 17, 1, 900], "uniform", 0, 0, -1, 0),
+    ("bn254", [500], "uniform", 11, 33, 0, 0),          # no GLV: 255-bit scalars
+    ("bn254", [400], "uniform", 0, 0, -1, 16),          # small-scalar plan
+    ("bls12_381", [600], "uniform", 16, 16, -1, 0),     # 9 windows for 128-bit halves
+    ("bls12_381", [250, 0, 40], "witness", 0, 0, -1, 0),
+    ("bls12_381", [300], "uniform", 13, 64, 0, 0),
+]
+
+
+@pytest.mark.parametrize("curve,counts,dist,window,chunk,glv,bits", CASES)
+def test_schedule_model(curve, counts, dist, window, chunk, glv, bits):
+    C = R.CURVES[curve]
+    cid = zl.BN254 if curve == "bn254" else zl.BLS12_381
+    pl = plan(cid, counts, 0, window, chunk, glv, bits)
+    rng = random.Random(sum(counts) + window)
+    total = sum(counts)
+    bases = [rng.randrange(1, C.r) for _ in range(total)]
+    if bits:
+        scalars = [rng.getrandbits(bits) for _ in range(total)]
+    elif dist == "uniform":
+        scalars = [rng.randrange(1 << 256) for _ in range(total)]
+    else:
+        scalars = []
+        for _ in range(total):
+            u = rng.randrange(100)
+            scalars.append(0 if u < 40 else 1 if u < 60 else rng.getrandbits(32) if u < 85 else rng.randrange(C.r))
+    got = run_model(C, pl, bases, scalars, seed=len(counts))
+    off = 0
+    for m, n in enumerate(counts):
+        # the plan puts every MSM on a prefix of one base table (base_off = 0)
+        want = sum(s * b for s, b in zip(scalars[off:off + n], bases[:n])) % C.r
+        assert got[m] == want, m
+        off += n
+
+
+def test_plan_sizes_2_24():
+    """The full-size plan: entry and bucket counts fit 32-bit indices and the
+    window choice is the cost model's."""
+    pl = plan(zl.BN254, [1 << 24])
+    d = pl["descs"][0]
+    assert d[4] * (1 << (d[3] - 1)) == pl["nbuckets"]
+    assert pl["entry_bound"] == 2 * (1 << 24) * d[4] < (1 << 32)
+    assert 14 <= d[3] <= 21

@@ -1,0 +1,11 @@
+"""zkmetal_b200: B200-native (sm_100a CUDA) multi-scalar multiplication.
+
+A drop-in for zkMetal's G1 MSM path (BN254 and BLS12-381): the C ABI in
+``include/zkmsm.h`` keeps the reference FFI's entry points; ``msm`` mirrors
+the Swift engine API.  All arithmetic runs in ``libzkmsm.so``.
+"""
+from . import lib  # noqa: F401  (raises ImportError when the CUDA library is missing)
+from .msm import (BLS12381MSM, CommitmentTable, MetalMSM, MSMError,  # noqa: F401
+                  PointProjective, multiMSM)
+
+__all__ = ["MetalMSM", "BLS12381MSM", "MSMError", "PointProjective", "multiMSM", "CommitmentTable", "lib"]

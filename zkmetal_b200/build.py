@@ -1,0 +1,79 @@
+#!/usr/bin/env python3
+"""Build the CUDA library ``zkmetal_b200/libzkmsm.so`` for sm_100a.
+
+nvcc cross-compiles without a GPU.  The library is built in-tree so it
+travels with the working tree; it is git-ignored.
+
+    python zkmetal_b200/build.py [--force] [--verbose-ptxas]
+"""
+import hashlib
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+CSRC = os.path.join(HERE, "csrc")
+ROOT = os.path.dirname(HERE)
+LIB = os.path.join(HERE, "libzkmsm.so")
+NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
+
+SOURCES = ["capi.cu", "inst_bn254.cu", "inst_bls381.cu", "peak.cu"]
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+
+
+def _inputs():
+    files = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cu", ".cuh", ".h"))]
+    files.append(os.path.join(ROOT, "include", "zkmsm.h"))
+    files.append(os.path.abspath(__file__))
+    return files
+
+
+STAMP = LIB + ".stamp"
+
+
+def _digest():
+    h = hashlib.sha256()
+    for f in sorted(_inputs()):
+        h.update(os.path.basename(f).encode())
+        with open(f, "rb") as fh:
+            h.update(fh.read())
+    return h.hexdigest()
+
+
+def up_to_date():
+    """True when the library exists and was built from the current sources
+    (content hash, so copies that reset file times do not force a rebuild)."""
+    if not os.path.exists(LIB) or not os.path.exists(STAMP):
+        return False
+    with open(STAMP) as f:
+        return f.read().strip() == _digest()
+
+
+def build(force=False, ptxas_verbose=False, extra=None):
+    if not force and up_to_date():
+        return LIB
+    objdir = os.path.join(HERE, "_build")
+    os.makedirs(objdir, exist_ok=True)
+    base = [NVCC, "-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC,-O2", "--expt-relaxed-constexpr",
+            "-I", os.path.join(ROOT, "include")] + ARCH
+    if ptxas_verbose:
+        base += ["-Xptxas", "-v"]
+    base += extra or []
+    procs, objs = [], []
+    for s in SOURCES:
+        obj = os.path.join(objdir, s.replace(".cu", ".o"))
+        objs.append(obj)
+        procs.append((s, subprocess.Popen(base + ["-c", os.path.join(CSRC, s), "-o", obj])))
+    bad = [s for s, p in procs if p.wait() != 0]
+    if bad:
+        raise RuntimeError("nvcc failed for " + ", ".join(bad))
+    tmp = LIB + ".tmp"
+    subprocess.check_call([NVCC, "-shared"] + ARCH + objs + ["-o", tmp, "-lcudart"])
+    os.replace(tmp, LIB)
+    with open(STAMP, "w") as f:
+        f.write(_digest())
+    return LIB
+
+
+if __name__ == "__main__":
+    print(build(force="--force" in sys.argv, ptxas_verbose="--verbose-ptxas" in sys.argv))

@@ -1,0 +1,517 @@
+// C ABI (include/zkmsm.h): the zkMetal-ffi compatible MSM entry points and
+// the new device-resident / batched entry points.  Argument checks, status
+// codes and the count == 0 convention follow the reference FFI
+// (Sources/zkMetal-ffi/zkMetal_ffi.swift:302-379, 1048-1300).
+#include <cuda_runtime.h>
+
+#include <cstdio>
+#include <memory>
+#include <mutex>
+#include <new>
+
+#include "../../include/zkmsm.h"
+#include "engine.cuh"
+
+namespace zkmsm {
+
+static thread_local std::string g_last_error;
+void set_error(const std::string& s) { g_last_error = s; }
+
+static int fp_bytes(int curve) { return curve == ZKMSM_BLS12_381 ? 48 : 32; }
+
+// Map exceptions to reference status codes.
+template <class F>
+static ZkMetalStatus guarded(F&& f) {
+    try {
+        g_last_error.clear();
+        return f();
+    } catch (const CudaError& e) {
+        set_error(std::string(e.where) + ": " + cudaGetErrorString(e.code));
+        cudaGetLastError();  // clear a sticky non-fatal error state where possible
+        if (e.code == cudaErrorMemoryAllocation) return ZKMETAL_ERR_ALLOC_FAILED;
+        if (e.code == cudaErrorNoDevice || e.code == cudaErrorInsufficientDriver) return ZKMETAL_ERR_NO_GPU;
+        return ZKMETAL_ERR_GPU_ERROR;
+    } catch (const std::bad_alloc&) {
+        set_error("host allocation failed");
+        return ZKMETAL_ERR_ALLOC_FAILED;
+    } catch (const std::exception& e) {
+        set_error(e.what());
+        return ZKMETAL_ERR_GPU_ERROR;
+    }
+}
+
+static bool have_gpu() {
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
+        cudaGetLastError();
+        return false;
+    }
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, 0) != cudaSuccess) return false;
+    return prop.major == 10;
+}
+
+// Copy host data to a device buffer of the engine's workspace.
+static void h2d(Engine& e, DevBuf& buf, const void* src, size_t bytes) {
+    buf.ensure(bytes + 16);
+    if (bytes) ZK_CUDA(cudaMemcpyAsync(buf.p, src, bytes, cudaMemcpyHostToDevice, e.stream));
+}
+
+template <class C>
+static ZkMetalStatus msm_host(Engine& e, const uint8_t* points, const uint8_t* scalars, uint32_t n, int fmt,
+                              uint32_t scalar_bits, uint8_t* rx, uint8_t* ry, uint8_t* rz) {
+    using P = typename C::Fp;
+    const int fb = P::N * 4;
+    if (n == 0 || !points || !scalars || !rx || !ry || !rz) return ZKMETAL_ERR_INVALID_INPUT;
+    h2d(e, e.w_points, points, (size_t)n * 2 * fb);
+    h2d(e, e.w_scalars, scalars, (size_t)n * 32);
+    Plan& pl = e.get_plan<C>({n}, {0}, fmt, scalar_bits);
+    bool glv = pl.descs[0].glv;
+    if (glv) {
+        e.w_phi.ensure((size_t)n * 2 * fb + 16);
+        e.make_phi<C>(e.w_points.as<uint32_t>(), n, e.w_phi.as<uint32_t>());
+    }
+    uint8_t out[3 * 48];
+    e.run_device<C>(pl, e.w_points.as<uint32_t>(), glv ? e.w_phi.as<uint32_t>() : e.w_points.as<uint32_t>(),
+                    e.w_scalars.as<uint32_t>(), out);
+    memcpy(rx, out, fb);
+    memcpy(ry, out + fb, fb);
+    memcpy(rz, out + 2 * fb, fb);
+    return ZKMETAL_SUCCESS;
+}
+
+// small-scalar variants: zero-extend to 32 B (zkMetal_ffi.swift:1150-1190)
+static ZkMetalStatus msm_small(Engine& e, const uint8_t* points, const uint8_t* scalars, uint32_t n, int width,
+                               uint8_t* rx, uint8_t* ry, uint8_t* rz) {
+    if (n == 0 || !points || !scalars) return ZKMETAL_ERR_INVALID_INPUT;
+    std::vector<uint32_t> wide((size_t)n * 8, 0);
+    for (uint32_t i = 0; i < n; i++) {
+        uint32_t v = 0;
+        for (int b = 0; b < width; b++) v |= (uint32_t)scalars[(size_t)i * width + b] << (8 * b);
+        wide[(size_t)i * 8] = v;
+    }
+    return msm_host<Bn254>(e, points, reinterpret_cast<const uint8_t*>(wide.data()), n, ZKMSM_SCALAR_INT,
+                           8 * width, rx, ry, rz);
+}
+
+template <class C>
+static ZkMetalStatus msm_batch_host(Engine& e, const uint8_t* all_points, const uint8_t* all_scalars,
+                                    const uint32_t* counts, uint32_t n_msms, int fmt, uint8_t* results) {
+    using P = typename C::Fp;
+    const int fb = P::N * 4;
+    if (n_msms == 0 || !counts || !results) return ZKMETAL_ERR_INVALID_INPUT;
+    std::vector<uint32_t> cnt(counts, counts + n_msms), boff(n_msms);
+    uint64_t total = 0;
+    for (uint32_t m = 0; m < n_msms; m++) {
+        boff[m] = (uint32_t)total;
+        total += cnt[m];
+    }
+    if (total >= (1ull << 30)) return ZKMETAL_ERR_INVALID_INPUT;
+    if (total && (!all_points || !all_scalars)) return ZKMETAL_ERR_INVALID_INPUT;
+    h2d(e, e.w_points, all_points, (size_t)total * 2 * fb);
+    h2d(e, e.w_scalars, all_scalars, (size_t)total * 32);
+    Plan& pl = e.get_plan<C>(cnt, boff, fmt);
+    e.w_phi.ensure((size_t)total * 2 * fb + 16);
+    e.make_phi<C>(e.w_points.as<uint32_t>(), total, e.w_phi.as<uint32_t>());
+    std::vector<uint8_t> out((size_t)n_msms * 3 * fb);
+    e.run_device<C>(pl, e.w_points.as<uint32_t>(), e.w_phi.as<uint32_t>(), e.w_scalars.as<uint32_t>(), out.data());
+    for (uint32_t m = 0; m < n_msms; m++) {
+        uint8_t* dst = results + (size_t)m * 3 * fb;
+        if (cnt[m] == 0) memset(dst, 0, 3 * fb);
+        else memcpy(dst, out.data() + (size_t)m * 3 * fb, 3 * fb);
+    }
+    return ZKMETAL_SUCCESS;
+}
+
+// Resident base table (commitment key).
+struct Table {
+    Engine* engine;
+    int curve;
+    uint64_t n;
+    DevBuf points, phi;
+};
+
+// lazily created shared engine for the _auto entry points (zkMetal_ffi.swift:22-35)
+static std::mutex g_auto_mu;
+static Engine* g_auto = nullptr;
+static Engine& auto_engine() {
+    if (!g_auto) g_auto = new Engine();
+    return *g_auto;
+}
+
+}  // namespace zkmsm
+
+using namespace zkmsm;
+
+extern "C" {
+
+ZkMetalStatus zkmetal_msm_engine_create(ZkMetalMSMEngine* out) {
+    if (!out) return ZKMETAL_ERR_INVALID_INPUT;
+    if (!have_gpu()) {
+        set_error("no compute-capability 10.x CUDA device");
+        return ZKMETAL_ERR_NO_GPU;
+    }
+    return guarded([&] {
+        *out = new Engine();
+        return ZKMETAL_SUCCESS;
+    });
+}
+
+void zkmetal_msm_engine_destroy(ZkMetalMSMEngine engine) { delete static_cast<Engine*>(engine); }
+
+#define ENG(x) (*static_cast<Engine*>(x))
+
+ZkMetalStatus zkmetal_bn254_msm(ZkMetalMSMEngine engine, const uint8_t* points, const uint8_t* scalars,
+                                uint32_t n, uint8_t* rx, uint8_t* ry, uint8_t* rz) {
+    if (!engine) return ZKMETAL_ERR_INVALID_INPUT;
+    return guarded([&] { return msm_host<Bn254>(ENG(engine), points, scalars, n, ZKMSM_SCALAR_INT, 0, rx, ry, rz); });
+}
+
+ZkMetalStatus zkmetal_bn254_msm_fr(ZkMetalMSMEngine engine, const uint8_t* points, const uint8_t* scalars,
+                                   uint32_t n, uint8_t* rx, uint8_t* ry, uint8_t* rz) {
+    if (!engine) return ZKMETAL_ERR_INVALID_INPUT;
+    return guarded([&] { return msm_host<Bn254>(ENG(engine), points, scalars, n, ZKMSM_SCALAR_MONT, 0, rx, ry, rz); });
+}
+
+ZkMetalStatus zkmetal_bn254_msm_auto(const uint8_t* points, const uint8_t* scalars, uint32_t n, uint8_t* rx,
+                                     uint8_t* ry, uint8_t* rz) {
+    if (!have_gpu()) return ZKMETAL_ERR_NO_GPU;
+    std::lock_guard<std::mutex> lk(g_auto_mu);
+    return guarded([&] { return msm_host<Bn254>(auto_engine(), points, scalars, n, ZKMSM_SCALAR_INT, 0, rx, ry, rz); });
+}
+
+#define SMALL_VARIANT(NAME, W)                                                                                \
+    ZkMetalStatus NAME(ZkMetalMSMEngine engine, const uint8_t* points, const uint8_t* scalars, uint32_t n,    \
+                       uint8_t* rx, uint8_t* ry, uint8_t* rz) {                                               \
+        if (!engine) return ZKMETAL_ERR_INVALID_INPUT;                                                        \
+        return guarded([&] { return msm_small(ENG(engine), points, scalars, n, W, rx, ry, rz); });          \
+    }                                                                                                         \
+    ZkMetalStatus NAME##_auto(const uint8_t* points, const uint8_t* scalars, uint32_t n, uint8_t* rx,         \
+                              uint8_t* ry, uint8_t* rz) {                                                     \
+        if (!have_gpu()) return ZKMETAL_ERR_NO_GPU;                                                           \
+        std::lock_guard<std::mutex> lk(g_auto_mu);                                                            \
+        return guarded([&] { return msm_small(auto_engine(), points, scalars, n, W, rx, ry, rz); });        \
+    }
+
+SMALL_VARIANT(zkmetal_bn254_msm_u8, 1)
+SMALL_VARIANT(zkmetal_bn254_msm_u16, 2)
+SMALL_VARIANT(zkmetal_bn254_msm_u32, 4)
+
+ZkMetalStatus zkmetal_bn254_msm_batch(ZkMetalMSMEngine engine, const uint8_t* all_points, const uint8_t* all_scalars,
+                                      const uint32_t* counts, uint32_t n_msms, uint8_t* results) {
+    if (!engine) return ZKMETAL_ERR_INVALID_INPUT;
+    return guarded([&] {
+        return msm_batch_host<Bn254>(ENG(engine), all_points, all_scalars, counts, n_msms, ZKMSM_SCALAR_INT, results);
+    });
+}
+
+ZkMetalStatus zkmetal_bn254_msm_batch_auto(const uint8_t* all_points, const uint8_t* all_scalars,
+                                           const uint32_t* counts, uint32_t n_msms, uint8_t* results) {
+    if (!have_gpu()) return ZKMETAL_ERR_NO_GPU;
+    std::lock_guard<std::mutex> lk(g_auto_mu);
+    return guarded([&] {
+        return msm_batch_host<Bn254>(auto_engine(), all_points, all_scalars, counts, n_msms, ZKMSM_SCALAR_INT,
+                                     results);
+    });
+}
+
+ZkMetalStatus zkmetal_bls12_381_g1_msm(ZkMetalMSMEngine engine, const uint8_t* points, const uint8_t* scalars,
+                                       uint32_t n, uint8_t* rx, uint8_t* ry, uint8_t* rz) {
+    if (!engine) return ZKMETAL_ERR_INVALID_INPUT;
+    return guarded([&] { return msm_host<Bls381>(ENG(engine), points, scalars, n, ZKMSM_SCALAR_INT, 0, rx, ry, rz); });
+}
+
+ZkMetalStatus zkmetal_bls12_381_g1_msm_fr(ZkMetalMSMEngine engine, const uint8_t* points, const uint8_t* scalars,
+                                          uint32_t n, uint8_t* rx, uint8_t* ry, uint8_t* rz) {
+    if (!engine) return ZKMETAL_ERR_INVALID_INPUT;
+    return guarded(
+        [&] { return msm_host<Bls381>(ENG(engine), points, scalars, n, ZKMSM_SCALAR_MONT, 0, rx, ry, rz); });
+}
+
+ZkMetalStatus zkmetal_bls12_381_g1_msm_batch(ZkMetalMSMEngine engine, const uint8_t* all_points,
+                                             const uint8_t* all_scalars, const uint32_t* counts, uint32_t n_msms,
+                                             uint8_t* results) {
+    if (!engine) return ZKMETAL_ERR_INVALID_INPUT;
+    return guarded([&] {
+        return msm_batch_host<Bls381>(ENG(engine), all_points, all_scalars, counts, n_msms, ZKMSM_SCALAR_INT,
+                                      results);
+    });
+}
+
+void zkmetal_set_shader_dir(const char*) {}
+
+int32_t zkmetal_gpu_available(void) { return have_gpu() ? 1 : 0; }
+
+const char* zkmetal_version(void) { return "zkmsm-b200 0.1.0"; }
+
+const char* zkmsm_last_error(void) { return g_last_error.c_str(); }
+
+ZkMetalStatus zkmsm_msm_device(ZkMetalMSMEngine engine, int curve, const void* d_points, const void* d_scalars,
+                               int fmt, uint32_t n, uint8_t* result, void* stream) {
+    if (!engine || !d_points || !d_scalars || !result || n == 0) return ZKMETAL_ERR_INVALID_INPUT;
+    if (curve != ZKMSM_BN254 && curve != ZKMSM_BLS12_381) return ZKMETAL_ERR_INVALID_INPUT;
+    if (fmt != ZKMSM_SCALAR_INT && fmt != ZKMSM_SCALAR_MONT) return ZKMETAL_ERR_INVALID_INPUT;
+    return guarded([&] {
+        Engine& e = ENG(engine);
+        cudaStream_t saved = e.stream;
+        if (stream) e.stream = static_cast<cudaStream_t>(stream);
+        struct Restore {
+            Engine& e;
+            cudaStream_t s;
+            ~Restore() { e.stream = s; }
+        } restore{e, saved};
+        const uint32_t* pts = static_cast<const uint32_t*>(d_points);
+        const uint32_t* sc = static_cast<const uint32_t*>(d_scalars);
+        if (curve == ZKMSM_BN254) {
+            Plan& pl = e.get_plan<Bn254>({n}, {0}, fmt);
+            e.w_phi.ensure((size_t)n * 64 + 16);
+            e.make_phi<Bn254>(pts, n, e.w_phi.as<uint32_t>());
+            e.run_device<Bn254>(pl, pts, e.w_phi.as<uint32_t>(), sc, result);
+        } else {
+            Plan& pl = e.get_plan<Bls381>({n}, {0}, fmt);
+            e.w_phi.ensure((size_t)n * 96 + 16);
+            e.make_phi<Bls381>(pts, n, e.w_phi.as<uint32_t>());
+            e.run_device<Bls381>(pl, pts, e.w_phi.as<uint32_t>(), sc, result);
+        }
+        return ZKMETAL_SUCCESS;
+    });
+}
+
+ZkMetalStatus zkmsm_msm_device_async(ZkMetalMSMEngine engine, int curve, const void* d_points, const void* d_phi,
+                                     const void* d_scalars, int fmt, uint32_t n, void* d_result, void* stream) {
+    if (!engine || !d_points || !d_scalars || !d_result || n == 0 || n >= (1u << 30)) return ZKMETAL_ERR_INVALID_INPUT;
+    if (curve != ZKMSM_BN254 && curve != ZKMSM_BLS12_381) return ZKMETAL_ERR_INVALID_INPUT;
+    if (fmt != ZKMSM_SCALAR_INT && fmt != ZKMSM_SCALAR_MONT) return ZKMETAL_ERR_INVALID_INPUT;
+    return guarded([&] {
+        Engine& e = ENG(engine);
+        cudaStream_t saved = e.stream;
+        if (stream) e.stream = static_cast<cudaStream_t>(stream);
+        struct Restore {
+            Engine& e;
+            cudaStream_t s;
+            ~Restore() { e.stream = s; }
+        } restore{e, saved};
+        const uint32_t* pts = static_cast<const uint32_t*>(d_points);
+        const uint32_t* phi = static_cast<const uint32_t*>(d_phi);
+        const uint32_t* sc = static_cast<const uint32_t*>(d_scalars);
+        uint32_t* res = static_cast<uint32_t*>(d_result);
+        if (curve == ZKMSM_BN254) {
+            Plan& pl = e.get_plan<Bn254>({n}, {0}, fmt);
+            e.ensure_workspace<Bn254>(pl);
+            if (!phi) {
+                e.w_phi.ensure((size_t)n * 64 + 16);
+                e.make_phi<Bn254>(pts, n, e.w_phi.as<uint32_t>());
+                phi = e.w_phi.as<uint32_t>();
+            }
+            e.enqueue<Bn254>(pl, pts, phi, sc, res);
+        } else {
+            Plan& pl = e.get_plan<Bls381>({n}, {0}, fmt);
+            e.ensure_workspace<Bls381>(pl);
+            if (!phi) {
+                e.w_phi.ensure((size_t)n * 96 + 16);
+                e.make_phi<Bls381>(pts, n, e.w_phi.as<uint32_t>());
+                phi = e.w_phi.as<uint32_t>();
+            }
+            e.enqueue<Bls381>(pl, pts, phi, sc, res);
+        }
+        return ZKMETAL_SUCCESS;
+    });
+}
+
+ZkMetalStatus zkmsm_table_create(ZkMetalMSMEngine engine, int curve, const void* points, uint64_t n,
+                                 int on_device, ZkMsmTable* out) {
+    if (!engine || !points || !out || n == 0 || n >= (1ull << 30)) return ZKMETAL_ERR_INVALID_INPUT;
+    if (curve != ZKMSM_BN254 && curve != ZKMSM_BLS12_381) return ZKMETAL_ERR_INVALID_INPUT;
+    return guarded([&] {
+        Engine& e = ENG(engine);
+        std::unique_ptr<Table> t(new Table{&e, curve, n, {}, {}});
+        size_t bytes = (size_t)n * 2 * fp_bytes(curve);
+        t->points.ensure(bytes);
+        t->phi.ensure(bytes);
+        ZK_CUDA(cudaMemcpyAsync(t->points.p, points, bytes, on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
+                                e.stream));
+        if (curve == ZKMSM_BN254) e.make_phi<Bn254>(t->points.as<uint32_t>(), n, t->phi.as<uint32_t>());
+        else e.make_phi<Bls381>(t->points.as<uint32_t>(), n, t->phi.as<uint32_t>());
+        ZK_CUDA(cudaStreamSynchronize(e.stream));
+        *out = t.release();
+        return ZKMETAL_SUCCESS;
+    });
+}
+
+void zkmsm_table_destroy(ZkMsmTable table) { delete static_cast<Table*>(table); }
+
+const void* zkmsm_table_device_points(ZkMsmTable table) {
+    return table ? static_cast<Table*>(table)->points.p : nullptr;
+}
+
+ZkMetalStatus zkmsm_batch_commit(ZkMetalMSMEngine engine, ZkMsmTable table, const void* scalars, int on_device,
+                                 int fmt, const uint32_t* counts, uint32_t n_msms, uint8_t* results) {
+    if (!engine || !table || !scalars || !counts || !results || n_msms == 0) return ZKMETAL_ERR_INVALID_INPUT;
+    if (fmt != ZKMSM_SCALAR_INT && fmt != ZKMSM_SCALAR_MONT) return ZKMETAL_ERR_INVALID_INPUT;
+    Table& t = *static_cast<Table*>(table);
+    uint64_t total = 0;
+    for (uint32_t m = 0; m < n_msms; m++) {
+        if (counts[m] > t.n) return ZKMETAL_ERR_INVALID_INPUT;
+        total += counts[m];
+    }
+    return guarded([&] {
+        Engine& e = ENG(engine);
+        std::vector<uint32_t> cnt(counts, counts + n_msms), boff(n_msms, 0);
+        const uint32_t* sc = static_cast<const uint32_t*>(scalars);
+        if (!on_device) {
+            h2d(e, e.w_scalars, scalars, (size_t)total * 32);
+            sc = e.w_scalars.as<uint32_t>();
+        }
+        int fb = fp_bytes(t.curve);
+        std::vector<uint8_t> out((size_t)n_msms * 3 * fb);
+        if (t.curve == ZKMSM_BN254) {
+            Plan& pl = e.get_plan<Bn254>(cnt, boff, fmt);
+            e.run_device<Bn254>(pl, t.points.as<uint32_t>(), t.phi.as<uint32_t>(), sc, out.data());
+        } else {
+            Plan& pl = e.get_plan<Bls381>(cnt, boff, fmt);
+            e.run_device<Bls381>(pl, t.points.as<uint32_t>(), t.phi.as<uint32_t>(), sc, out.data());
+        }
+        for (uint32_t m = 0; m < n_msms; m++) {
+            uint8_t* dst = results + (size_t)m * 3 * fb;
+            if (counts[m] == 0) memset(dst, 0, 3 * fb);
+            else memcpy(dst, out.data() + (size_t)m * 3 * fb, 3 * fb);
+        }
+        return ZKMETAL_SUCCESS;
+    });
+}
+
+ZkMetalStatus zkmsm_engine_set_tuning(ZkMetalMSMEngine engine, int window_bits, int chunk, int glv) {
+    if (!engine || window_bits < 0 || window_bits > 24 || window_bits == 1 || chunk < 0 || chunk > 4096)
+        return ZKMETAL_ERR_INVALID_INPUT;
+    Engine& e = ENG(engine);
+    e.tuning.window_bits = window_bits;
+    e.tuning.chunk = chunk;
+    e.tuning.glv = glv < 0 ? -1 : (glv ? 1 : 0);
+    return ZKMETAL_SUCCESS;
+}
+
+ZkMetalStatus zkmsm_gen_bases(ZkMetalMSMEngine engine, int curve, uint64_t seed, uint64_t index0, uint64_t n,
+                              void* d_out) {
+    if (!engine || !d_out) return ZKMETAL_ERR_INVALID_INPUT;
+    return guarded([&] {
+        if (curve == ZKMSM_BN254) ENG(engine).gen_bases<Bn254>(seed, index0, n, static_cast<uint32_t*>(d_out));
+        else if (curve == ZKMSM_BLS12_381) ENG(engine).gen_bases<Bls381>(seed, index0, n, static_cast<uint32_t*>(d_out));
+        else return ZKMETAL_ERR_INVALID_INPUT;
+        return ZKMETAL_SUCCESS;
+    });
+}
+
+ZkMetalStatus zkmsm_gen_scalars(ZkMetalMSMEngine engine, int curve, uint64_t seed, uint64_t index0, uint64_t n,
+                                int dist, int fmt, void* d_out) {
+    if (!engine || !d_out || (dist != 0 && dist != 1) || (fmt != 0 && fmt != 1)) return ZKMETAL_ERR_INVALID_INPUT;
+    return guarded([&] {
+        if (curve == ZKMSM_BN254)
+            ENG(engine).gen_scalars<Bn254>(seed, index0, n, dist, fmt, static_cast<uint32_t*>(d_out));
+        else if (curve == ZKMSM_BLS12_381)
+            ENG(engine).gen_scalars<Bls381>(seed, index0, n, dist, fmt, static_cast<uint32_t*>(d_out));
+        else return ZKMETAL_ERR_INVALID_INPUT;
+        return ZKMETAL_SUCCESS;
+    });
+}
+
+ZkMetalStatus zkmsm_engine_profile(ZkMetalMSMEngine engine, int enable) {
+    if (!engine) return ZKMETAL_ERR_INVALID_INPUT;
+    ENG(engine).profile = enable != 0;
+    return ZKMETAL_SUCCESS;
+}
+
+ZkMetalStatus zkmsm_engine_phase_times(ZkMetalMSMEngine engine, double* ms5, uint64_t* calls, int reset) {
+    if (!engine || !ms5) return ZKMETAL_ERR_INVALID_INPUT;
+    return guarded([&] {
+        Engine& e = ENG(engine);
+        e.prof_collect();
+        for (int i = 0; i < Engine::NPHASE; i++) ms5[i] = e.phase_ms[i];
+        if (calls) *calls = e.phase_calls;
+        if (reset) {
+            for (int i = 0; i < Engine::NPHASE; i++) e.phase_ms[i] = 0;
+            e.phase_calls = 0;
+        }
+        return ZKMETAL_SUCCESS;
+    });
+}
+
+ZkMetalStatus zkmsm_plan_describe(int curve, const uint32_t* counts, uint32_t n_msms, int fmt, int window_bits,
+                                  int chunk, int glv, int scalar_bits, char* buf, uint64_t buflen) {
+    if (!counts || !buf || n_msms == 0) return ZKMETAL_ERR_INVALID_INPUT;
+    return guarded([&] {
+        Tuning t;
+        t.window_bits = window_bits;
+        t.chunk = chunk;
+        t.glv = glv;
+        std::vector<uint32_t> cnt(counts, counts + n_msms), boff(n_msms, 0);
+        Plan pl;
+        if (curve == ZKMSM_BN254) Engine::plan_shape<Bn254>(pl, t, cnt, boff, fmt, scalar_bits);
+        else Engine::plan_shape<Bls381>(pl, t, cnt, boff, fmt, scalar_bits);
+        std::string s = "{\"descs\":[";
+        for (size_t i = 0; i < pl.descs.size(); i++) {
+            auto& d = pl.descs[i];
+            s += (i ? "," : "") + std::string("[") + std::to_string(d.scalar_off) + "," + std::to_string(d.n) + "," +
+                 std::to_string(d.base_off) + "," + std::to_string(d.c) + "," + std::to_string(d.nwin) + "," +
+                 std::to_string(d.glv) + "," + std::to_string(d.bucket_off) + "," + std::to_string(d.fmt) + "," +
+                 std::to_string(d.win_off) + "]";
+        }
+        s += "],\"entry_bound\":" + std::to_string(pl.entry_bound) + ",\"nbuckets\":" + std::to_string(pl.nbuckets) +
+             ",\"acc\":[";
+        for (size_t l = 0; l < pl.acc_K.size(); l++)
+            s += (l ? "," : "") + std::string("[") + std::to_string(pl.acc_K[l]) + "," + std::to_string(pl.acc_T[l]) +
+                 "," + std::to_string(pl.acc_Mbound[l]) + "]";
+        s += "],\"red_L\":" + std::to_string(pl.red_L) + ",\"red_log2L\":" + std::to_string(pl.red_log2L) +
+             ",\"red\":[";
+        for (size_t l = 0; l < pl.red_tasks.size(); l++) {
+            s += (l ? "," : "") + std::string("[");
+            for (size_t k = 0; k < pl.red_tasks[l].size(); k++) {
+                auto& tk = pl.red_tasks[l][k];
+                s += (k ? "," : "") + std::string("[") + std::to_string(tk.in_off) + "," + std::to_string(tk.n_in) +
+                     "," + std::to_string(tk.out_off) + "," + std::to_string(tk.n_out) + "]";
+            }
+            s += "]";
+        }
+        s += "]}";
+        if (s.size() + 1 > buflen) return ZKMETAL_ERR_INVALID_INPUT;
+        memcpy(buf, s.c_str(), s.size() + 1);
+        return ZKMETAL_SUCCESS;
+    });
+}
+
+uint64_t zkmsm_engine_launch_count(ZkMetalMSMEngine engine) { return engine ? ENG(engine).launches : 0; }
+
+void* zkmsm_device_alloc(uint64_t bytes) {
+    void* p = nullptr;
+    if (cudaMalloc(&p, bytes) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    return p;
+}
+
+void zkmsm_device_free(void* p) {
+    if (p) cudaFree(p);
+}
+
+ZkMetalStatus zkmsm_memcpy_h2d(void* d_dst, const void* src, uint64_t bytes) {
+    return guarded([&] {
+        ZK_CUDA(cudaMemcpy(d_dst, src, bytes, cudaMemcpyHostToDevice));
+        return ZKMETAL_SUCCESS;
+    });
+}
+
+ZkMetalStatus zkmsm_memcpy_d2h(void* dst, const void* d_src, uint64_t bytes) {
+    return guarded([&] {
+        ZK_CUDA(cudaMemcpy(dst, d_src, bytes, cudaMemcpyDeviceToHost));
+        return ZKMETAL_SUCCESS;
+    });
+}
+
+ZkMetalStatus zkmsm_device_sync(void) {
+    return guarded([&] {
+        ZK_CUDA(cudaDeviceSynchronize());
+        return ZKMETAL_SUCCESS;
+    });
+}
+
+}  // extern "C"

@@ -1,0 +1,386 @@
+// Host-side MSM engine: plans a batch of MSMs, owns the device workspace and
+// issues the kernel pipeline on its stream.
+//
+// Replaces the orchestration of the reference's MetalMSM.msm
+// (MSM/MSMEngine.swift:287-909) and BLS12381MSM.msm
+// (MSM/BLS12381MSMEngine.swift:260-513): buffer caching (ensureBuffers,
+// MSMEngine.swift:232-277) becomes a grow-only device workspace; window
+// selection (MSMEngine.swift:356-373) becomes a per-MSM cost model
+// (overridable, and refined by the autotuner); the CPU sort and CPU Horner
+// become device kernels so a whole batch runs without host round trips.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "types.cuh"
+
+namespace zkmsm {
+
+void set_error(const std::string& s);
+
+struct CudaError {
+    cudaError_t code;
+    std::string where;
+};
+
+#define ZK_CUDA(call)                                                       \
+    do {                                                                    \
+        cudaError_t e__ = (call);                                           \
+        if (e__ != cudaSuccess) throw ::zkmsm::CudaError{e__, #call};       \
+    } while (0)
+
+// Grow-only device buffer.
+struct DevBuf {
+    void* p = nullptr;
+    size_t cap = 0;
+    void ensure(size_t bytes) {
+        if (bytes <= cap) return;
+        if (p) cudaFree(p);
+        p = nullptr;
+        cap = 0;
+        size_t want = bytes + bytes / 8 + 256;
+        ZK_CUDA(cudaMalloc(&p, want));
+        cap = want;
+    }
+    template <class T>
+    T* as() const { return static_cast<T*>(p); }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        cap = 0;
+    }
+    DevBuf() = default;
+    DevBuf(const DevBuf&) = delete;
+    DevBuf& operator=(const DevBuf&) = delete;
+    ~DevBuf() { release(); }
+};
+
+struct Tuning {
+    int window_bits = 0;  // 0: cost model
+    int chunk = 0;        // level-1 chunk length, 0: automatic
+    int glv = -1;         // -1: automatic (on), 0 off, 1 on
+};
+
+// Host description of one batch run.
+struct Plan {
+    int curve = 0;
+    std::vector<MsmDesc> descs;
+    uint64_t total_scalars = 0;
+    uint64_t entry_bound = 0;
+    uint32_t nbuckets = 0;
+    uint32_t nwin_total = 0;
+    // segmented-sum levels: chunk length and chunk-count bound per level
+    std::vector<uint32_t> acc_K, acc_T;
+    std::vector<uint64_t> acc_Mbound;
+    // bucket-reduction levels
+    uint32_t red_L = 8, red_log2L = 3;
+    std::vector<std::vector<RedTask>> red_tasks;
+    std::vector<uint32_t> red_nout;
+    // device copies of descs and reduction tasks (uploaded once per plan)
+    DevBuf d_descs, d_tasks;
+    std::vector<size_t> task_level_off;
+};
+
+// Signed windows a half-scalar of `bits` bits needs at width c.
+inline uint32_t windows_for(uint32_t bits, uint32_t c) { return (bits + 1 + c - 1) / c; }
+
+// Relative cost of window width c for `entries_per_window` entries: mixed
+// additions (one per nonzero digit) plus ~3 XYZZ additions per bucket in the
+// reduction, plus a latency term for the reduction depth and Horner chain.
+inline uint32_t choose_window(uint64_t entries_per_window, uint32_t bits) {
+    double best = 1e300;
+    uint32_t bc = 8;
+    for (uint32_t c = 4; c <= 22; c++) {
+        uint32_t w = windows_for(bits, c);
+        double add = (double)entries_per_window * w;
+        double red = 4.2 * (double)w * (double)(1u << (c - 1));
+        double lat = 2.0e5 * (c + 6) + 4.0e4 * (double)w * c;  // serial tails, in madd units
+        double cost = add + red + lat;
+        if (cost < best) {
+            best = cost;
+            bc = c;
+        }
+    }
+    return bc;
+}
+
+template <class C>
+struct CurveTraits;
+template <>
+struct CurveTraits<Bn254> {
+    static constexpr int id = 0;
+    static constexpr uint32_t half_bits = Bn254Glv::HALF_BITS;
+    static constexpr uint32_t fr_bits = Bn254Fr::BITS;
+};
+template <>
+struct CurveTraits<Bls381> {
+    static constexpr int id = 1;
+    static constexpr uint32_t half_bits = Bls381Glv::HALF_BITS;
+    static constexpr uint32_t fr_bits = Bls381Fr::BITS;
+};
+
+class Engine {
+   public:
+    cudaStream_t stream = nullptr;
+    Tuning tuning;
+    int device = 0;
+    uint64_t launches = 0;  // kernels launched by this engine (for reporting)
+
+    // Optional per-phase timing with CUDA events on the engine's stream:
+    // phases 0 scalar prep + sort, 1 level-1 accumulation, 2 later
+    // segmented-sum levels, 3 bucket reduction, 4 window combine.
+    static constexpr int NPHASE = 5;
+    bool profile = false;
+    std::vector<std::vector<cudaEvent_t>> prof_pending;
+    double phase_ms[NPHASE] = {0, 0, 0, 0, 0};
+    uint64_t phase_calls = 0;
+    std::vector<cudaEvent_t> prof_begin() {
+        std::vector<cudaEvent_t> ev;
+        if (!profile) return ev;
+        ev.resize(NPHASE + 1);
+        for (auto& x : ev) ZK_CUDA(cudaEventCreate(&x));
+        return ev;
+    }
+    void prof_mark(std::vector<cudaEvent_t>& ev, int i) {
+        if (!ev.empty()) ZK_CUDA(cudaEventRecord(ev[i], stream));
+    }
+    void prof_end(std::vector<cudaEvent_t>& ev) {
+        if (!ev.empty()) prof_pending.push_back(std::move(ev));
+    }
+    // Wait for recorded calls and fold their phase times into phase_ms.
+    void prof_collect() {
+        for (auto& ev : prof_pending) {
+            ZK_CUDA(cudaEventSynchronize(ev.back()));
+            for (int p = 0; p < NPHASE; p++) {
+                float ms = 0;
+                ZK_CUDA(cudaEventElapsedTime(&ms, ev[p], ev[p + 1]));
+                phase_ms[p] += ms;
+            }
+            for (auto& x : ev) cudaEventDestroy(x);
+            phase_calls++;
+        }
+        prof_pending.clear();
+    }
+
+    // workspace
+    DevBuf w_points, w_phi, w_scalars, w_counts, w_offsets, w_cursor, w_keys, w_vals, w_buckets;
+    DevBuf w_cnt, w_pos, w_tiles, w_totals, w_pkeys[2], w_pvals[2], w_redS[2], w_redW[2];
+    DevBuf w_results, w_comb;
+    bool comb_ready[2] = {false, false};
+    uint32_t* h_results = nullptr;  // pinned
+    size_t h_results_cap = 0;
+
+    Engine() {
+        ZK_CUDA(cudaGetDevice(&device));
+        ZK_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+    }
+    ~Engine() {
+        if (stream) cudaStreamDestroy(stream);
+        if (h_results) cudaFreeHost(h_results);
+    }
+
+    // ------------------------------------------------------------ planning
+    template <class C>
+    void make_plan(Plan& pl, const std::vector<uint32_t>& counts, const std::vector<uint32_t>& base_offs,
+                   int fmt, uint32_t scalar_bits) const {
+        plan_shape<C>(pl, tuning, counts, base_offs, fmt, scalar_bits);
+    }
+
+    // Pure host planning (no device needed): window widths, bucket layout,
+    // chunking of the segmented sums and the reduction tree.
+    template <class C>
+    static void plan_shape(Plan& pl, const Tuning& tuning, const std::vector<uint32_t>& counts,
+                           const std::vector<uint32_t>& base_offs, int fmt, uint32_t scalar_bits) {
+        pl.curve = CurveTraits<C>::id;
+        uint64_t soff = 0;
+        uint32_t boff = 0, woff = 0;
+        for (size_t m = 0; m < counts.size(); m++) {
+            MsmDesc d{};
+            d.scalar_off = soff;
+            d.n = counts[m];
+            d.base_off = base_offs[m];
+            d.fmt = fmt;
+            bool small = scalar_bits > 0 && scalar_bits <= 64;
+            d.glv = small ? 0 : (tuning.glv == 0 ? 0 : 1);
+            uint32_t bits = small ? scalar_bits : (d.glv ? CurveTraits<C>::half_bits : CurveTraits<C>::fr_bits);
+            uint64_t epw = (uint64_t)d.n * (d.glv ? 2 : 1);
+            uint32_t c = tuning.window_bits > 0 ? (uint32_t)tuning.window_bits : choose_window(epw, bits);
+            if (c > bits + 1) c = bits + 1 < 2 ? 2 : bits + 1;
+            if (c < 2) c = 2;
+            d.c = c;
+            d.nwin = d.n ? windows_for(bits, c) : 0;
+            d.bucket_off = boff;
+            d.win_off = woff;
+            boff += d.nwin * (1u << (c - 1));
+            woff += d.nwin;
+            pl.entry_bound += epw * d.nwin;
+            soff += d.n;
+            pl.descs.push_back(d);
+        }
+        pl.total_scalars = soff;
+        pl.nbuckets = boff;
+        pl.nwin_total = woff;
+        // segmented-sum levels
+        uint64_t M = pl.entry_bound;
+        uint32_t K1 = tuning.chunk > 0 ? (uint32_t)tuning.chunk : 0;
+        if (!K1) {
+            uint64_t resident = 148ull * 512;
+            uint64_t k = M / (resident * 16);
+            K1 = (uint32_t)(k < 8 ? 8 : k > 128 ? 128 : k);
+        }
+        uint32_t K = K1;
+        for (int lvl = 0; lvl < 40; lvl++) {
+            uint64_t T = (M + K - 1) / K;
+            if (T == 0) T = 1;
+            pl.acc_K.push_back(K);
+            pl.acc_T.push_back((uint32_t)T);
+            pl.acc_Mbound.push_back(M);
+            if (T <= 1) break;
+            M = 2 * T;
+            K = 16;
+        }
+        // reduction levels
+        std::vector<RedTask> lvl0;
+        uint32_t off = 0;
+        for (auto& d : pl.descs) {
+            uint32_t B = 1u << (d.c - 1);
+            for (uint32_t w = 0; w < d.nwin; w++) {
+                RedTask t;
+                t.in_off = d.bucket_off + w * B;
+                t.n_in = B;
+                t.out_off = off;
+                t.n_out = (B + pl.red_L - 1) / pl.red_L;
+                off += t.n_out;
+                lvl0.push_back(t);
+            }
+        }
+        pl.red_tasks.push_back(lvl0);
+        pl.red_nout.push_back(off);
+        while (true) {
+            auto& prev = pl.red_tasks.back();
+            bool done = true;
+            for (auto& t : prev)
+                if (t.n_out > 1) done = false;
+            if (done) break;
+            std::vector<RedTask> nx;
+            uint32_t o = 0;
+            for (auto& t : prev) {
+                RedTask u;
+                u.in_off = t.out_off;
+                u.n_in = t.n_out;
+                u.out_off = o;
+                u.n_out = (u.n_in + pl.red_L - 1) / pl.red_L;
+                o += u.n_out;
+                nx.push_back(u);
+            }
+            pl.red_tasks.push_back(nx);
+            pl.red_nout.push_back(o);
+        }
+    }
+
+    // Plans are cached by shape, with their tables uploaded once, so that
+    // repeated calls of the same shape issue no host-to-device copies.
+    std::map<std::string, std::unique_ptr<Plan>> plan_cache;
+
+    template <class C>
+    Plan& get_plan(const std::vector<uint32_t>& counts, const std::vector<uint32_t>& base_offs, int fmt,
+                   uint32_t scalar_bits = 0) {
+        std::string key;
+        auto put = [&](uint64_t v) { key.append(reinterpret_cast<const char*>(&v), sizeof v); };
+        put(CurveTraits<C>::id);
+        put(fmt);
+        put(scalar_bits);
+        put((uint64_t)(uint32_t)tuning.window_bits << 32 | (uint32_t)tuning.chunk);
+        put((uint64_t)(int64_t)tuning.glv);
+        for (auto c : counts) put(c);
+        for (auto b : base_offs) put(b);
+        auto it = plan_cache.find(key);
+        if (it != plan_cache.end()) return *it->second;
+        if (plan_cache.size() >= 256) plan_cache.clear();  // cudaFree in ~DevBuf waits for the device
+        std::unique_ptr<Plan> pl(new Plan());
+        make_plan<C>(*pl, counts, base_offs, fmt, scalar_bits);
+        std::vector<RedTask> blob;
+        for (auto& v : pl->red_tasks) {
+            pl->task_level_off.push_back(blob.size());
+            blob.insert(blob.end(), v.begin(), v.end());
+        }
+        pl->d_tasks.ensure((blob.size() + 1) * sizeof(RedTask));
+        pl->d_descs.ensure((pl->descs.size() + 1) * sizeof(MsmDesc));
+        ZK_CUDA(cudaMemcpy(pl->d_tasks.p, blob.data(), blob.size() * sizeof(RedTask), cudaMemcpyHostToDevice));
+        ZK_CUDA(cudaMemcpy(pl->d_descs.p, pl->descs.data(), pl->descs.size() * sizeof(MsmDesc),
+                           cudaMemcpyHostToDevice));
+        Plan& ref = *pl;
+        plan_cache.emplace(key, std::move(pl));
+        return ref;
+    }
+
+    template <class C>
+    void ensure_workspace(const Plan& pl) {
+        using P = typename C::Fp;
+        const size_t xs = sizeof(Xyzz<P>);
+        w_counts.ensure(((size_t)pl.nbuckets + 1) * 4);
+        w_cursor.ensure(((size_t)pl.nbuckets + 1) * 4);
+        w_keys.ensure(pl.entry_bound * 4 + 16);
+        w_vals.ensure(pl.entry_bound * 4 + 16);
+        w_buckets.ensure((size_t)pl.nbuckets * xs + xs);
+        uint64_t tmax = 1, m2 = 1, m3 = 1;
+        for (size_t l = 0; l < pl.acc_T.size(); l++) tmax = std::max<uint64_t>(tmax, pl.acc_T[l]);
+        if (pl.acc_Mbound.size() > 1) m2 = pl.acc_Mbound[1];
+        for (size_t l = 2; l < pl.acc_Mbound.size(); l++) m3 = std::max<uint64_t>(m3, pl.acc_Mbound[l]);
+        w_cnt.ensure(tmax * 4 + 16);
+        w_pkeys[0].ensure(m2 * 4 + 16);
+        w_pvals[0].ensure(m2 * xs + xs);
+        w_pkeys[1].ensure(m3 * 4 + 16);
+        w_pvals[1].ensure(m3 * xs + xs);
+        w_totals.ensure(64 * 4);
+        size_t r0 = pl.red_nout.empty() ? 1 : pl.red_nout[0];
+        for (int i = 0; i < 2; i++) {
+            w_redS[i].ensure(r0 * xs + xs);
+            w_redW[i].ensure(r0 * xs + xs);
+        }
+        w_results.ensure((pl.descs.size() + 1) * 3 * P::N * 4);
+    }
+
+    // Curve-specific device work: defined in engine_impl.cuh and instantiated
+    // once per curve (inst_bn254.cu, inst_bls381.cu).
+    template <class C>
+    void enqueue(const Plan& pl, const uint32_t* d_bases, const uint32_t* d_phi, const uint32_t* d_scalars,
+                 uint32_t* d_results);
+    template <class C>
+    void make_phi(const uint32_t* d_bases, uint64_t n, uint32_t* d_phi);
+    template <class C>
+    void gen_bases(uint64_t seed, uint64_t index0, uint64_t n, uint32_t* d_out);
+    template <class C>
+    void gen_scalars(uint64_t seed, uint64_t index0, uint64_t n, int dist, int fmt, uint32_t* d_out);
+
+    // Full MSM batch from device inputs: results copied to host `out`
+    // (n_msms x 3 x fp_bytes).
+    template <class C>
+    void run_device(const Plan& pl, const uint32_t* d_bases, const uint32_t* d_phi, const uint32_t* d_scalars,
+                    uint8_t* out) {
+        using P = typename C::Fp;
+        ensure_workspace<C>(pl);
+        enqueue<C>(pl, d_bases, d_phi, d_scalars, w_results.as<uint32_t>());
+        size_t bytes = pl.descs.size() * 3 * P::N * 4;
+        ZK_CUDA(cudaMemcpyAsync(out, w_results.p, bytes, cudaMemcpyDeviceToHost, stream));
+        ZK_CUDA(cudaStreamSynchronize(stream));
+    }
+
+};
+
+// Curve-specific device code is instantiated in its own translation unit
+// (inst_bn254.cu, inst_bls381.cu) so the two curves compile in parallel.
+#define ZKMSM_ENGINE_TEMPLATES(EXT, C)                                                                  \
+    EXT template void Engine::enqueue<C>(const Plan&, const uint32_t*, const uint32_t*, const uint32_t*, \
+                                         uint32_t*);                                                    \
+    EXT template void Engine::make_phi<C>(const uint32_t*, uint64_t, uint32_t*);                        \
+    EXT template void Engine::gen_bases<C>(uint64_t, uint64_t, uint64_t, uint32_t*);                    \
+    EXT template void Engine::gen_scalars<C>(uint64_t, uint64_t, uint64_t, int, int, uint32_t*);
+
+}  // namespace zkmsm

@@ -1,0 +1,148 @@
+// Device-side halves of the Engine: kernel launch sequences.  Included only
+// by the per-curve instantiation units so each curve's kernels compile once.
+#pragma once
+#include "engine.cuh"
+#include "msm_kernels.cuh"
+
+namespace zkmsm {
+
+// Exclusive scan of n u32 in place; total to d_total; optional copy.
+static void scan_u32(Engine& e, uint32_t* d_in_out, uint32_t n, uint32_t* d_total, uint32_t* d_copy) {
+    uint32_t tiles = (n + SCAN_TILE - 1) / SCAN_TILE;
+    if (tiles == 0) tiles = 1;
+    e.w_tiles.ensure((size_t)tiles * 4);
+    k_scan_tiles<<<tiles, SCAN_THREADS, 0, e.stream>>>(d_in_out, n, d_in_out, e.w_tiles.as<uint32_t>());
+    e.launches++;
+    k_scan_sums<<<1, SCAN_THREADS, 0, e.stream>>>(e.w_tiles.as<uint32_t>(), tiles, d_total);
+    e.launches++;
+    k_scan_add<<<tiles, SCAN_THREADS, 0, e.stream>>>(d_in_out, n, e.w_tiles.as<uint32_t>(), d_copy);
+    e.launches++;
+    ZK_CUDA(cudaGetLastError());
+}
+
+
+// ------------------------------------------------------------ pipeline
+// Enqueue the whole batch; results (n_msms x 3 field elements) land in
+// d_results.  No host synchronisation inside (graph capturable).
+template <class C>
+void Engine::enqueue(const Plan& pl, const uint32_t* d_bases, const uint32_t* d_phi, const uint32_t* d_scalars,
+             uint32_t* d_results) {
+    using P = typename C::Fp;
+    const int nd = (int)pl.descs.size();
+    const MsmDesc* dd = pl.d_descs.as<MsmDesc>();
+    uint32_t* tot = w_totals.as<uint32_t>();
+    auto ev = prof_begin();
+    prof_mark(ev, 0);
+    ZK_CUDA(cudaMemsetAsync(w_counts.p, 0, ((size_t)pl.nbuckets + 1) * 4, stream));
+    ZK_CUDA(cudaMemsetAsync(w_buckets.p, 0, (size_t)pl.nbuckets * sizeof(Xyzz<P>), stream));
+    if (pl.total_scalars) {
+        uint64_t g = (pl.total_scalars + 255) / 256;
+        k_digit_hist<C><<<(unsigned)g, 256, 0, stream>>>(d_scalars, dd, nd, pl.total_scalars,
+                                                        w_counts.as<uint32_t>());
+        launches++;
+        ZK_CUDA(cudaGetLastError());
+    }
+    // bucket offsets (exclusive) -> counts array in place, copy to cursor
+    scan_u32(*this, w_counts.as<uint32_t>(), pl.nbuckets, tot + 0, w_cursor.as<uint32_t>());
+    if (pl.total_scalars) {
+        uint64_t g = (pl.total_scalars + 255) / 256;
+        k_digit_scatter<C><<<(unsigned)g, 256, 0, stream>>>(d_scalars, dd, nd, pl.total_scalars,
+                                                           w_cursor.as<uint32_t>(), w_keys.as<uint32_t>(),
+                                                           w_vals.as<uint32_t>());
+        launches++;
+        ZK_CUDA(cudaGetLastError());
+    }
+    prof_mark(ev, 1);
+    // segmented sums
+    const uint32_t* keys = w_keys.as<uint32_t>();
+    int cur = 0;
+    for (size_t l = 0; l < pl.acc_K.size(); l++) {
+        uint32_t K = pl.acc_K[l], T = pl.acc_T[l];
+        uint32_t* d_len = tot + l;
+        uint32_t* d_next = tot + l + 1;
+        k_chunk_count<<<(T + 255) / 256, 256, 0, stream>>>(keys, d_len, K, T, w_cnt.as<uint32_t>());
+        launches++;
+        ZK_CUDA(cudaGetLastError());
+        scan_u32(*this, w_cnt.as<uint32_t>(), T, d_next, nullptr);
+        uint32_t* okeys = w_pkeys[cur].as<uint32_t>();
+        Xyzz<P>* ovals = w_pvals[cur].as<Xyzz<P>>();
+        if (l == 0) {
+            k_acc_l1<C><<<(T + 255) / 256, 256, 0, stream>>>(keys, w_vals.as<uint32_t>(), d_len, K, d_bases,
+                                                             d_phi, w_cnt.as<uint32_t>(),
+                                                             w_buckets.as<Xyzz<P>>(), okeys, ovals);
+            launches++;
+        } else {
+            const Xyzz<P>* ivals = w_pvals[cur ^ 1].as<Xyzz<P>>();
+            k_acc_lj<C><<<(T + 255) / 256, 256, 0, stream>>>(keys, ivals, d_len, K, w_cnt.as<uint32_t>(),
+                                                             w_buckets.as<Xyzz<P>>(), okeys, ovals);
+            launches++;
+        }
+        ZK_CUDA(cudaGetLastError());
+        keys = okeys;
+        cur ^= 1;
+        if (l == 0) prof_mark(ev, 2);
+    }
+    prof_mark(ev, 3);
+    // bucket reduction
+    const Xyzz<P>* inS = w_buckets.as<Xyzz<P>>();
+    const Xyzz<P>* inW = nullptr;
+    int rc = 0;
+    for (size_t l = 0; l < pl.red_tasks.size(); l++) {
+        uint32_t nout = pl.red_nout[l];
+        const RedTask* tk = pl.d_tasks.as<RedTask>() + pl.task_level_off[l];
+        Xyzz<P>* oS = w_redS[rc].as<Xyzz<P>>();
+        Xyzz<P>* oW = w_redW[rc].as<Xyzz<P>>();
+        k_reduce_level<C><<<(nout + 127) / 128, 128, 0, stream>>>(inS, inW, tk, (int)pl.red_tasks[l].size(),
+                                                                 nout, pl.red_L,
+                                                                 (uint32_t)l * pl.red_log2L, oS, oW);
+        launches++;
+        ZK_CUDA(cudaGetLastError());
+        inS = oS;
+        inW = oW;
+        rc ^= 1;
+    }
+    prof_mark(ev, 4);
+    k_combine<C><<<(nd + 31) / 32, 32, 0, stream>>>(inS, inW, dd, nd, d_results);
+    launches++;
+    ZK_CUDA(cudaGetLastError());
+    prof_mark(ev, 5);
+    prof_end(ev);
+}
+
+// endomorphism table for a base array
+template <class C>
+void Engine::make_phi(const uint32_t* d_bases, uint64_t n, uint32_t* d_phi) {
+    if (!n) return;
+    k_endo<C><<<(unsigned)((n + 255) / 256), 256, 0, stream>>>(d_bases, (uint32_t)n, d_phi);
+    launches++;
+    ZK_CUDA(cudaGetLastError());
+}
+
+template <class C>
+void Engine::gen_bases(uint64_t seed, uint64_t index0, uint64_t n, uint32_t* d_out) {
+    using P = typename C::Fp;
+    int ci = CurveTraits<C>::id;
+    if (!comb_ready[ci]) {
+        w_comb.ensure(2 * 32 * 256 * 2 * 12 * 4);
+        uint32_t* tab = w_comb.as<uint32_t>() + ci * 32 * 256 * 2 * 12;
+        k_comb_table<C><<<(32 * 256 + 127) / 128, 128, 0, stream>>>(tab);
+        launches++;
+        ZK_CUDA(cudaGetLastError());
+        comb_ready[ci] = true;
+    }
+    uint32_t* tab = w_comb.as<uint32_t>() + ci * 32 * 256 * 2 * 12;
+    (void)sizeof(P);
+    if (n) k_gen_bases<C><<<(unsigned)((n + 127) / 128), 128, 0, stream>>>(tab, d_out, n, seed, index0);
+    launches += (n) ? 1 : 0;
+    ZK_CUDA(cudaGetLastError());
+    ZK_CUDA(cudaStreamSynchronize(stream));
+}
+
+template <class C>
+void Engine::gen_scalars(uint64_t seed, uint64_t index0, uint64_t n, int dist, int fmt, uint32_t* d_out) {
+    if (n) k_gen_scalars<C><<<(unsigned)((n + 255) / 256), 256, 0, stream>>>(d_out, n, seed, index0, dist, fmt);
+    launches += (n) ? 1 : 0;
+    ZK_CUDA(cudaGetLastError());
+    ZK_CUDA(cudaStreamSynchronize(stream));
+}
+}  // namespace zkmsm

@@ -1,0 +1,771 @@
+// Pippenger MSM kernels (sm_100a), templated on the curve.
+//
+// Pipeline for a batch of MSMs over one base table (a single plain call is a
+// batch of one).  Reference counterparts (Shaders/msm/*.metal and the Swift
+// engine MSM/MSMEngine.swift) are cited per kernel.
+//
+//  1. k_digit_hist    scalar -> integer (Montgomery reduce or mod r), GLV
+//                     split, signed c-bit digits; histogram of global bucket
+//                     ids.          [glv_kernels.metal:172-256,
+//                     msm_kernels.metal:399-439, MSMEngine.swift:595-661]
+//  2. scan            exclusive prefix sum of the histogram (bucket offsets)
+//  3. k_digit_scatter recompute digits, place (bucket, point|endo|sign) at
+//                     the bucket's cursor: a counting sort by bucket.
+//                     [msm_kernels.metal:279-397 (GPU sort, disabled there)]
+//  4. k_acc_l1        bucket accumulation: each thread sums a fixed-length
+//                     chunk of the sorted list with mixed XYZZ additions;
+//                     runs wholly inside a chunk are final buckets, runs cut
+//                     by a chunk edge become partial sums.
+//                     [msm_kernels.metal:16-62]
+//  5. k_acc_lj        the same segmented reduction over the partial sums,
+//                     repeated until no bucket is cut (handles any skew, e.g.
+//                     20% of all points in one bucket for witness scalars).
+//  6. k_reduce_level  per window sum_b b*B_b by a tree of running sums.
+//                     [msm_kernels.metal:152-248]
+//  7. k_combine       Horner over windows, normalise to affine.
+//                     [MSMEngine.swift:899-904, msm_kernels.metal:251-275]
+#pragma once
+#include "types.cuh"
+
+namespace zkmsm {
+
+// Scalar state after preparation: up to two halves, each a magnitude (up to
+// 9 limbs: 256 bits plus a zero guard limb) and a sign.
+struct Halves {
+    uint32_t k[2][9];
+    uint32_t neg[2];
+    int count;
+};
+
+// ------------------------------------------------------------ scalar prep
+
+template <class C>
+ZK_DEV void prepare_scalar(Halves& h, const uint32_t* __restrict__ s8, uint32_t fmt, uint32_t glv) {
+    using Fr = typename C::Fr;
+    using G = typename C::Glv;
+    Fe<Fr> s;
+    const uint4* p4 = reinterpret_cast<const uint4*>(s8);
+    uint4 a = __ldg(p4), b = __ldg(p4 + 1);
+    s.v[0] = a.x; s.v[1] = a.y; s.v[2] = a.z; s.v[3] = a.w;
+    s.v[4] = b.x; s.v[5] = b.y; s.v[6] = b.z; s.v[7] = b.w;
+    if (fmt == 1) {
+        fe_from_mont(s, s);  // s * R^-1 mod r  (bn254_msm.c:1537-1552)
+    } else {
+        // integer form may exceed r: subtract r until below (MSMEngine.swift:182-200);
+        // 2^256 < 6r for both curves, so five passes always suffice
+        Fe<Fr> r;
+#pragma unroll
+        for (int i = 0; i < 8; i++) r.v[i] = Fr::P(i);
+#pragma unroll 1
+        for (int it = 0; it < 6 && fe_geq_int(s, r); it++) fe_sub_int(s, s, r);
+    }
+    if (!glv) {
+#pragma unroll
+        for (int i = 0; i < 8; i++) h.k[0][i] = s.v[i];
+        h.k[0][8] = 0;
+        h.neg[0] = 0;
+        h.count = 1;
+        return;
+    }
+    // c_j = (s * G_j + 2^255) >> 256, 5 limbs each
+    uint32_t c[2][5];
+#pragma unroll
+    for (int j = 0; j < 2; j++) {
+        uint32_t prod[13];
+#pragma unroll
+        for (int i = 0; i < 13; i++) prod[i] = 0;
+#pragma unroll
+        for (int i = 0; i < 8; i++) {
+            uint64_t carry = 0;
+#pragma unroll
+            for (int l = 0; l < 5; l++) {
+                uint32_t g = j == 0 ? G::G1(l) : G::G2(l);
+                uint64_t t = (uint64_t)s.v[i] * g + prod[i + l] + carry;
+                prod[i + l] = (uint32_t)t;
+                carry = t >> 32;
+            }
+            prod[i + 5] = (uint32_t)carry;
+        }
+        // + 2^255 (bit 31 of limb 7)
+        uint64_t t = (uint64_t)prod[7] + 0x80000000u;
+        prod[7] = (uint32_t)t;
+        uint32_t cy = (uint32_t)(t >> 32);
+#pragma unroll
+        for (int i = 8; i < 13; i++) {
+            uint64_t u = (uint64_t)prod[i] + cy;
+            prod[i] = (uint32_t)u;
+            cy = (uint32_t)(u >> 32);
+        }
+#pragma unroll
+        for (int i = 0; i < 5; i++) c[j][i] = prod[8 + i];
+    }
+    // k1 = s - c1*a1 - c2*a2, k2 = -c1*b1 - c2*b2   (mod 2^160, signed)
+    uint32_t k1[5], k2[5];
+#pragma unroll
+    for (int i = 0; i < 5; i++) { k1[i] = s.v[i]; k2[i] = 0; }
+    auto mac = [](uint32_t* acc, const uint32_t* x, int which, bool subtract) {
+        // acc -/+= x * K  where K is the lattice constant selected by `which`
+        uint32_t prod[5] = {0, 0, 0, 0, 0};
+#pragma unroll
+        for (int i = 0; i < 5; i++) {
+            uint64_t carry = 0;
+#pragma unroll
+            for (int l = 0; l + i < 5; l++) {
+                uint32_t kv = which == 0 ? G::A1(l) : which == 1 ? G::A2(l) : which == 2 ? G::B1(l) : G::B2(l);
+                uint64_t t = (uint64_t)x[i] * kv + prod[i + l] + carry;
+                prod[i + l] = (uint32_t)t;
+                carry = t >> 32;
+            }
+        }
+        uint64_t cy = subtract ? 1 : 0;  // two's complement: acc + ~prod + 1
+#pragma unroll
+        for (int i = 0; i < 5; i++) {
+            uint64_t t = (uint64_t)acc[i] + (subtract ? (uint32_t)~prod[i] : prod[i]) + cy;
+            acc[i] = (uint32_t)t;
+            cy = t >> 32;
+        }
+    };
+    mac(k1, c[0], 0, !G::A1_NEG);
+    mac(k1, c[1], 1, !G::A2_NEG);
+    mac(k2, c[0], 2, !G::B1_NEG);
+    mac(k2, c[1], 3, !G::B2_NEG);
+    uint32_t* ks[2] = {k1, k2};
+#pragma unroll
+    for (int j = 0; j < 2; j++) {
+        uint32_t* k = ks[j];
+        uint32_t neg = k[4] >> 31;
+        if (neg) {  // magnitude = -k
+            uint64_t cy = 1;
+#pragma unroll
+            for (int i = 0; i < 5; i++) {
+                uint64_t t = (uint64_t)(~k[i]) + cy;
+                k[i] = (uint32_t)t;
+                cy = t >> 32;
+            }
+        }
+#pragma unroll
+        for (int i = 0; i < 9; i++) h.k[j][i] = i < 5 ? k[i] : 0;
+        h.neg[j] = neg;
+    }
+    h.count = 2;
+}
+
+// c-bit field of a multi-limb magnitude starting at bit `off` (c <= 31, off + c <= 288)
+ZK_DEV uint32_t bit_field(const uint32_t* k, uint32_t off, uint32_t c) {
+    uint32_t li = off >> 5, sh = off & 31;
+    uint64_t w = k[li];
+    if (li + 1 < 9) w |= (uint64_t)k[li + 1] << 32;
+    return (uint32_t)(w >> sh) & ((1u << c) - 1);
+}
+
+// Signed-digit recoding of one half: calls f(window, |digit|, digit_negative)
+// for every window; digits lie in [-2^(c-1), 2^(c-1)].
+template <class F>
+ZK_DEV void for_each_digit(const uint32_t* k, uint32_t c, uint32_t nwin, F&& f) {
+    const uint32_t half = 1u << (c - 1);
+    uint32_t carry = 0;
+#pragma unroll 1
+    for (uint32_t w = 0; w < nwin; w++) {
+        uint32_t v = bit_field(k, w * c, c) + carry;
+        if (v > half) {
+            f(w, (1u << c) - v, 1u);
+            carry = 1;
+        } else {
+            f(w, v, 0u);
+            carry = 0;
+        }
+    }
+}
+
+// Binary search: the MSM owning global scalar index gi (descs sorted by scalar_off)
+ZK_DEV int find_msm(const MsmDesc* __restrict__ d, int nd, uint64_t gi) {
+    int lo = 0, hi = nd - 1;
+    while (lo < hi) {
+        int mid = (lo + hi + 1) >> 1;
+        if (d[mid].scalar_off <= gi) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+// Warp-aggregated atomic increment: lanes that share `key` with the warp's
+// first active lane are served by one atomic (the hot-bucket case); the
+// others issue their own.  Returns the pre-increment value for this lane.
+ZK_DEV uint32_t agg_atomic_inc(uint32_t* base, uint32_t key) {
+    uint32_t active = __activemask();
+    int leader = __ffs(active) - 1;
+    uint32_t lkey = __shfl_sync(active, key, leader);
+    uint32_t same = __ballot_sync(active, key == lkey);
+    uint32_t lane = threadIdx.x & 31;
+    if (key == lkey) {
+        uint32_t basev = 0;
+        if ((int)lane == leader) basev = atomicAdd(base + key, (uint32_t)__popc(same));
+        basev = __shfl_sync(same, basev, leader);
+        return basev + __popc(same & ((1u << lane) - 1));
+    }
+    return atomicAdd(base + key, 1u);
+}
+
+template <class C>
+__global__ void __launch_bounds__(256) k_digit_hist(const uint32_t* __restrict__ scalars,
+                                                    const MsmDesc* __restrict__ descs, int nd,
+                                                    uint64_t total, uint32_t* __restrict__ counts) {
+    uint64_t gi = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (gi >= total) return;
+    const MsmDesc d = descs[find_msm(descs, nd, gi)];
+    Halves h;
+    prepare_scalar<C>(h, scalars + gi * 8, d.fmt, d.glv);
+    const uint32_t B = 1u << (d.c - 1);
+#pragma unroll 1
+    for (int j = 0; j < h.count; j++) {
+        for_each_digit(h.k[j], d.c, d.nwin, [&](uint32_t w, uint32_t a, uint32_t) {
+            if (a) agg_atomic_inc(counts, d.bucket_off + w * B + (a - 1));
+        });
+    }
+}
+
+template <class C>
+__global__ void __launch_bounds__(256) k_digit_scatter(const uint32_t* __restrict__ scalars,
+                                                       const MsmDesc* __restrict__ descs, int nd,
+                                                       uint64_t total, uint32_t* __restrict__ cursor,
+                                                       uint32_t* __restrict__ keys, uint32_t* __restrict__ vals) {
+    uint64_t gi = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (gi >= total) return;
+    const MsmDesc d = descs[find_msm(descs, nd, gi)];
+    Halves h;
+    prepare_scalar<C>(h, scalars + gi * 8, d.fmt, d.glv);
+    const uint32_t B = 1u << (d.c - 1);
+    const uint32_t idx = d.base_off + (uint32_t)(gi - d.scalar_off);
+#pragma unroll 1
+    for (int j = 0; j < h.count; j++) {
+        const uint32_t hneg = h.neg[j];
+        for_each_digit(h.k[j], d.c, d.nwin, [&](uint32_t w, uint32_t a, uint32_t dneg) {
+            if (a) {
+                uint32_t gb = d.bucket_off + w * B + (a - 1);
+                uint32_t pos = agg_atomic_inc(cursor, gb);
+                keys[pos] = gb;
+                vals[pos] = idx | ((uint32_t)j << 30) | ((hneg ^ dneg) << 31);
+            }
+        });
+    }
+}
+
+// ------------------------------------------------------------ loads/stores
+
+template <class P>
+ZK_DEV void load_fe(Fe<P>& f, const uint4* __restrict__ s) {
+#pragma unroll
+    for (int i = 0; i < P::N / 4; i++) {
+        uint4 q = __ldg(s + i);
+        f.v[4 * i] = q.x; f.v[4 * i + 1] = q.y; f.v[4 * i + 2] = q.z; f.v[4 * i + 3] = q.w;
+    }
+}
+
+template <class P>
+ZK_DEV void store_fe(uint4* d, const Fe<P>& f) {
+#pragma unroll
+    for (int i = 0; i < P::N / 4; i++) d[i] = make_uint4(f.v[4 * i], f.v[4 * i + 1], f.v[4 * i + 2], f.v[4 * i + 3]);
+}
+
+template <class P>
+ZK_DEV void load_affine(Affine<P>& a, const uint32_t* __restrict__ table, uint32_t idx) {
+    const uint4* s = reinterpret_cast<const uint4*>(table + (size_t)idx * 2 * P::N);
+    load_fe(a.x, s);
+    load_fe(a.y, s + P::N / 4);
+}
+
+template <class P>
+ZK_DEV void load_xyzz(Xyzz<P>& a, const Xyzz<P>* __restrict__ src) {
+    const uint4* s = reinterpret_cast<const uint4*>(src);
+    load_fe(a.x, s);
+    load_fe(a.y, s + P::N / 4);
+    load_fe(a.zz, s + P::N / 2);
+    load_fe(a.zzz, s + 3 * P::N / 4);
+}
+
+template <class P>
+ZK_DEV void store_xyzz(Xyzz<P>* dst, const Xyzz<P>& a) {
+    uint4* d = reinterpret_cast<uint4*>(dst);
+    store_fe(d, a.x);
+    store_fe(d + P::N / 4, a.y);
+    store_fe(d + P::N / 2, a.zz);
+    store_fe(d + 3 * P::N / 4, a.zzz);
+}
+
+// ------------------------------------------------------------ endomorphism
+
+// phi[i] = (beta * x_i, y_i)   [glv_kernels.metal:260-297]
+template <class C>
+__global__ void __launch_bounds__(256) k_endo(const uint32_t* __restrict__ bases, uint32_t n,
+                                              uint32_t* __restrict__ phi) {
+    using P = typename C::Fp;
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    Affine<P> a;
+    load_affine(a, bases, i);
+    Fe<P> beta;
+#pragma unroll
+    for (int l = 0; l < P::N; l++) beta.v[l] = C::Glv::BETA_MONT(l);
+    fe_mul(a.x, a.x, beta);
+    uint4* d = reinterpret_cast<uint4*>(phi + (size_t)i * 2 * P::N);
+    store_fe(d, a.x);
+    store_fe(d + P::N / 4, a.y);
+}
+
+// ------------------------------------------------------------ segmented sums
+
+// Partial-slot count of a chunk: a run touching the chunk's first entry that
+// began earlier, and a run touching its last entry that goes on after it,
+// are partial; a single run that is cut on either side is one partial.
+static __global__ void __launch_bounds__(256) k_chunk_count(const uint32_t* __restrict__ keys,
+                                                     const uint32_t* __restrict__ d_len, uint32_t K,
+                                                     uint32_t nchunks, uint32_t* __restrict__ cnt) {
+    uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nchunks) return;
+    uint32_t M = *d_len;
+    uint64_t start = (uint64_t)t * K;
+    if (start >= M) {
+        cnt[t] = 0;
+        return;
+    }
+    uint32_t end = (uint32_t)(start + K < (uint64_t)M ? start + K : (uint64_t)M);
+    uint32_t k0 = keys[start], k1 = keys[end - 1];
+    uint32_t cb = start > 0 && keys[start - 1] == k0;
+    uint32_t ca = end < M && keys[end] == k1;
+    cnt[t] = (k0 == k1) ? (cb | ca) : (cb + ca);
+}
+
+// Level 1: chunks of the sorted entry list, mixed additions of gathered bases.
+template <class C>
+__global__ void __launch_bounds__(256) k_acc_l1(const uint32_t* __restrict__ keys, const uint32_t* __restrict__ vals,
+                                                const uint32_t* __restrict__ d_len, uint32_t K,
+                                                const uint32_t* __restrict__ bases,
+                                                const uint32_t* __restrict__ phi,
+                                                const uint32_t* __restrict__ slot_pos,
+                                                Xyzz<typename C::Fp>* __restrict__ buckets,
+                                                uint32_t* __restrict__ pkeys,
+                                                Xyzz<typename C::Fp>* __restrict__ pvals) {
+    using P = typename C::Fp;
+    uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t M = *d_len;
+    uint64_t start64 = (uint64_t)t * K;
+    if (start64 >= M) return;
+    uint32_t start = (uint32_t)start64;
+    uint32_t end = (uint32_t)(start64 + K < (uint64_t)M ? start64 + K : (uint64_t)M);
+    uint32_t cur = keys[start];
+    bool cont_before = start > 0 && keys[start - 1] == cur;
+    bool first_run = true;
+    uint32_t slot = slot_pos[t];
+    Xyzz<P> acc;
+    xyzz_set_id(acc);
+#pragma unroll 1
+    for (uint32_t i = start; i < end; i++) {
+        uint32_t k = keys[i];
+        if (k != cur) {
+            if (first_run && cont_before) {
+                pkeys[slot] = cur;
+                store_xyzz(pvals + slot, acc);
+                slot++;
+            } else {
+                store_xyzz(buckets + cur, acc);
+            }
+            xyzz_set_id(acc);
+            cur = k;
+            first_run = false;
+        }
+        uint32_t v = vals[i];
+        Affine<P> q;
+        load_affine(q, (v >> 30) & 1 ? phi : bases, v & VAL_IDX_MASK);
+        if (!affine_is_id(q)) {
+            if (v >> 31) fe_neg(q.y, q.y);
+            xyzz_add_affine(acc, q);
+        }
+    }
+    bool cont_after = end < M && keys[end] == cur;
+    if ((first_run && cont_before) || cont_after) {
+        pkeys[slot] = cur;
+        store_xyzz(pvals + slot, acc);
+    } else {
+        store_xyzz(buckets + cur, acc);
+    }
+}
+
+// Level >= 2: the same over partial sums (XYZZ + XYZZ additions).
+template <class C>
+__global__ void __launch_bounds__(256) k_acc_lj(const uint32_t* __restrict__ keys,
+                                                const Xyzz<typename C::Fp>* __restrict__ vals,
+                                                const uint32_t* __restrict__ d_len, uint32_t K,
+                                                const uint32_t* __restrict__ slot_pos,
+                                                Xyzz<typename C::Fp>* __restrict__ buckets,
+                                                uint32_t* __restrict__ pkeys,
+                                                Xyzz<typename C::Fp>* __restrict__ pvals) {
+    using P = typename C::Fp;
+    uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t M = *d_len;
+    uint64_t start64 = (uint64_t)t * K;
+    if (start64 >= M) return;
+    uint32_t start = (uint32_t)start64;
+    uint32_t end = (uint32_t)(start64 + K < (uint64_t)M ? start64 + K : (uint64_t)M);
+    uint32_t cur = keys[start];
+    bool cont_before = start > 0 && keys[start - 1] == cur;
+    bool first_run = true;
+    uint32_t slot = slot_pos[t];
+    Xyzz<P> acc;
+    xyzz_set_id(acc);
+#pragma unroll 1
+    for (uint32_t i = start; i < end; i++) {
+        uint32_t k = keys[i];
+        if (k != cur) {
+            if (first_run && cont_before) {
+                pkeys[slot] = cur;
+                store_xyzz(pvals + slot, acc);
+                slot++;
+            } else {
+                store_xyzz(buckets + cur, acc);
+            }
+            xyzz_set_id(acc);
+            cur = k;
+            first_run = false;
+        }
+        Xyzz<P> q;
+        load_xyzz(q, vals + i);
+        xyzz_add_ni(acc, q);
+    }
+    bool cont_after = end < M && keys[end] == cur;
+    if ((first_run && cont_before) || cont_after) {
+        pkeys[slot] = cur;
+        store_xyzz(pvals + slot, acc);
+    } else {
+        store_xyzz(buckets + cur, acc);
+    }
+}
+
+// ------------------------------------------------------------ bucket reduction
+//
+// A window's sum is sum_{b=1..B} b*B_b = sum_i (i+1) A_i with A_i = B_{i+1}.
+// Each tree node over a bucket range keeps S = sum A_i and W = sum (i - lo) A_i.
+// Merging L children of span `span`: S' = sum S_s and
+// W' = sum W_s + span * sum_s s*S_s, the last sum by a running sum.
+// At the root: window sum = W + S.
+
+ZK_DEV int find_task(const RedTask* __restrict__ t, int nt, uint32_t g) {
+    int lo = 0, hi = nt - 1;
+    while (lo < hi) {
+        int mid = (lo + hi + 1) >> 1;
+        if (t[mid].out_off <= g) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+template <class C>
+__global__ void __launch_bounds__(128) k_reduce_level(const Xyzz<typename C::Fp>* __restrict__ inS,
+                                                      const Xyzz<typename C::Fp>* __restrict__ inW,
+                                                      const RedTask* __restrict__ tasks, int ntasks,
+                                                      uint32_t nout_total, uint32_t L, uint32_t log2span,
+                                                      Xyzz<typename C::Fp>* __restrict__ outS,
+                                                      Xyzz<typename C::Fp>* __restrict__ outW) {
+    using P = typename C::Fp;
+    uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= nout_total) return;
+    const RedTask tk = tasks[find_task(tasks, ntasks, g)];
+    uint32_t local = g - tk.out_off;
+    uint32_t c0 = tk.in_off + local * L;
+    uint32_t cnt = min(L, tk.n_in - local * L);
+    Xyzz<P> run, x, q;
+    xyzz_set_id(run);
+    xyzz_set_id(x);
+#pragma unroll 1
+    for (int s = (int)cnt - 1; s >= 1; s--) {
+        load_xyzz(q, inS + c0 + s);
+        xyzz_add_ni(run, q);
+        xyzz_add_ni(x, run);
+    }
+    load_xyzz(q, inS + c0);
+    xyzz_add_ni(run, q);
+    store_xyzz(outS + g, run);
+#pragma unroll 1
+    for (uint32_t d = 0; d < log2span; d++) xyzz_dbl_ni(x, x);
+    if (inW != nullptr) {
+#pragma unroll 1
+        for (uint32_t s = 0; s < cnt; s++) {
+            load_xyzz(q, inW + c0 + s);
+            xyzz_add_ni(x, q);
+        }
+    }
+    store_xyzz(outW + g, x);
+}
+
+// Horner over each MSM's windows; output reference-layout Jacobian (X, Y, Z)
+// Montgomery with Z = 1 (or the identity (1, 1, 0)).
+template <class C>
+__global__ void k_combine(const Xyzz<typename C::Fp>* __restrict__ rootS,
+                          const Xyzz<typename C::Fp>* __restrict__ rootW,
+                          const MsmDesc* __restrict__ descs, int nd, uint32_t* __restrict__ out) {
+    using P = typename C::Fp;
+    int m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= nd) return;
+    const MsmDesc d = descs[m];
+    Xyzz<P> acc, q;
+    xyzz_set_id(acc);
+    uint32_t* o = out + (size_t)m * 3 * P::N;
+    if (d.n == 0) {
+        Fe<P> one;
+        fe_set_one(one);
+        for (int l = 0; l < P::N; l++) { o[l] = one.v[l]; o[P::N + l] = one.v[l]; o[2 * P::N + l] = 0; }
+        return;
+    }
+#pragma unroll 1
+    for (int w = (int)d.nwin - 1; w >= 0; w--) {
+        if (w != (int)d.nwin - 1) {
+#pragma unroll 1
+            for (uint32_t b = 0; b < d.c; b++) xyzz_dbl_ni(acc, acc);
+        }
+        load_xyzz(q, rootS + d.win_off + w);
+        xyzz_add_ni(acc, q);
+        load_xyzz(q, rootW + d.win_off + w);
+        xyzz_add_ni(acc, q);
+    }
+    Affine<P> a;
+    xyzz_to_affine_ni(a, acc);
+    Fe<P> one;
+    fe_set_one(one);
+    bool id = xyzz_is_id(acc);
+    for (int l = 0; l < P::N; l++) {
+        o[l] = id ? one.v[l] : a.x.v[l];
+        o[P::N + l] = id ? one.v[l] : a.y.v[l];
+        o[2 * P::N + l] = id ? 0u : one.v[l];
+    }
+}
+
+// ------------------------------------------------------------ scan (u32)
+
+constexpr int SCAN_THREADS = 256;
+constexpr int SCAN_ITEMS = 8;
+constexpr int SCAN_TILE = SCAN_THREADS * SCAN_ITEMS;
+
+ZK_DEV uint32_t block_excl_scan(uint32_t v, uint32_t* sh, uint32_t& total) {
+    uint32_t lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    uint32_t x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= (uint32_t)o) x += y;
+    }
+    if (lane == 31) sh[wid] = x;
+    __syncthreads();
+    if (wid == 0) {
+        uint32_t s = lane < SCAN_THREADS / 32 ? sh[lane] : 0;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            uint32_t y = __shfl_up_sync(0xffffffffu, s, o);
+            if (lane >= (uint32_t)o) s += y;
+        }
+        if (lane < SCAN_THREADS / 32) sh[lane] = s;
+    }
+    __syncthreads();
+    total = sh[SCAN_THREADS / 32 - 1];
+    uint32_t pre = wid ? sh[wid - 1] : 0;
+    __syncthreads();
+    return pre + x - v;
+}
+
+// phase 1: per-tile exclusive scan, tile totals
+static __global__ void __launch_bounds__(SCAN_THREADS) k_scan_tiles(const uint32_t* __restrict__ in, uint32_t n,
+                                                             uint32_t* __restrict__ out,
+                                                             uint32_t* __restrict__ tile_sums) {
+    __shared__ uint32_t sh[SCAN_THREADS / 32];
+    uint64_t base = (uint64_t)blockIdx.x * SCAN_TILE + (uint64_t)threadIdx.x * SCAN_ITEMS;
+    uint32_t v[SCAN_ITEMS], s = 0;
+#pragma unroll
+    for (int i = 0; i < SCAN_ITEMS; i++) {
+        v[i] = base + i < n ? in[base + i] : 0;
+        s += v[i];
+    }
+    uint32_t total;
+    uint32_t pre = block_excl_scan(s, sh, total);
+#pragma unroll
+    for (int i = 0; i < SCAN_ITEMS; i++) {
+        if (base + i < n) out[base + i] = pre;
+        pre += v[i];
+    }
+    if (threadIdx.x == 0) tile_sums[blockIdx.x] = total;
+}
+
+// phase 2: one block scans the tile totals in place; writes the grand total
+static __global__ void __launch_bounds__(SCAN_THREADS) k_scan_sums(uint32_t* __restrict__ tile_sums, uint32_t ntiles,
+                                                            uint32_t* __restrict__ d_total) {
+    __shared__ uint32_t sh[SCAN_THREADS / 32];
+    uint32_t carry = 0;
+    for (uint32_t b0 = 0; b0 < ntiles; b0 += SCAN_THREADS) {
+        uint32_t i = b0 + threadIdx.x;
+        uint32_t v = i < ntiles ? tile_sums[i] : 0;
+        uint32_t total;
+        uint32_t pre = block_excl_scan(v, sh, total);
+        if (i < ntiles) tile_sums[i] = carry + pre;
+        carry += total;
+    }
+    if (threadIdx.x == 0) *d_total = carry;
+}
+
+// phase 3: add tile offsets; optionally duplicate into a second array
+static __global__ void __launch_bounds__(SCAN_THREADS) k_scan_add(uint32_t* __restrict__ out, uint32_t n,
+                                                           const uint32_t* __restrict__ tile_sums,
+                                                           uint32_t* __restrict__ copy) {
+    uint64_t base = (uint64_t)blockIdx.x * SCAN_TILE;
+    uint32_t add = tile_sums[blockIdx.x];
+#pragma unroll
+    for (int i = 0; i < SCAN_ITEMS; i++) {
+        uint64_t j = base + (uint64_t)i * SCAN_THREADS + threadIdx.x;
+        if (j < n) {
+            uint32_t v = out[j] + add;
+            out[j] = v;
+            if (copy) copy[j] = v;
+        }
+    }
+}
+
+// ------------------------------------------------------------ synthetic inputs
+// Counter-based generator shared with the Python restatement in the oracle:
+// word = splitmix64(splitmix64(seed*FNV ^ stream*golden ^ (index*8 + word)) ^ attempt*C)
+
+ZK_DEV uint64_t splitmix64(uint64_t x) {
+    x += 0x9E3779B97F4A7C15ull;
+    uint64_t z = x;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+
+ZK_DEV uint64_t draw_word(uint64_t seed, uint64_t stream, uint64_t index, uint64_t attempt, uint64_t word) {
+    uint64_t ctr = seed * 0x100000001B3ull + stream * 0x9E3779B1ull;
+    ctr = splitmix64(ctr ^ (index * 8 + word));
+    return splitmix64(ctr ^ (attempt * 0xD1B54A32D192ED03ull));
+}
+
+// uniform in [lo, r) by masked rejection (at most 64 attempts; the chance of
+// needing more is below 2^-130 for both curves, then 1 is used)
+template <class Fr>
+ZK_DEV void uniform_fr(uint32_t out[8], uint64_t seed, uint64_t stream, uint64_t index, uint32_t lo) {
+    const int nbits = Fr::BITS;
+#pragma unroll 1
+    for (uint64_t att = 0; att < 64; att++) {
+        Fe<Fr> v;
+#pragma unroll
+        for (int w = 0; w < 4; w++) {
+            uint64_t x = draw_word(seed, stream, index, att, w);
+            v.v[2 * w] = (uint32_t)x;
+            v.v[2 * w + 1] = (uint32_t)(x >> 32);
+        }
+        // mask to the bit length of r
+        const int top = nbits - 224;  // bits kept in limb 7
+        v.v[7] &= top >= 32 ? 0xffffffffu : ((1u << top) - 1);
+        Fe<Fr> r;
+#pragma unroll
+        for (int i = 0; i < 8; i++) r.v[i] = Fr::P(i);
+        bool below = !fe_geq_int(v, r);
+        bool atleast = true;
+        if (lo) atleast = !fe_is_zero(v);
+        if (below && atleast) {
+#pragma unroll
+            for (int i = 0; i < 8; i++) out[i] = v.v[i];
+            return;
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < 8; i++) out[i] = i == 0 ? 1u : 0u;
+}
+
+constexpr uint64_t STREAM_BASE_K = 1, STREAM_SCALAR = 2, STREAM_KIND = 3;
+
+// scalars: dist 0 uniform Fr, 1 witness-like; fmt 0 integer, 1 Montgomery
+template <class C>
+__global__ void k_gen_scalars(uint32_t* __restrict__ out, uint64_t n, uint64_t seed, uint64_t index0,
+                              int dist, int fmt) {
+    using Fr = typename C::Fr;
+    uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    uint64_t gi = index0 + i;
+    uint32_t s[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    if (dist == 0) {
+        uniform_fr<Fr>(s, seed, STREAM_SCALAR, gi, 0);
+    } else {
+        uint64_t u = draw_word(seed, STREAM_KIND, gi, 0, 0) % 100;
+        if (u < 40) {
+        } else if (u < 60) {
+            s[0] = 1;
+        } else if (u < 85) {
+            s[0] = (uint32_t)draw_word(seed, STREAM_SCALAR, gi, 0, 0);
+        } else {
+            uniform_fr<Fr>(s, seed, STREAM_SCALAR, gi, 0);
+        }
+    }
+    if (fmt == 1) {
+        Fe<Fr> v;
+#pragma unroll
+        for (int l = 0; l < 8; l++) v.v[l] = s[l];
+        fe_to_mont(v, v);
+#pragma unroll
+        for (int l = 0; l < 8; l++) s[l] = v.v[l];
+    }
+    uint4* o = reinterpret_cast<uint4*>(out + i * 8);
+    o[0] = make_uint4(s[0], s[1], s[2], s[3]);
+    o[1] = make_uint4(s[4], s[5], s[6], s[7]);
+}
+
+// Fixed-base comb: table[j*256 + v] = v * 2^(8j) * G (affine), j < 32.
+// Built by one thread per entry with double-and-add from G.
+template <class C>
+__global__ void k_comb_table(uint32_t* __restrict__ table) {
+    using P = typename C::Fp;
+    uint32_t e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= 32 * 256) return;
+    uint32_t j = e >> 8, v = e & 255;
+    Affine<P> g;
+#pragma unroll
+    for (int l = 0; l < P::N; l++) { g.x.v[l] = C::Gen::X_MONT(l); g.y.v[l] = C::Gen::Y_MONT(l); }
+    Xyzz<P> acc;
+    xyzz_set_id(acc);
+    // acc = v * 2^(8j) * G: bits of v from the top, then 8j doublings
+#pragma unroll 1
+    for (int b = 7; b >= 0; b--) {
+        xyzz_dbl_ni(acc, acc);
+        if ((v >> b) & 1) xyzz_add_affine_ni(acc, g);
+    }
+#pragma unroll 1
+    for (uint32_t d = 0; d < 8 * j; d++) xyzz_dbl_ni(acc, acc);
+    Affine<P> a;
+    xyzz_to_affine_ni(a, acc);
+    uint4* o = reinterpret_cast<uint4*>(table + (size_t)e * 2 * P::N);
+    store_fe(o, a.x);
+    store_fe(o + P::N / 4, a.y);
+}
+
+// bases[i] = k_i * G with k_i uniform in [1, r): 32 mixed additions from the comb
+template <class C>
+__global__ void __launch_bounds__(128) k_gen_bases(const uint32_t* __restrict__ table, uint32_t* __restrict__ out,
+                                                   uint64_t n, uint64_t seed, uint64_t index0) {
+    using P = typename C::Fp;
+    uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    uint32_t k[8];
+    uniform_fr<typename C::Fr>(k, seed, STREAM_BASE_K, index0 + i, 1);
+    Xyzz<P> acc;
+    xyzz_set_id(acc);
+#pragma unroll 1
+    for (int j = 0; j < 32; j++) {
+        uint32_t byte = (k[j >> 2] >> (8 * (j & 3))) & 255;
+        if (byte) {
+            Affine<P> q;
+            load_affine(q, table, j * 256 + byte);
+            xyzz_add_affine_ni(acc, q);
+        }
+    }
+    Affine<P> a;
+    xyzz_to_affine_ni(a, acc);
+    uint4* o = reinterpret_cast<uint4*>(out + i * 2 * P::N);
+    store_fe(o, a.x);
+    store_fe(o + P::N / 4, a.y);
+}
+
+}  // namespace zkmsm

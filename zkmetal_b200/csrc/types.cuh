@@ -1,0 +1,40 @@
+// Plain data shared by the host engine and the kernels.
+#pragma once
+#include "curve.cuh"
+
+namespace zkmsm {
+
+template <class Fp_, class Fr_, class Glv_, class Gen_>
+struct CurveCfg {
+    using Fp = Fp_;
+    using Fr = Fr_;
+    using Glv = Glv_;
+    using Gen = Gen_;
+};
+using Bn254 = CurveCfg<Bn254Fp, Bn254Fr, Bn254Glv, Bn254Gen>;
+using Bls381 = CurveCfg<Bls381Fp, Bls381Fr, Bls381Glv, Bls381Gen>;
+
+// One MSM of a batch, as the kernels see it.
+struct MsmDesc {
+    uint64_t scalar_off;  // index of its first scalar in the scalar array
+    uint32_t n;           // number of (base, scalar) pairs
+    uint32_t base_off;    // index of its first base in the base table
+    uint32_t c;           // window bits
+    uint32_t nwin;        // number of windows
+    uint32_t glv;         // 1: split scalars with the endomorphism
+    uint32_t bucket_off;  // first global bucket id
+    uint32_t fmt;         // 0: integer scalars, 1: Montgomery-form Fr
+    uint32_t win_off;     // first window-sum slot
+};
+
+// Sorted-entry value: base index (30 bits) | endo << 30 | negate << 31
+constexpr uint32_t VAL_IDX_MASK = 0x3fffffffu;
+
+struct RedTask {
+    uint32_t in_off;   // first child node
+    uint32_t n_in;     // children
+    uint32_t out_off;  // first parent node (prefix sum of parents per task)
+    uint32_t n_out;
+};
+
+}  // namespace zkmsm
