@@ -192,7 +192,10 @@ def run_ours(args):
     assert L.zkmsm_gen_scalars(eng.handle, 0, args.seed, rank * n, n, 0 if args.dist == "uniform" else 1, 1,
                                sc.data_ptr()) == 0
     log("rank %d: inputs generated in %.1f s" % (rank, time.time() - t0))
-    stream = torch.cuda.current_stream()
+    # a dedicated stream: torch's default stream has handle 0, which the
+    # library reads as "use the engine's own stream"
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
     gathered = torch.empty(world * 96, dtype=torch.uint8, device="cuda")
     final = torch.empty(96, dtype=torch.uint8, device="cuda")
 
