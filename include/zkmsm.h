@@ -205,6 +205,22 @@ ZkMetalStatus zkmsm_sum_results(int curve, const uint8_t* results, uint32_t coun
 /* Same on device buffers, enqueued on `stream` (cudaStream_t) without waiting. */
 ZkMetalStatus zkmsm_sum_results_device(int curve, const void* d_results, uint32_t count, void* d_out, void* stream);
 
+/* NEW, with no counterpart in the reference: a BN254 G1 MSM that allocates no
+ * device memory, for callers that cannot call cudaMalloc -- e.g. a framework
+ * that has already reserved nearly all of HBM for its own pool, or a hot loop
+ * that forbids allocation after start-up because cudaMalloc/cudaFree may
+ * synchronise the device.  Inputs and output are the caller's device buffers:
+ * n_points affine points (64 B), n_points scalars (32 B, scalar_fmt), result
+ * 3 x 32 B (Jacobian, Z = 1 or the identity).  n_points <= 8192; larger ->
+ * ZKMETAL_ERR_INVALID_INPUT.  Scratch is one static device array of about
+ * 7.6 MB that every GPU loading the library holds until exit and that all
+ * calls share: calls whose GPU work overlaps race, so serialise them.  The
+ * first call on a device looks the array's address up (do it before any
+ * stream capture).  Enqueues on `stream` (cudaStream_t; 0 = legacy default
+ * stream) and returns without waiting. */
+ZkMetalStatus zkmsm_bn254_msm_noalloc(const void* d_points, const void* d_scalars, int scalar_fmt,
+                                      uint32_t n_points, void* d_result, void* stream);
+
 /* Device memory helpers for callers without a CUDA runtime of their own. */
 void* zkmsm_device_alloc(uint64_t bytes);
 void zkmsm_device_free(void* p);

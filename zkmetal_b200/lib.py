@@ -82,6 +82,7 @@ _SIGS = {
                                     ctypes.POINTER(ctypes.c_double)]),
     "zkmsm_sum_results": (c_i32, [c_int, c_vp, c_u32, c_vp]),
     "zkmsm_sum_results_device": (c_i32, [c_int, c_vp, c_u32, c_vp, c_vp]),
+    "zkmsm_bn254_msm_noalloc": (c_i32, [c_vp, c_vp, c_int, c_u32, c_vp, c_vp]),
     "zkmsm_device_alloc": (c_vp, [c_u64]),
     "zkmsm_device_free": (None, [c_vp]),
     "zkmsm_memcpy_h2d": (c_i32, [c_vp, c_vp, c_u64]),
