@@ -275,7 +275,10 @@ def run_ours(args):
     prod_s = ctypes.c_double()
     bn_mul = ctypes.c_double()
     assert L.zkmsm_measure_peaks(ctypes.byref(prod_s), ctypes.byref(bn_mul), None) == 0
-    peak = prod_s.value / 1e9
+    # the integer-multiply ceiling is the single-instruction 64-bit product
+    # (mad.wide.u32), twice the rate of the low/high multiply-add pair
+    wide = L.zkmsm_wide_products_per_s()
+    peak = max(prod_s.value, wide) / 1e9
     acc_ms = phases[1]
     achieved = CANON_PRODUCTS_PER_POINT["bn254"] * n / (acc_ms * 1e-3) / 1e9 if acc_ms > 0 else None
     msm_achieved = CANON_PRODUCTS_PER_POINT["bn254"] * n / (ms * 1e-3) / 1e9
@@ -310,7 +313,8 @@ def run_ours(args):
                      "peak": round(peak, 1), "unit": "G word-products/s",
                      "frac": round(achieved / peak, 4) if achieved else None, "traffic": traffic,
                      "kernel": "k_acc_l1 (bucket accumulation)",
-                     "peak_source": "measured live: mad.lo.cc+madc.hi pairs, all SMs (zkmsm_measure_peaks)",
+                     "peak_source": "measured live: 64-bit mad.wide.u32 products, all SMs (zkmsm_measure_peaks); "
+                                    "low/high multiply-add pairs reach %.1f G/s" % (prod_s.value / 1e9),
                      "msm_achieved": round(msm_achieved, 1), "msm_frac": round(msm_achieved / peak, 4),
                      "bn254_fe_mul_per_s": round(bn_mul.value / 1e9, 2)},
         "e2e": {"value": round(e2e_ms, 3) if e2e_ms else None, "unit": "ms", "h2d_bytes_per_step": n * 96,

@@ -199,6 +199,10 @@ uint64_t zkmsm_engine_launch_count(ZkMetalMSMEngine engine);
  * BLS12-381 field code (either output pointer may be NULL). */
 ZkMetalStatus zkmsm_measure_peaks(double* products_per_s, double* bn254_mul_per_s, double* bls381_mul_per_s);
 
+/* Word products per second of the single-instruction 64-bit form
+ * (mad.wide.u32) measured by the last zkmsm_measure_peaks call. */
+double zkmsm_wide_products_per_s(void);
+
 /* Sum `count` results (each 3 field elements in the result layout above) into
  * one; used to combine the partial MSMs of point-range shards. */
 ZkMetalStatus zkmsm_sum_results(int curve, const uint8_t* results, uint32_t count, uint8_t* out);

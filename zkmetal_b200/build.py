@@ -49,10 +49,14 @@ def up_to_date():
         return f.read().strip() == _digest()
 
 
-def build(force=False, ptxas_verbose=False, extra=None):
-    if not force and up_to_date():
+def build(force=False, ptxas_verbose=False, extra=None, out=None):
+    """Compile the library.  `extra` adds nvcc flags (e.g. -D tuning switches)
+    and `out` writes the library elsewhere (used to compare variants)."""
+    lib = os.path.abspath(out) if out else LIB
+    os.makedirs(os.path.dirname(lib), exist_ok=True)
+    if not force and not extra and not out and up_to_date():
         return LIB
-    objdir = os.path.join(HERE, "_build")
+    objdir = os.path.join(HERE, "_build" if not out else "_build_" + os.path.basename(out).replace(".", "_"))
     os.makedirs(objdir, exist_ok=True)
     base = [NVCC, "-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC,-O2", "--expt-relaxed-constexpr",
             "-I", os.path.join(ROOT, "include")] + ARCH
@@ -67,13 +71,21 @@ def build(force=False, ptxas_verbose=False, extra=None):
     bad = [s for s, p in procs if p.wait() != 0]
     if bad:
         raise RuntimeError("nvcc failed for " + ", ".join(bad))
-    tmp = LIB + ".tmp"
+    tmp = lib + ".tmp"
     subprocess.check_call([NVCC, "-shared"] + ARCH + objs + ["-o", tmp, "-lcudart"])
-    os.replace(tmp, LIB)
-    with open(STAMP, "w") as f:
-        f.write(_digest())
-    return LIB
+    os.replace(tmp, lib)
+    if lib == LIB and not extra:
+        with open(STAMP, "w") as f:
+            f.write(_digest())
+    return lib
 
 
 if __name__ == "__main__":
-    print(build(force="--force" in sys.argv, ptxas_verbose="--verbose-ptxas" in sys.argv))
+    import argparse
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--force", action="store_true")
+    ap.add_argument("--verbose-ptxas", action="store_true")
+    ap.add_argument("-D", dest="defines", action="append", default=[], help="extra -D for nvcc")
+    ap.add_argument("--out", default=None, help="write the library to this path instead")
+    a = ap.parse_args()
+    print(build(force=a.force, ptxas_verbose=a.verbose_ptxas, extra=["-D" + d for d in a.defines], out=a.out))

@@ -113,7 +113,9 @@ ZK_DEV void xyzz_dbl(Xyzz<P>& r, const Xyzz<P>& a) {
     fe_mul(r.zzz, w, a.zzz);
 }
 
-// acc += (x, y) with (x, y) affine and not the identity (madd-2008-s)
+// acc += (x, y) with (x, y) affine and not the identity (madd-2008-s).
+// The order of the products is chosen to keep few values live at once
+// (ZZ3, ZZZ3 early; PP and PPP retired as soon as possible).
 template <class P>
 ZK_DEV void xyzz_add_affine(Xyzz<P>& acc, const Affine<P>& q) {
     if (xyzz_is_id(acc)) {
@@ -123,30 +125,30 @@ ZK_DEV void xyzz_add_affine(Xyzz<P>& acc, const Affine<P>& q) {
         fe_set_one(acc.zzz);
         return;
     }
-    Fe<P> u2, s2, pp, ppp, qq, t;
-    fe_mul(u2, q.x, acc.zz);     // U2 = X2*ZZ1
-    fe_mul(s2, q.y, acc.zzz);    // S2 = Y2*ZZZ1
-    fe_sub(u2, u2, acc.x);       // P = U2 - X1
-    fe_sub(s2, s2, acc.y);       // R = S2 - Y1
-    if (fe_is_zero(u2)) {
-        if (fe_is_zero(s2)) xyzz_dbl_affine_ni(acc, q);
+    Fe<P> p, r, t;
+    fe_mul(p, q.x, acc.zz);      // U2 = X2*ZZ1
+    fe_mul(r, q.y, acc.zzz);     // S2 = Y2*ZZZ1
+    fe_sub(p, p, acc.x);         // P = U2 - X1
+    fe_sub(r, r, acc.y);         // R = S2 - Y1
+    if (fe_is_zero(p)) {
+        if (fe_is_zero(r)) xyzz_dbl_affine_ni(acc, q);
         else xyzz_set_id(acc);
         return;
     }
-    fe_sqr(pp, u2);              // PP = P^2
-    fe_mul(ppp, u2, pp);         // PPP = P*PP
-    fe_mul(qq, acc.x, pp);       // Q = X1*PP
-    fe_sqr(t, s2);
+    Fe<P> pp, ppp;
+    fe_sqr(pp, p);               // PP = P^2
+    fe_mul(ppp, p, pp);          // PPP = P*PP
+    fe_mul(acc.zz, acc.zz, pp);  // ZZ3 = ZZ1*PP
+    fe_mul(acc.zzz, acc.zzz, ppp);  // ZZZ3 = ZZZ1*PPP
+    fe_mul(pp, acc.x, pp);       // Q = X1*PP
+    fe_sqr(t, r);
     fe_sub(t, t, ppp);
-    fe_sub(t, t, qq);
-    fe_sub(t, t, qq);            // X3 = R^2 - PPP - 2Q
-    fe_sub(qq, qq, t);
-    fe_mul(qq, s2, qq);          // R(Q - X3)
-    fe_mul(s2, acc.y, ppp);      // Y1*PPP
-    fe_sub(acc.y, qq, s2);
-    acc.x = t;
-    fe_mul(acc.zz, acc.zz, pp);
-    fe_mul(acc.zzz, acc.zzz, ppp);
+    fe_sub(t, t, pp);
+    fe_sub(acc.x, t, pp);        // X3 = R^2 - PPP - 2Q
+    fe_mul(ppp, acc.y, ppp);     // Y1*PPP
+    fe_sub(pp, pp, acc.x);
+    fe_mul(pp, r, pp);           // R(Q - X3)
+    fe_sub(acc.y, pp, ppp);      // Y3
 }
 
 // acc += b, both XYZZ (add-2008-s)

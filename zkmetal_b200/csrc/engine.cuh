@@ -11,6 +11,7 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdint>
 #include <cstring>
 #include <map>
@@ -169,7 +170,7 @@ class Engine {
     }
 
     // workspace
-    DevBuf w_points, w_phi, w_scalars, w_counts, w_offsets, w_cursor, w_keys, w_vals, w_buckets;
+    DevBuf w_points, w_phi, w_scalars, w_counts, w_offsets, w_cursor, w_ents, w_buckets;
     DevBuf w_cnt, w_pos, w_tiles, w_totals, w_pkeys[2], w_pvals[2], w_redS[2], w_redW[2];
     DevBuf w_results, w_comb;
     bool comb_ready[2] = {false, false};
@@ -230,9 +231,13 @@ class Engine {
         uint64_t M = pl.entry_bound;
         uint32_t K1 = tuning.chunk > 0 ? (uint32_t)tuning.chunk : 0;
         if (!K1) {
-            uint64_t resident = 148ull * 512;
-            uint64_t k = M / (resident * 16);
-            K1 = (uint32_t)(k < 8 ? 8 : k > 128 ? 128 : k);
+            // long enough to hold about two average buckets (so few buckets are
+            // cut and the partial-sum levels stay small), short enough to give
+            // at least 8 waves of resident threads
+            uint64_t waves8 = M / (8ull * 148 * 512);
+            uint64_t avg = pl.nbuckets ? M / pl.nbuckets : 1;
+            uint64_t k = std::min<uint64_t>(std::max<uint64_t>(8, waves8), std::max<uint64_t>(16, 2 * avg));
+            K1 = (uint32_t)std::min<uint64_t>(k, 512);
         }
         uint32_t K = K1;
         for (int lvl = 0; lvl < 40; lvl++) {
@@ -326,8 +331,7 @@ class Engine {
         const size_t xs = sizeof(Xyzz<P>);
         w_counts.ensure(((size_t)pl.nbuckets + 1) * 4);
         w_cursor.ensure(((size_t)pl.nbuckets + 1) * 4);
-        w_keys.ensure(pl.entry_bound * 4 + 16);
-        w_vals.ensure(pl.entry_bound * 4 + 16);
+        w_ents.ensure(pl.entry_bound * 8 + 16);
         w_buckets.ensure((size_t)pl.nbuckets * xs + xs);
         uint64_t tmax = 1, m2 = 1, m3 = 1;
         for (size_t l = 0; l < pl.acc_T.size(); l++) tmax = std::max<uint64_t>(tmax, pl.acc_T[l]);

@@ -47,27 +47,28 @@ void Engine::enqueue(const Plan& pl, const uint32_t* d_bases, const uint32_t* d_
     if (pl.total_scalars) {
         uint64_t g = (pl.total_scalars + 255) / 256;
         k_digit_scatter<C><<<(unsigned)g, 256, 0, stream>>>(d_scalars, dd, nd, pl.total_scalars,
-                                                           w_cursor.as<uint32_t>(), w_keys.as<uint32_t>(),
-                                                           w_vals.as<uint32_t>());
+                                                           w_cursor.as<uint32_t>(), w_ents.as<uint2>());
         launches++;
         ZK_CUDA(cudaGetLastError());
     }
     prof_mark(ev, 1);
     // segmented sums
-    const uint32_t* keys = w_keys.as<uint32_t>();
+    const uint32_t* keys = w_ents.as<uint32_t>();  // level 1: keys are the .x of packed entries
+    uint32_t kstride = 2;
     int cur = 0;
     for (size_t l = 0; l < pl.acc_K.size(); l++) {
         uint32_t K = pl.acc_K[l], T = pl.acc_T[l];
         uint32_t* d_len = tot + l;
         uint32_t* d_next = tot + l + 1;
-        k_chunk_count<<<(T + 255) / 256, 256, 0, stream>>>(keys, d_len, K, T, w_cnt.as<uint32_t>());
+        k_chunk_count<<<(T + 255) / 256, 256, 0, stream>>>(keys, kstride, d_len, K, T, w_cnt.as<uint32_t>());
         launches++;
         ZK_CUDA(cudaGetLastError());
         scan_u32(*this, w_cnt.as<uint32_t>(), T, d_next, nullptr);
         uint32_t* okeys = w_pkeys[cur].as<uint32_t>();
         Xyzz<P>* ovals = w_pvals[cur].as<Xyzz<P>>();
         if (l == 0) {
-            k_acc_l1<C><<<(T + 255) / 256, 256, 0, stream>>>(keys, w_vals.as<uint32_t>(), d_len, K, d_bases,
+            k_acc_l1<C><<<(T + ZKMSM_ACC_THREADS - 1) / ZKMSM_ACC_THREADS, ZKMSM_ACC_THREADS, 0, stream>>>(
+                    w_ents.as<uint2>(), d_len, K, d_bases,
                                                              d_phi, w_cnt.as<uint32_t>(),
                                                              w_buckets.as<Xyzz<P>>(), okeys, ovals);
             launches++;
@@ -79,6 +80,7 @@ void Engine::enqueue(const Plan& pl, const uint32_t* d_bases, const uint32_t* d_
         }
         ZK_CUDA(cudaGetLastError());
         keys = okeys;
+        kstride = 1;
         cur ^= 1;
         if (l == 0) prof_mark(ev, 2);
     }

@@ -3,9 +3,13 @@
 // One template serves the BN254 base field (8 limbs) and the BLS12-381 base
 // field (12 limbs); the constants come from params.cuh.  The hot routine is
 // the CIOS Montgomery product (Koc, Acar, Kaliski 1996) written as explicit
-// PTX carry chains: per outer iteration four chains of N integer
-// multiply-adds (low halves of a*b_i, high halves, low halves of m*p, high
-// halves), 4N+3 instructions, with the accumulator kept in N+1 registers.
+// PTX carry chains.  fe_mul_body_eo (the default) splits each row into an
+// even-index and an odd-index chain that run independently; fe_mul_body is
+// the straight form (four chains of N multiply-adds per row, 4N+3
+// instructions, accumulator in N+1 registers).  One out-of-line copy of the
+// product per kernel keeps the hot loops within the instruction cache.
+// Carry chains are written as asm volatile so the compiler keeps their order
+// (the carry flag is invisible to it).
 // Bounds: both moduli satisfy 4p < 2^(32N), so for inputs below 2p the
 // accumulator stays below 2^(32(N+1)) (no carry is ever dropped) and the
 // result before the last conditional subtraction is below 2p.
@@ -113,7 +117,7 @@ ZK_DEV void fe_neg(Fe<P>& r, const Fe<P>& a) {
 
 // r = a*b / 2^(32N) mod p, canonical (a, b < p; also correct mod p for a, b < 2p)
 template <class P>
-ZK_DEV void fe_mul(Fe<P>& r, const Fe<P>& a, const Fe<P>& b) {
+ZK_DEV void fe_mul_body(Fe<P>& r, const Fe<P>& a, const Fe<P>& b) {
     constexpr int N = P::N;
     uint32_t t[N + 1];
 #pragma unroll
@@ -158,6 +162,121 @@ ZK_DEV void fe_mul(Fe<P>& r, const Fe<P>& a, const Fe<P>& b) {
 #pragma unroll
     for (int j = 0; j < N; j++) s.v[j] = t[j];
     fe_reduce_once(r, s);
+}
+
+
+// Even/odd-split CIOS: a*b_i = E + 2^32*O where E holds the products a_j*b_i
+// of even j (low word at limb j, high word at limb j+1) and O those of odd j
+// shifted down one limb, so each is one carry chain without collisions and
+// the two chains of a phase are independent.  State t = e + 2^32*o; after the
+// reduction step e_0 = 0 and t/2^32 = (e >> 32) + o is re-split as
+// e' = o + e_1 (the carry of that one addition enters the next odd chain,
+// whose limb 0 has the same weight) and o' = e >> 64 (a register renaming).
+// Bounds as for fe_mul_body (validated by emulating this exact schedule).
+template <class P>
+ZK_DEV void fe_mul_body_eo(Fe<P>& r, const Fe<P>& a, const Fe<P>& b) {
+    constexpr int N = P::N;
+    uint32_t e[N + 1], o[N + 1];
+#pragma unroll
+    for (int i = 0; i < N; i++) {
+        const uint32_t bi = b.v[i];
+        if (i == 0) {
+#pragma unroll
+            for (int j = 0; j < N; j += 2) {
+                e[j] = a.v[j] * bi;
+                e[j + 1] = __umulhi(a.v[j], bi);
+                o[j] = a.v[j + 1] * bi;
+                o[j + 1] = __umulhi(a.v[j + 1], bi);
+            }
+            e[N] = 0;
+            o[N] = 0;
+        } else {
+            uint32_t x[N + 1], y[N + 1];
+            asm volatile("add.cc.u32 %0, %1, %2;" : "=r"(x[0]) : "r"(o[0]), "r"(e[1]));
+#pragma unroll
+            for (int j = 0; j < N; j += 2) {
+                const uint32_t slo = j + 2 < N ? e[j + 2] : e[N];
+                const uint32_t shi = j + 3 < N ? e[j + 3] : 0u;
+                asm volatile("madc.lo.cc.u32 %0, %1, %2, %3;" : "=r"(y[j]) : "r"(a.v[j + 1]), "r"(bi), "r"(slo));
+                if (j + 2 < N)
+                    asm volatile("madc.hi.cc.u32 %0, %1, %2, %3;" : "=r"(y[j + 1]) : "r"(a.v[j + 1]), "r"(bi), "r"(shi));
+                else
+                    asm volatile("madc.hi.u32 %0, %1, %2, %3;" : "=r"(y[j + 1]) : "r"(a.v[j + 1]), "r"(bi), "r"(shi));
+            }
+            y[N] = 0;
+#pragma unroll
+            for (int j = 1; j <= N; j++) x[j] = o[j];
+            asm volatile("mad.lo.cc.u32 %0, %1, %2, %0;" : "+r"(x[0]) : "r"(a.v[0]), "r"(bi));
+            asm volatile("madc.hi.cc.u32 %0, %1, %2, %0;" : "+r"(x[1]) : "r"(a.v[0]), "r"(bi));
+#pragma unroll
+            for (int j = 2; j < N; j += 2) {
+                asm volatile("madc.lo.cc.u32 %0, %1, %2, %0;" : "+r"(x[j]) : "r"(a.v[j]), "r"(bi));
+                asm volatile("madc.hi.cc.u32 %0, %1, %2, %0;" : "+r"(x[j + 1]) : "r"(a.v[j]), "r"(bi));
+            }
+            asm volatile("addc.u32 %0, %0, 0;" : "+r"(x[N]));
+#pragma unroll
+            for (int j = 0; j <= N; j++) {
+                e[j] = x[j];
+                o[j] = y[j];
+            }
+        }
+        const uint32_t m = e[0] * P::N0;
+        asm volatile("mad.lo.cc.u32 %0, %1, %2, %0;" : "+r"(e[0]) : "r"(m), "r"(P::P(0)));
+        asm volatile("madc.hi.cc.u32 %0, %1, %2, %0;" : "+r"(e[1]) : "r"(m), "r"(P::P(0)));
+#pragma unroll
+        for (int j = 2; j < N; j += 2) {
+            asm volatile("madc.lo.cc.u32 %0, %1, %2, %0;" : "+r"(e[j]) : "r"(m), "r"(P::P(j)));
+            asm volatile("madc.hi.cc.u32 %0, %1, %2, %0;" : "+r"(e[j + 1]) : "r"(m), "r"(P::P(j)));
+        }
+        asm volatile("addc.u32 %0, %0, 0;" : "+r"(e[N]));
+        asm volatile("mad.lo.cc.u32 %0, %1, %2, %0;" : "+r"(o[0]) : "r"(m), "r"(P::P(1)));
+        asm volatile("madc.hi.cc.u32 %0, %1, %2, %0;" : "+r"(o[1]) : "r"(m), "r"(P::P(1)));
+#pragma unroll
+        for (int j = 2; j < N; j += 2) {
+            asm volatile("madc.lo.cc.u32 %0, %1, %2, %0;" : "+r"(o[j]) : "r"(m), "r"(P::P(j + 1)));
+            asm volatile("madc.hi.cc.u32 %0, %1, %2, %0;" : "+r"(o[j + 1]) : "r"(m), "r"(P::P(j + 1)));
+        }
+        asm volatile("addc.u32 %0, %0, 0;" : "+r"(o[N]));
+    }
+    // t = (e >> 32) + o, below 2p
+    Fe<P> s;
+    asm volatile("add.cc.u32 %0, %1, %2;" : "=r"(s.v[0]) : "r"(e[1]), "r"(o[0]));
+#pragma unroll
+    for (int j = 1; j < N - 1; j++)
+        asm volatile("addc.cc.u32 %0, %1, %2;" : "=r"(s.v[j]) : "r"(e[j + 1]), "r"(o[j]));
+    asm volatile("addc.u32 %0, %1, %2;" : "=r"(s.v[N - 1]) : "r"(e[N]), "r"(o[N - 1]));
+    fe_reduce_once(r, s);
+}
+
+#ifndef ZKMSM_MUL_OUTLINE
+#define ZKMSM_MUL_OUTLINE 1
+#endif
+#ifndef ZKMSM_MUL_EO
+#define ZKMSM_MUL_EO 1
+#endif
+
+// One out-of-line copy of the product per kernel keeps the hot loops inside
+// the instruction cache (arguments and result travel in registers).
+template <class P>
+__device__ __noinline__ Fe<P> fe_mul_ool(const Fe<P> a, const Fe<P> b) {
+    Fe<P> r;
+#if ZKMSM_MUL_EO
+    fe_mul_body_eo(r, a, b);
+#else
+    fe_mul_body(r, a, b);
+#endif
+    return r;
+}
+
+template <class P>
+ZK_DEV void fe_mul(Fe<P>& r, const Fe<P>& a, const Fe<P>& b) {
+#if ZKMSM_MUL_OUTLINE
+    r = fe_mul_ool(a, b);
+#elif ZKMSM_MUL_EO
+    fe_mul_body_eo(r, a, b);
+#else
+    fe_mul_body(r, a, b);
+#endif
 }
 
 template <class P>

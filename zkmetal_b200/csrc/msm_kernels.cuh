@@ -158,25 +158,6 @@ ZK_DEV uint32_t bit_field(const uint32_t* k, uint32_t off, uint32_t c) {
     return (uint32_t)(w >> sh) & ((1u << c) - 1);
 }
 
-// Signed-digit recoding of one half: calls f(window, |digit|, digit_negative)
-// for every window; digits lie in [-2^(c-1), 2^(c-1)].
-template <class F>
-ZK_DEV void for_each_digit(const uint32_t* k, uint32_t c, uint32_t nwin, F&& f) {
-    const uint32_t half = 1u << (c - 1);
-    uint32_t carry = 0;
-#pragma unroll 1
-    for (uint32_t w = 0; w < nwin; w++) {
-        uint32_t v = bit_field(k, w * c, c) + carry;
-        if (v > half) {
-            f(w, (1u << c) - v, 1u);
-            carry = 1;
-        } else {
-            f(w, v, 0u);
-            carry = 0;
-        }
-    }
-}
-
 // Binary search: the MSM owning global scalar index gi (descs sorted by scalar_off)
 ZK_DEV int find_msm(const MsmDesc* __restrict__ d, int nd, uint64_t gi) {
     int lo = 0, hi = nd - 1;
@@ -188,22 +169,69 @@ ZK_DEV int find_msm(const MsmDesc* __restrict__ d, int nd, uint64_t gi) {
     return lo;
 }
 
-// Warp-aggregated atomic increment: lanes that share `key` with the warp's
-// first active lane are served by one atomic (the hot-bucket case); the
-// others issue their own.  Returns the pre-increment value for this lane.
-ZK_DEV uint32_t agg_atomic_inc(uint32_t* base, uint32_t key) {
-    uint32_t active = __activemask();
-    int leader = __ffs(active) - 1;
-    uint32_t lkey = __shfl_sync(active, key, leader);
-    uint32_t same = __ballot_sync(active, key == lkey);
-    uint32_t lane = threadIdx.x & 31;
-    if (key == lkey) {
-        uint32_t basev = 0;
-        if ((int)lane == leader) basev = atomicAdd(base + key, (uint32_t)__popc(same));
-        basev = __shfl_sync(same, basev, leader);
-        return basev + __popc(same & ((1u << lane) - 1));
+// Signed-digit stream of a prepared scalar.  Digits of half j, window w:
+// v = field + carry; v > 2^(c-1) gives digit v - 2^c (negative, carry 1),
+// otherwise v (carry 0); digits lie in [-2^(c-1), 2^(c-1)].  The stream
+// yields only nonzero digits, DBATCH at a time, so a thread can issue a whole
+// batch of independent atomics before waiting for any of them.
+constexpr int DBATCH = 8;
+
+struct DigitGen {
+    uint32_t j, w, carry;
+};
+
+ZK_DEV void next_digits(DigitGen& g, const Halves& h, const MsmDesc& d, uint32_t idx, bool (&valid)[DBATCH],
+                        uint32_t (&gb)[DBATCH], uint32_t (&val)[DBATCH]) {
+    const uint32_t half = 1u << (d.c - 1);
+#pragma unroll
+    for (int s = 0; s < DBATCH; s++) {
+        valid[s] = false;
+        gb[s] = 0;
+        val[s] = 0;
+#pragma unroll 1
+        while (g.j < (uint32_t)h.count) {
+            uint32_t v = bit_field(h.k[g.j], g.w * d.c, d.c) + g.carry;
+            uint32_t a, dn;
+            if (v > half) {
+                a = (1u << d.c) - v;
+                dn = 1;
+                g.carry = 1;
+            } else {
+                a = v;
+                dn = 0;
+                g.carry = 0;
+            }
+            uint32_t w = g.w, j = g.j;
+            if (++g.w == d.nwin) {
+                g.w = 0;
+                g.carry = 0;
+                g.j++;
+            }
+            if (a) {
+                valid[s] = true;
+                gb[s] = d.bucket_off + w * half + (a - 1);
+                val[s] = idx | (j << 30) | ((h.neg[j] ^ dn) << 31);
+                break;
+            }
+        }
     }
-    return atomicAdd(base + key, 1u);
+}
+
+// Lanes of `mask` whose key equals the first valid lane's key share one
+// atomic (the hot-bucket case, e.g. many scalars equal to 1).
+struct AggSlot {
+    uint32_t leader, same;
+    bool grp;
+};
+
+ZK_DEV AggSlot agg_slot(uint32_t mask, bool valid, uint32_t key) {
+    AggSlot a;
+    uint32_t m = __ballot_sync(mask, valid);
+    a.leader = m ? __ffs(m) - 1 : 0;
+    uint32_t lk = __shfl_sync(mask, key, a.leader);
+    a.grp = valid && m && key == lk;
+    a.same = __ballot_sync(mask, a.grp);
+    return a;
 }
 
 template <class C>
@@ -212,41 +240,66 @@ __global__ void __launch_bounds__(256) k_digit_hist(const uint32_t* __restrict__
                                                     uint64_t total, uint32_t* __restrict__ counts) {
     uint64_t gi = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (gi >= total) return;
+    const uint32_t mask = __activemask();
+    const uint32_t lane = threadIdx.x & 31;
     const MsmDesc d = descs[find_msm(descs, nd, gi)];
     Halves h;
     prepare_scalar<C>(h, scalars + gi * 8, d.fmt, d.glv);
-    const uint32_t B = 1u << (d.c - 1);
+    DigitGen g{0, 0, 0};
+    if (d.nwin == 0) g.j = (uint32_t)h.count;
+    bool valid[DBATCH];
+    uint32_t gb[DBATCH], val[DBATCH];
 #pragma unroll 1
-    for (int j = 0; j < h.count; j++) {
-        for_each_digit(h.k[j], d.c, d.nwin, [&](uint32_t w, uint32_t a, uint32_t) {
-            if (a) agg_atomic_inc(counts, d.bucket_off + w * B + (a - 1));
-        });
+    while (__any_sync(mask, g.j < (uint32_t)h.count)) {
+        next_digits(g, h, d, 0, valid, gb, val);
+#pragma unroll
+        for (int s = 0; s < DBATCH; s++) {
+            AggSlot a = agg_slot(mask, valid[s], gb[s]);
+            if (a.grp) {
+                if (lane == a.leader) atomicAdd(counts + gb[s], (uint32_t)__popc(a.same));
+            } else if (valid[s]) {
+                atomicAdd(counts + gb[s], 1u);
+            }
+        }
     }
 }
 
+// Counting-sort scatter: entry = (global bucket id, base index | endo << 30 | negate << 31)
 template <class C>
 __global__ void __launch_bounds__(256) k_digit_scatter(const uint32_t* __restrict__ scalars,
                                                        const MsmDesc* __restrict__ descs, int nd,
                                                        uint64_t total, uint32_t* __restrict__ cursor,
-                                                       uint32_t* __restrict__ keys, uint32_t* __restrict__ vals) {
+                                                       uint2* __restrict__ ents) {
     uint64_t gi = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (gi >= total) return;
+    const uint32_t mask = __activemask();
+    const uint32_t lane = threadIdx.x & 31;
     const MsmDesc d = descs[find_msm(descs, nd, gi)];
     Halves h;
     prepare_scalar<C>(h, scalars + gi * 8, d.fmt, d.glv);
-    const uint32_t B = 1u << (d.c - 1);
     const uint32_t idx = d.base_off + (uint32_t)(gi - d.scalar_off);
+    DigitGen g{0, 0, 0};
+    if (d.nwin == 0) g.j = (uint32_t)h.count;
+    bool valid[DBATCH];
+    uint32_t gb[DBATCH], val[DBATCH], base[DBATCH];
+    AggSlot a[DBATCH];
 #pragma unroll 1
-    for (int j = 0; j < h.count; j++) {
-        const uint32_t hneg = h.neg[j];
-        for_each_digit(h.k[j], d.c, d.nwin, [&](uint32_t w, uint32_t a, uint32_t dneg) {
-            if (a) {
-                uint32_t gb = d.bucket_off + w * B + (a - 1);
-                uint32_t pos = agg_atomic_inc(cursor, gb);
-                keys[pos] = gb;
-                vals[pos] = idx | ((uint32_t)j << 30) | ((hneg ^ dneg) << 31);
-            }
-        });
+    while (__any_sync(mask, g.j < (uint32_t)h.count)) {
+        next_digits(g, h, d, idx, valid, gb, val);
+        // issue every atomic of the batch before consuming any result
+#pragma unroll
+        for (int s = 0; s < DBATCH; s++) {
+            a[s] = agg_slot(mask, valid[s], gb[s]);
+            base[s] = 0;
+            if (valid[s] && (!a[s].grp || lane == a[s].leader))
+                base[s] = atomicAdd(cursor + gb[s], a[s].grp ? (uint32_t)__popc(a[s].same) : 1u);
+        }
+#pragma unroll
+        for (int s = 0; s < DBATCH; s++) {
+            uint32_t b = __shfl_sync(mask, base[s], a[s].leader);
+            uint32_t pos = a[s].grp ? b + __popc(a[s].same & ((1u << lane) - 1)) : base[s];
+            if (valid[s]) ents[pos] = make_uint2(gb[s], val[s]);
+        }
     }
 }
 
@@ -317,7 +370,7 @@ __global__ void __launch_bounds__(256) k_endo(const uint32_t* __restrict__ bases
 // Partial-slot count of a chunk: a run touching the chunk's first entry that
 // began earlier, and a run touching its last entry that goes on after it,
 // are partial; a single run that is cut on either side is one partial.
-static __global__ void __launch_bounds__(256) k_chunk_count(const uint32_t* __restrict__ keys,
+static __global__ void __launch_bounds__(256) k_chunk_count(const uint32_t* __restrict__ keys, uint32_t kstride,
                                                      const uint32_t* __restrict__ d_len, uint32_t K,
                                                      uint32_t nchunks, uint32_t* __restrict__ cnt) {
     uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -329,15 +382,21 @@ static __global__ void __launch_bounds__(256) k_chunk_count(const uint32_t* __re
         return;
     }
     uint32_t end = (uint32_t)(start + K < (uint64_t)M ? start + K : (uint64_t)M);
-    uint32_t k0 = keys[start], k1 = keys[end - 1];
-    uint32_t cb = start > 0 && keys[start - 1] == k0;
-    uint32_t ca = end < M && keys[end] == k1;
+    uint32_t k0 = keys[start * kstride], k1 = keys[(uint64_t)(end - 1) * kstride];
+    uint32_t cb = start > 0 && keys[(start - 1) * kstride] == k0;
+    uint32_t ca = end < M && keys[(uint64_t)end * kstride] == k1;
     cnt[t] = (k0 == k1) ? (cb | ca) : (cb + ca);
 }
 
 // Level 1: chunks of the sorted entry list, mixed additions of gathered bases.
+#ifndef ZKMSM_ACC_MINBLOCKS
+#define ZKMSM_ACC_MINBLOCKS 1
+#endif
+#ifndef ZKMSM_ACC_THREADS
+#define ZKMSM_ACC_THREADS 256
+#endif
 template <class C>
-__global__ void __launch_bounds__(256) k_acc_l1(const uint32_t* __restrict__ keys, const uint32_t* __restrict__ vals,
+__global__ void __launch_bounds__(ZKMSM_ACC_THREADS, ZKMSM_ACC_MINBLOCKS) k_acc_l1(const uint2* __restrict__ ents,
                                                 const uint32_t* __restrict__ d_len, uint32_t K,
                                                 const uint32_t* __restrict__ bases,
                                                 const uint32_t* __restrict__ phi,
@@ -352,15 +411,16 @@ __global__ void __launch_bounds__(256) k_acc_l1(const uint32_t* __restrict__ key
     if (start64 >= M) return;
     uint32_t start = (uint32_t)start64;
     uint32_t end = (uint32_t)(start64 + K < (uint64_t)M ? start64 + K : (uint64_t)M);
-    uint32_t cur = keys[start];
-    bool cont_before = start > 0 && keys[start - 1] == cur;
+    uint32_t cur = ents[start].x;
+    bool cont_before = start > 0 && ents[start - 1].x == cur;
     bool first_run = true;
     uint32_t slot = slot_pos[t];
     Xyzz<P> acc;
     xyzz_set_id(acc);
 #pragma unroll 1
     for (uint32_t i = start; i < end; i++) {
-        uint32_t k = keys[i];
+        const uint2 e = ents[i];
+        const uint32_t k = e.x;
         if (k != cur) {
             if (first_run && cont_before) {
                 pkeys[slot] = cur;
@@ -373,7 +433,7 @@ __global__ void __launch_bounds__(256) k_acc_l1(const uint32_t* __restrict__ key
             cur = k;
             first_run = false;
         }
-        uint32_t v = vals[i];
+        const uint32_t v = e.y;
         Affine<P> q;
         load_affine(q, (v >> 30) & 1 ? phi : bases, v & VAL_IDX_MASK);
         if (!affine_is_id(q)) {
@@ -381,7 +441,7 @@ __global__ void __launch_bounds__(256) k_acc_l1(const uint32_t* __restrict__ key
             xyzz_add_affine(acc, q);
         }
     }
-    bool cont_after = end < M && keys[end] == cur;
+    bool cont_after = end < M && ents[end].x == cur;
     if ((first_run && cont_before) || cont_after) {
         pkeys[slot] = cur;
         store_xyzz(pvals + slot, acc);
@@ -429,7 +489,7 @@ __global__ void __launch_bounds__(256) k_acc_lj(const uint32_t* __restrict__ key
         }
         Xyzz<P> q;
         load_xyzz(q, vals + i);
-        xyzz_add_ni(acc, q);
+        xyzz_add(acc, q);
     }
     bool cont_after = end < M && keys[end] == cur;
     if ((first_run && cont_before) || cont_after) {
@@ -478,19 +538,19 @@ __global__ void __launch_bounds__(128) k_reduce_level(const Xyzz<typename C::Fp>
 #pragma unroll 1
     for (int s = (int)cnt - 1; s >= 1; s--) {
         load_xyzz(q, inS + c0 + s);
-        xyzz_add_ni(run, q);
-        xyzz_add_ni(x, run);
+        xyzz_add(run, q);
+        xyzz_add(x, run);
     }
     load_xyzz(q, inS + c0);
-    xyzz_add_ni(run, q);
+    xyzz_add(run, q);
     store_xyzz(outS + g, run);
 #pragma unroll 1
-    for (uint32_t d = 0; d < log2span; d++) xyzz_dbl_ni(x, x);
+    for (uint32_t d = 0; d < log2span; d++) xyzz_dbl(x, x);
     if (inW != nullptr) {
 #pragma unroll 1
         for (uint32_t s = 0; s < cnt; s++) {
             load_xyzz(q, inW + c0 + s);
-            xyzz_add_ni(x, q);
+            xyzz_add(x, q);
         }
     }
     store_xyzz(outW + g, x);
@@ -519,12 +579,12 @@ __global__ void k_combine(const Xyzz<typename C::Fp>* __restrict__ rootS,
     for (int w = (int)d.nwin - 1; w >= 0; w--) {
         if (w != (int)d.nwin - 1) {
 #pragma unroll 1
-            for (uint32_t b = 0; b < d.c; b++) xyzz_dbl_ni(acc, acc);
+            for (uint32_t b = 0; b < d.c; b++) xyzz_dbl(acc, acc);
         }
         load_xyzz(q, rootS + d.win_off + w);
-        xyzz_add_ni(acc, q);
+        xyzz_add(acc, q);
         load_xyzz(q, rootW + d.win_off + w);
-        xyzz_add_ni(acc, q);
+        xyzz_add(acc, q);
     }
     Affine<P> a;
     xyzz_to_affine_ni(a, acc);

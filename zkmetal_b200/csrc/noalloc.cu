@@ -59,9 +59,8 @@ constexpr size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
 // byte offsets inside the scratch array
 constexpr size_t OFF_COUNTS = 0;
 constexpr size_t OFF_CURSOR = align256(OFF_COUNTS + (NB + 1) * 4);
-constexpr size_t OFF_KEYS = align256(OFF_CURSOR + (NB + 1) * 4);
-constexpr size_t OFF_VALS = align256(OFF_KEYS + E_MAX * 4);
-constexpr size_t OFF_BUCKETS = align256(OFF_VALS + E_MAX * 4);
+constexpr size_t OFF_ENTS = align256(OFF_CURSOR + (NB + 1) * 4);
+constexpr size_t OFF_BUCKETS = align256(OFF_ENTS + E_MAX * 8);
 constexpr size_t OFF_CNT = align256(OFF_BUCKETS + NB * XS);
 constexpr size_t OFF_TILES = align256(OFF_CNT + T1_MAX * 4);
 constexpr size_t OFF_TOTALS = align256(OFF_TILES + 4096);
@@ -177,8 +176,7 @@ extern "C" ZkMetalStatus zkmsm_bn254_msm_noalloc(const void* d_points, const voi
     uint32_t* phi = reinterpret_cast<uint32_t*>(base + OFF_PHI);
     uint32_t* counts = reinterpret_cast<uint32_t*>(base + OFF_COUNTS);
     uint32_t* cursor = reinterpret_cast<uint32_t*>(base + OFF_CURSOR);
-    uint32_t* keys = reinterpret_cast<uint32_t*>(base + OFF_KEYS);
-    uint32_t* vals = reinterpret_cast<uint32_t*>(base + OFF_VALS);
+    uint2* ents = reinterpret_cast<uint2*>(base + OFF_ENTS);
     uint32_t* cnt = reinterpret_cast<uint32_t*>(base + OFF_CNT);
     uint32_t* tot = reinterpret_cast<uint32_t*>(base + OFF_TOTALS);
     Xyzz<P>* buckets = reinterpret_cast<Xyzz<P>*>(base + OFF_BUCKETS);
@@ -192,19 +190,21 @@ extern "C" ZkMetalStatus zkmsm_bn254_msm_noalloc(const void* d_points, const voi
     k_endo<C><<<(n + 255) / 256, 256, 0, s>>>(pts, n, phi);
     k_digit_hist<C><<<(n + 255) / 256, 256, 0, s>>>(sc, dd, 1, n, counts);
     scan(base, counts, NB, tot + 0, cursor, s);
-    k_digit_scatter<C><<<(n + 255) / 256, 256, 0, s>>>(sc, dd, 1, n, cursor, keys, vals);
-    const uint32_t* lk = keys;
+    k_digit_scatter<C><<<(n + 255) / 256, 256, 0, s>>>(sc, dd, 1, n, cursor, ents);
+    const uint32_t* lk = reinterpret_cast<const uint32_t*>(ents);
+    uint32_t ks = 2;
     int cur = 0;
     for (int l = 0; l < nacc; l++) {
         uint32_t Kl = accK[l], Tl = accT[l];
-        k_chunk_count<<<(Tl + 255) / 256, 256, 0, s>>>(lk, tot + l, Kl, Tl, cnt);
+        k_chunk_count<<<(Tl + 255) / 256, 256, 0, s>>>(lk, ks, tot + l, Kl, Tl, cnt);
         scan(base, cnt, Tl, tot + l + 1, nullptr, s);
         if (l == 0)
-            k_acc_l1<C><<<(Tl + 255) / 256, 256, 0, s>>>(lk, vals, tot + l, Kl, pts, phi, cnt, buckets, pk[cur],
+            k_acc_l1<C><<<(Tl + ZKMSM_ACC_THREADS - 1) / ZKMSM_ACC_THREADS, ZKMSM_ACC_THREADS, 0, s>>>(ents, tot + l, Kl, pts, phi, cnt, buckets, pk[cur],
                                                           pv[cur]);
         else
             k_acc_lj<C><<<(Tl + 255) / 256, 256, 0, s>>>(lk, pv[cur ^ 1], tot + l, Kl, cnt, buckets, pk[cur], pv[cur]);
         lk = pk[cur];
+        ks = 1;
         cur ^= 1;
     }
     const Xyzz<P>* inS = buckets;

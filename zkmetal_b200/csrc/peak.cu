@@ -41,6 +41,31 @@ __global__ void __launch_bounds__(256) k_imad_peak(uint32_t iters, uint32_t seed
     if (x == 0x12345678u) sink[0] = x;  // keep the work observable
 }
 
+// 64-bit multiply-add form of the same work: one mad.wide.u32 per product
+__global__ void __launch_bounds__(256) k_imad_wide_peak(uint32_t iters, uint32_t seed, uint32_t* sink) {
+    uint32_t a[8], b = seed ^ threadIdx.x;
+    uint64_t acc[8];
+#pragma unroll
+    for (int j = 0; j < 8; j++) {
+        a[j] = seed * (j + 3) + threadIdx.x;
+        acc[j] = j;
+    }
+#pragma unroll 1
+    for (uint32_t it = 0; it < iters; it++) {
+#pragma unroll
+        for (int r = 0; r < 8; r++) {
+#pragma unroll
+            for (int j = 0; j < 8; j++) {
+                asm volatile("mad.wide.u32 %0, %1, %2, %0;" : "+l"(acc[j]) : "r"(a[j]), "r"(b));
+            }
+        }
+    }
+    uint64_t x = 0;
+#pragma unroll
+    for (int j = 0; j < 8; j++) x ^= acc[j];
+    if (x == 0x12345678u) sink[0] = (uint32_t)x;
+}
+
 template <class P>
 __global__ void __launch_bounds__(256) k_fe_mul_peak(uint32_t iters, uint32_t* sink) {
     Fe<P> x[2], y;
@@ -114,6 +139,7 @@ static double time_kernel(void (*launch)(cudaStream_t), cudaStream_t s) {
 }
 
 static uint32_t* g_sink = nullptr;
+static double g_wide_products_per_s = 0;
 static int g_blocks = 0;
 constexpr uint32_t IMAD_ITERS = 2048;
 constexpr uint32_t FE_ITERS = 256;
@@ -130,6 +156,9 @@ extern "C" ZkMetalStatus zkmsm_measure_peaks(double* products_per_s, double* bn2
     double t = time_kernel([](cudaStream_t st) { k_imad_peak<<<g_blocks, 256, 0, st>>>(IMAD_ITERS, 7, g_sink); }, s);
     double threads = (double)g_blocks * 256;
     *products_per_s = threads * IMAD_ITERS * 64 / t;  // 64 lo+hi pairs per iteration
+    double tw = time_kernel(
+        [](cudaStream_t st) { k_imad_wide_peak<<<g_blocks, 256, 0, st>>>(IMAD_ITERS, 7, g_sink); }, s);
+    g_wide_products_per_s = threads * IMAD_ITERS * 64 / tw;
     if (bn254_mul_per_s) {
         double t2 = time_kernel(
             [](cudaStream_t st) { k_fe_mul_peak<Bn254Fp><<<g_blocks, 256, 0, st>>>(FE_ITERS, g_sink); }, s);
@@ -144,6 +173,10 @@ extern "C" ZkMetalStatus zkmsm_measure_peaks(double* products_per_s, double* bn2
     cudaStreamDestroy(s);
     return e == cudaSuccess ? ZKMETAL_SUCCESS : ZKMETAL_ERR_GPU_ERROR;
 }
+
+// products/s of the single-instruction 64-bit form (mad.wide.u32), measured
+// by the last zkmsm_measure_peaks call
+extern "C" double zkmsm_wide_products_per_s(void) { return g_wide_products_per_s; }
 
 extern "C" ZkMetalStatus zkmsm_sum_results_device(int curve, const void* d_results, uint32_t count, void* d_out,
                                                   void* stream) {

@@ -81,6 +81,7 @@ _SIGS = {
     "zkmsm_measure_peaks": (c_i32, [ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double),
                                     ctypes.POINTER(ctypes.c_double)]),
     "zkmsm_sum_results": (c_i32, [c_int, c_vp, c_u32, c_vp]),
+    "zkmsm_wide_products_per_s": (ctypes.c_double, []),
     "zkmsm_sum_results_device": (c_i32, [c_int, c_vp, c_u32, c_vp, c_vp]),
     "zkmsm_bn254_msm_noalloc": (c_i32, [c_vp, c_vp, c_int, c_u32, c_vp, c_vp]),
     "zkmsm_device_alloc": (c_vp, [c_u64]),
