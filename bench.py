@@ -163,6 +163,179 @@ def run_reference(args):
     return 0
 
 
+# --------------------------------------------------------------- batched / served configs
+def _dev(torch, nbytes):
+    return torch.empty(max(int(nbytes), 16), dtype=torch.uint8, device="cuda")
+
+
+def _pinned(torch, t):
+    h = torch.empty(t.numel(), dtype=torch.uint8, pin_memory=True)
+    h.copy_(t.cpu())
+    return h
+
+
+def run_batch_config(seed=0x5EED0002, table_log2=22, n_msms=24, lo=12, hi=22):
+    """24 BN254 commitments, sizes log-uniform in [2^12, 2^22], over prefixes
+    of one resident 2^22-point table: one batched graph launch against
+    back-to-back plain calls (drop-in API from host buffers, and device-resident)."""
+    import numpy as np
+    import torch
+    from zkmetal_b200 import CommitmentTable, MetalMSM
+    from zkmetal_b200 import lib as zl
+    L = zl.lib()
+    T = 1 << table_log2
+    e = MetalMSM()
+    pts = _dev(torch, T * 64)
+    torch.cuda.synchronize()
+    assert L.zkmsm_gen_bases(e.handle, 0, seed, 0, T, pts.data_ptr()) == 0
+    rng = np.random.default_rng(seed)
+    counts = [int(round(2 ** u)) for u in rng.uniform(lo, hi, n_msms)]
+    total = sum(counts)
+    sc = _dev(torch, total * 32)
+    assert L.zkmsm_gen_scalars(e.handle, 0, seed + 1, 0, total, 0, 1, sc.data_ptr()) == 0
+    sc_h, pts_h = _pinned(torch, sc), _pinned(torch, pts)
+    rep = ctypes.create_string_buffer(1 << 16)
+    t0 = time.perf_counter()
+    assert L.zkmsm_autotune(e.handle, 0, lo, hi, rep, len(rep)) == 0, zl.last_error()
+    tune_s = time.perf_counter() - t0
+    table = CommitmentTable(e, pts.data_ptr(), on_device=True, n=T)
+    rx, ry, rz = (ctypes.create_string_buffer(32) for _ in range(3))
+    out = ctypes.create_string_buffer(96)
+
+    def plain_dropin():
+        res, off = [], 0
+        for n in counts:
+            assert L.zkmetal_bn254_msm_fr(e.handle, pts_h.data_ptr(), sc_h.data_ptr() + off * 32, n, rx, ry, rz) == 0
+            res.append(rx.raw + ry.raw + rz.raw)
+            off += n
+        return res
+
+    def plain_device():
+        res, off = [], 0
+        for n in counts:
+            assert L.zkmsm_msm_device(e.handle, 0, pts.data_ptr(), sc.data_ptr() + off * 32, 1, n, out, None) == 0
+            res.append(out.raw)
+            off += n
+        return res
+
+    def batched():
+        r = table.batch_commit(sc_h.numpy(), counts, fmt=zl.SCALAR_MONT)
+        return [p.x + p.y + p.z for p in r]
+
+    def timed(fn, reps):
+        fn()  # warm-up (plans, graph capture)
+        best = 1e30
+        res = None
+        for _ in range(reps):
+            t = time.perf_counter()
+            res = fn()
+            best = min(best, time.perf_counter() - t)
+        return best, res
+
+    t_drop, r_drop = timed(plain_dropin, 2)
+    t_dev, r_dev = timed(plain_device, 2)
+    t_bat, r_bat = timed(batched, 3)
+    table.close()
+    e.close()
+    return {"workload": "24 BN254 MSMs, sizes 2^U (U ~ uniform[12,22]), prefixes of a 2^22 resident table",
+            "points": total, "msms": n_msms,
+            "plain_dropin_commits_per_s": round(n_msms / t_drop, 1),
+            "plain_device_commits_per_s": round(n_msms / t_dev, 1),
+            "batched_commits_per_s": round(n_msms / t_bat, 1),
+            "speedup_vs_plain_dropin": round(t_drop / t_bat, 2),
+            "speedup_vs_plain_device": round(t_dev / t_bat, 2),
+            "batched_ms": round(t_bat * 1e3, 2),
+            "bit_exact_vs_plain": r_bat == r_dev == r_drop,
+            "autotune_s": round(tune_s, 1),
+            "autotune": json.loads(rep.value.decode())}
+
+
+def run_serve_config(duration_s=60.0, rate=200.0, seed=0x5EED0004, table_log2=22, plain_sample=120):
+    """Poisson stream of commitment requests (70% BN254 / 30% BLS12-381, sizes
+    log-uniform in [2^10, 2^22], scalars half uniform / half witness-like) to
+    the continuous-batching server; p50/p99 latency and commitments/s against
+    back-to-back plain calls of the same requests."""
+    import threading
+    import numpy as np
+    import torch
+    from zkmetal_b200 import BLS12381MSM, CommitmentServer, CommitmentTable, MetalMSM
+    from zkmetal_b200 import lib as zl
+    L = zl.lib()
+    T = 1 << table_log2
+    engines = {0: MetalMSM(), 1: BLS12381MSM()}
+    fb = {0: 32, 1: 48}
+    pts, pts_h, tables, pools = {}, {}, {}, {}
+    for c in (0, 1):
+        pts[c] = _dev(torch, T * 2 * fb[c])
+        torch.cuda.synchronize()
+        assert L.zkmsm_gen_bases(engines[c].handle, c, seed + c, 0, T, pts[c].data_ptr()) == 0
+        pts_h[c] = _pinned(torch, pts[c])
+        tables[c] = CommitmentTable(engines[c], pts[c].data_ptr(), on_device=True, n=T)
+        for dist in (0, 1):
+            s = _dev(torch, 2 * T * 32)
+            assert L.zkmsm_gen_scalars(engines[c].handle, c, seed + 10 + 2 * c + dist, 0, 2 * T, dist, 1,
+                                       s.data_ptr()) == 0
+            pools[(c, dist)] = _pinned(torch, s).numpy()
+    rng = np.random.default_rng(seed)
+    reqs, t = [], 0.0
+    while True:
+        t += rng.exponential(1.0 / rate)
+        if t > duration_s:
+            break
+        c = 0 if rng.random() < 0.7 else 1
+        n = int(round(2 ** rng.uniform(10, 22)))
+        dist = int(rng.random() < 0.5)
+        off = int(rng.integers(0, T))
+        reqs.append((t, c, n, dist, off))
+    srv = CommitmentServer(tables[0], tables[1], workers=3)
+    ids = [None] * len(reqs)
+    start = time.perf_counter()
+
+    def submitter():
+        for i, (ta, c, n, dist, off) in enumerate(reqs):
+            d = start + ta - time.perf_counter()
+            if d > 0:
+                time.sleep(d)
+            view = pools[(c, dist)][off * 32:(off + n) * 32]
+            ids[i] = srv.submit(c, view, zl.SCALAR_MONT)
+
+    th = threading.Thread(target=submitter)
+    th.start()
+    served = []
+    for i in range(len(reqs)):
+        while ids[i] is None:
+            time.sleep(0.0005)
+        p, _lat = srv.wait(ids[i])
+        served.append(p.x + p.y + p.z)
+    th.join()
+    wall = time.perf_counter() - start
+    st = srv.stats()
+    srv.close()
+    # back-to-back plain drop-in calls on the first requests of the same stream
+    k = min(plain_sample, len(reqs))
+    rx, ry, rz = (ctypes.create_string_buffer(48) for _ in range(3))
+    fns = {0: L.zkmetal_bn254_msm_fr, 1: L.zkmetal_bls12_381_g1_msm_fr}
+    plain = []
+    for (ta, c, n, dist, off) in reqs[:2]:  # warm-up
+        fns[c](engines[c].handle, pts_h[c].data_ptr(), pools[(c, dist)].ctypes.data + off * 32, n, rx, ry, rz)
+    t0 = time.perf_counter()
+    for (ta, c, n, dist, off) in reqs[:k]:
+        assert fns[c](engines[c].handle, pts_h[c].data_ptr(), pools[(c, dist)].ctypes.data + off * 32, n,
+                      rx, ry, rz) == 0
+        plain.append(rx.raw[:fb[c]] + ry.raw[:fb[c]] + rz.raw[:fb[c]])
+    t_plain = time.perf_counter() - t0
+    for tb in tables.values():
+        tb.close()
+    return {"workload": "Poisson %.0f req/s for %.0f s, 70%% BN254 / 30%% BLS12-381, sizes 2^U (U ~ [10,22]), "
+                        "scalars 50/50 uniform / witness-like, 2^22-point resident tables" % (rate, duration_s),
+            "requests": len(reqs), "completed": st["completed"], "failed": st["failed"], "batches": st["batches"],
+            "max_batch": st["max_batch"], "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"],
+            "served_commits_per_s": round(st["completed"] / wall, 1),
+            "plain_dropin_commits_per_s": round(k / t_plain, 1),
+            "speedup_vs_plain_dropin": round((st["completed"] / wall) / (k / t_plain), 2),
+            "bit_exact_vs_plain": served[:k] == plain}
+
+
 # --------------------------------------------------------------- GPU arm
 def run_ours(args):
     import torch
@@ -332,6 +505,15 @@ def run_ours(args):
             "value": round(cms * scale, 1), "unit": "ms", "cores": threads, "kind": kind,
             "sample": "one %d-point BN254 MSM (first shard of the same inputs), reference C Pippenger, "
                       "%d OpenMP threads, time x%g to 2^%d" % (n_sample, threads, scale, args.log2n)}
+    if world == 1 and not args.no_extras:
+        try:
+            line["batch"] = run_batch_config()
+        except Exception as exc:  # reported, not hidden
+            line["batch"] = {"error": repr(exc)}
+        try:
+            line["serve"] = run_serve_config(duration_s=args.serve_seconds, plain_sample=40)
+        except Exception as exc:
+            line["serve"] = {"error": repr(exc)}
     print(json.dumps(line), flush=True)
     if world > 1:
         dist.barrier()
@@ -354,9 +536,21 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true", help="skip the batched and served summaries")
+    ap.add_argument("--serve-seconds", type=float, default=5.0, help="arrival window of the served summary")
+    ap.add_argument("--mode", choices=["plain", "batch", "serve"], default="plain",
+                    help="batch / serve: print only that configuration's line (serve runs 60 s of arrivals)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
+    if args.mode == "batch":
+        print(json.dumps({"metric": "BN254 batched commitments/s (24 MSMs, 2^12..2^22, 2^22 table)",
+                          **run_batch_config()}), flush=True)
+        return 0
+    if args.mode == "serve":
+        print(json.dumps({"metric": "served commitments/s and p50/p99 latency (Poisson 200 req/s)",
+                          **run_serve_config(duration_s=60.0)}), flush=True)
+        return 0
     return run_ours(args)
 
 

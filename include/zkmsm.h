@@ -164,6 +164,46 @@ ZkMetalStatus zkmsm_batch_commit(ZkMetalMSMEngine engine, ZkMsmTable table, cons
                                  int scalars_on_device, int scalar_fmt, const uint32_t* counts, uint32_t n_msms,
                                  uint8_t* results);
 
+/* Autotuner: times the MSM at window widths around the cost model's choice
+ * for every power-of-two size 2^min_log2n .. 2^max_log2n on synthetic
+ * inputs and keeps the fastest per size; later plans of this engine use the
+ * table (MSMs matched to the nearest power of two).  A JSON summary of the
+ * timings is written to `report` (may be NULL).  Replaces the reference's
+ * device tuning (Sources/zkMetal/Tuning.swift:9-127). */
+ZkMetalStatus zkmsm_autotune(ZkMetalMSMEngine engine, int curve, int min_log2n, int max_log2n, char* report,
+                             uint64_t report_len);
+/* Persist / restore the autotuned table (text file). */
+ZkMetalStatus zkmsm_tuning_save(ZkMetalMSMEngine engine, const char* path);
+ZkMetalStatus zkmsm_tuning_load(ZkMetalMSMEngine engine, const char* path);
+
+/* ---- commitment server (continuous batching) ----------------------------
+ * NEW.  Requests are MSMs over a prefix of a resident table; `workers`
+ * threads each own an engine (own stream and resident scratch).  A free
+ * worker batches, in arrival order, the pending requests of the oldest
+ * request's curve that fit `max_batch_points` (0 = 2^24) and the HBM budget
+ * (`hbm_budget_bytes`, 0 = 70% of free device memory), so requests arriving
+ * while others run join the next batch and batches of different workers
+ * overlap on the GPU.  The caller keeps `scalars` valid until the request
+ * completes.  Latency is measured from submit to completion. */
+typedef void* ZkMsmServer;
+ZkMetalStatus zkmsm_server_create(ZkMsmTable bn254_table, ZkMsmTable bls12_381_table, uint64_t hbm_budget_bytes,
+                                  int workers, uint64_t max_batch_points, ZkMsmServer* out);
+/* ZKMETAL_ERR_BUSY if the request alone exceeds the budget or the server stops */
+ZkMetalStatus zkmsm_server_submit(ZkMsmServer server, int curve, const void* scalars, int scalar_fmt,
+                                  uint32_t n_points, uint64_t* request_id);
+/* Remove a request that has not started (ZKMETAL_ERR_BUSY if it has). */
+ZkMetalStatus zkmsm_server_cancel(ZkMsmServer server, uint64_t request_id);
+/* Wait up to timeout_ms (< 0: forever) for a request; returns its status
+ * (ZKMETAL_ERR_BUSY on timeout or when it was cancelled), writes the result
+ * (3 field elements) and the submit-to-completion latency. */
+ZkMetalStatus zkmsm_server_wait(ZkMsmServer server, uint64_t request_id, int timeout_ms, uint8_t* result,
+                                double* latency_ms);
+/* JSON counters: completed, failed, batches, p50/p99 latency, memory in use. */
+ZkMetalStatus zkmsm_server_stats(ZkMsmServer server, char* buf, uint64_t buflen);
+/* Test hook: make the next `batches` batches fail on the host before any GPU work. */
+ZkMetalStatus zkmsm_server_inject_failures(ZkMsmServer server, int batches);
+void zkmsm_server_destroy(ZkMsmServer server);
+
 /* Tuning overrides (0 = automatic): window bits, chunk length, GLV on/off. */
 ZkMetalStatus zkmsm_engine_set_tuning(ZkMetalMSMEngine engine, int window_bits, int chunk, int glv);
 

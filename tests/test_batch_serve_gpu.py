@@ -1,0 +1,156 @@
+"""Batched commitments, autotuner and the commitment server (GPU).
+
+Every batched or served result must equal, bit for bit, the plain single
+MSM of the same scalars over the same table prefix.  The server's failure
+paths are exercised on the host only (admission refusal, cancellation,
+injected batch failures): nothing here faults or stalls the GPU.
+"""
+import ctypes
+import json
+import random
+
+import numpy as np
+import pytest
+import torch
+
+from oracle import pyref as R
+from tests.gpu_helpers import check, gen_inputs, jac_to_affine_bytes, msm_device, oracle_msm, to_host
+from zkmetal_b200 import BLS12381MSM, CommitmentServer, CommitmentTable, MetalMSM, MSMError
+from zkmetal_b200 import lib as zl
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def eng():
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    return {"bn254": MetalMSM(), "bls12_381": BLS12381MSM()}
+
+
+@pytest.fixture(scope="module")
+def tables(eng):
+    out = {}
+    for curve, T in (("bn254", 1 << 15), ("bls12_381", 1 << 13)):
+        p, _ = gen_inputs(eng[curve], curve, 301, T, "uniform", zl.SCALAR_MONT)
+        out[curve] = (CommitmentTable(eng[curve], p.data_ptr(), on_device=True, n=T), p)
+    yield out
+    for t, _ in out.values():
+        t.close()
+
+
+def scalars_host(eng, curve, seed, n, dist):
+    _, s = gen_inputs(eng, curve, seed, n, dist, zl.SCALAR_MONT)
+    return np.frombuffer(to_host(s), dtype=np.uint8).copy()
+
+
+def plain(eng, curve, table_points, scal_np, n):
+    s = torch.from_numpy(scal_np[: n * 32].copy()).cuda()
+    return msm_device(eng, curve, table_points, s, zl.SCALAR_MONT, n)
+
+
+def test_batch_graph_replay_and_launch_count(eng, tables):
+    e = eng["bn254"]
+    table, pts = tables["bn254"]
+    counts = [4096, 100, 1 << 15, 1, 777]
+    sc = scalars_host(e, "bn254", 310, sum(counts), "witness")
+    L = zl.lib()
+    r1 = table.batch_commit(sc, counts, fmt=zl.SCALAR_MONT)
+    l0 = L.zkmsm_engine_launch_count(e.handle)
+    r2 = table.batch_commit(sc, counts, fmt=zl.SCALAR_MONT)  # replayed graph
+    assert L.zkmsm_engine_launch_count(e.handle) > l0
+    off = 0
+    for i, c in enumerate(counts):
+        a = r1[i].x + r1[i].y + r1[i].z
+        assert a == r2[i].x + r2[i].y + r2[i].z
+        assert a == plain(e, "bn254", pts, sc[off * 32:], c)
+        off += c
+
+
+def test_autotune_keeps_results_and_persists(eng, oracles, tmp_path):
+    ref, cm = oracles
+    orc = ref if ref is not None else cm
+    e = MetalMSM()
+    L = zl.lib()
+    buf = ctypes.create_string_buffer(1 << 16)
+    check(L.zkmsm_autotune(e.handle, zl.BN254, 10, 13, buf, len(buf)))
+    rep = json.loads(buf.value.decode())
+    assert set(rep) == {"10", "11", "12", "13"}
+    for v in rep.values():
+        assert str(v["best"]) in v["ms"]
+    n = 3000
+    p, s = gen_inputs(e, "bn254", 320, n, "uniform", zl.SCALAR_MONT)
+    got = jac_to_affine_bytes(R.BN254, msm_device(e, "bn254", p, s, zl.SCALAR_MONT, n))
+    assert got == oracle_msm(orc, "bn254", to_host(p), to_host(s), n, zl.SCALAR_MONT)
+    path = str(tmp_path / "tuning.txt")
+    check(L.zkmsm_tuning_save(e.handle, path.encode()))
+    e2 = MetalMSM()
+    check(L.zkmsm_tuning_load(e2.handle, path.encode()))
+    assert msm_device(e2, "bn254", p, s, zl.SCALAR_MONT, n) == msm_device(e, "bn254", p, s, zl.SCALAR_MONT, n)
+    with open(path) as f:
+        assert f.readline().startswith("zkmsm-tuning")
+    e.close()
+    e2.close()
+
+
+def test_server_same_result_alone_and_in_the_mix(eng, tables):
+    srv = CommitmentServer(tables["bn254"][0], tables["bls12_381"][0], workers=2)
+    try:
+        rng = random.Random(5)
+        pool = {c: scalars_host(eng[c], c, 330 + i, tables[c][0].n, "uniform" if i else "witness")
+                for i, c in enumerate(("bn254", "bls12_381"))}
+        cid = {"bn254": zl.BN254, "bls12_381": zl.BLS12_381}
+        probe = ("bn254", 5000)
+        rid = srv.submit(cid["bn254"], pool["bn254"][: probe[1] * 32], zl.SCALAR_MONT)
+        alone, lat = srv.wait(rid)
+        assert lat > 0
+        reqs = []
+        for k in range(40):
+            curve = "bn254" if rng.random() < 0.7 else "bls12_381"
+            n = int(2 ** rng.uniform(4, np.log2(tables[curve][0].n)))
+            reqs.append((curve, n))
+            if k == 17:
+                reqs.append(probe)
+        ids = [srv.submit(cid[c], pool[c][: n * 32], zl.SCALAR_MONT) for c, n in reqs]
+        res = [srv.wait(i)[0] for i in ids]
+        for (c, n), r in zip(reqs, res):
+            want = plain(eng[c], c, tables[c][1], pool[c], n)
+            assert r.x + r.y + r.z == want, (c, n)
+        k = reqs.index(probe)
+        assert res[k].x + res[k].y + res[k].z == alone.x + alone.y + alone.z
+        st = srv.stats()
+        assert st["completed"] >= 42 and st["failed"] == 0 and st["p99_ms"] >= st["p50_ms"] > 0
+    finally:
+        srv.close()
+
+
+def test_server_admission_cancel_and_injected_failure(eng, tables):
+    t = tables["bn254"][0]
+    pool = scalars_host(eng["bn254"], "bn254", 340, t.n, "uniform")
+    small = CommitmentServer(t, None, hbm_budget_bytes=32 << 20, workers=1)
+    try:
+        with pytest.raises(MSMError):
+            small.submit(zl.BN254, pool[: t.n * 32], zl.SCALAR_MONT)  # needs more than the budget
+    finally:
+        small.close()
+    srv = CommitmentServer(t, None, workers=1, max_batch_points=1 << 12)
+    try:
+        srv.inject_failures(1)
+        first = srv.submit(zl.BN254, pool[: 2000 * 32], zl.SCALAR_MONT)
+        with pytest.raises(MSMError):
+            srv.wait(first)
+        ids = [srv.submit(zl.BN254, pool[: 3000 * 32], zl.SCALAR_MONT) for _ in range(12)]
+        cancelled = ids[-1]
+        st = srv.cancel(cancelled)
+        assert st in (zl.SUCCESS, zl.ERR_BUSY)  # BUSY if it had already started
+        for i in ids[:-1]:
+            r, _ = srv.wait(i)
+            assert r.x + r.y + r.z == plain(eng["bn254"], "bn254", tables["bn254"][1], pool, 3000)
+        if st == zl.SUCCESS:
+            with pytest.raises(MSMError):
+                srv.wait(cancelled)
+        else:
+            srv.wait(cancelled)
+        assert srv.stats()["failed"] == 1
+    finally:
+        srv.close()

@@ -131,12 +131,96 @@ struct Table {
     DevBuf points, phi;
 };
 
+// read-only view of a table for the commitment server (server.cu)
+struct TableView {
+    int curve;
+    uint64_t n;
+    const uint32_t* points;
+    const uint32_t* phi;
+};
+bool table_view(ZkMsmTable t, TableView* out) {
+    if (!t || !out) return false;
+    Table* tb = static_cast<Table*>(t);
+    out->curve = tb->curve;
+    out->n = tb->n;
+    out->points = tb->points.as<uint32_t>();
+    out->phi = tb->phi.as<uint32_t>();
+    return true;
+}
+
 // lazily created shared engine for the _auto entry points (zkMetal_ffi.swift:22-35)
 static std::mutex g_auto_mu;
 static Engine* g_auto = nullptr;
 static Engine& auto_engine() {
     if (!g_auto) g_auto = new Engine();
     return *g_auto;
+}
+
+// Autotuner: for each power-of-two size in [min_l2, max_l2], time the MSM at
+// window widths around the cost model's choice on synthetic inputs (the
+// library's generator) and keep the fastest.  The table feeds every later
+// plan of this engine (MSMs are matched to the nearest power of two).
+template <class C>
+static std::string autotune(Engine& e, int min_l2, int max_l2) {
+    using P = typename C::Fp;
+    const size_t fb = P::N * 4;
+    const uint64_t nmax = 1ull << max_l2;
+    DevBuf pts, phi, sc, res;
+    pts.ensure(nmax * 2 * fb);
+    phi.ensure(nmax * 2 * fb);
+    sc.ensure(nmax * 32);
+    res.ensure(3 * fb + 16);
+    e.gen_bases<C>(0xA070u, 0, nmax, pts.as<uint32_t>());
+    e.gen_scalars<C>(0xA070u, 0, nmax, 0, ZKMSM_SCALAR_MONT, sc.as<uint32_t>());
+    e.make_phi<C>(pts.as<uint32_t>(), nmax, phi.as<uint32_t>());
+    cudaEvent_t a, b;
+    ZK_CUDA(cudaEventCreate(&a));
+    ZK_CUDA(cudaEventCreate(&b));
+    const int saved_w = e.tuning.window_bits;
+    const bool saved_prof = e.profile;
+    e.profile = false;
+    std::string rep = "{";
+    for (int l2 = min_l2; l2 <= max_l2; l2++) {
+        uint32_t n = 1u << l2;
+        e.tuning.window_bits = 0;
+        e.tuning.window_table.erase({CurveTraits<C>::id * 2 + 1, l2});
+        e.tuning.version++;
+        int c0 = (int)e.get_plan<C>({n}, {0}, ZKMSM_SCALAR_MONT).descs[0].c;
+        int best_c = c0;
+        float best = 1e30f;
+        std::string row;
+        for (int c = std::max(4, c0 - 2); c <= std::min(22, c0 + 2); c++) {
+            e.tuning.window_bits = c;
+            Plan& pl = e.get_plan<C>({n}, {0}, ZKMSM_SCALAR_MONT);
+            e.ensure_workspace<C>(pl);
+            e.enqueue<C>(pl, pts.as<uint32_t>(), phi.as<uint32_t>(), sc.as<uint32_t>(), res.as<uint32_t>());
+            ZK_CUDA(cudaEventRecord(a, e.stream));
+            const int reps = l2 >= 20 ? 2 : 4;
+            for (int r = 0; r < reps; r++)
+                e.enqueue<C>(pl, pts.as<uint32_t>(), phi.as<uint32_t>(), sc.as<uint32_t>(), res.as<uint32_t>());
+            ZK_CUDA(cudaEventRecord(b, e.stream));
+            ZK_CUDA(cudaEventSynchronize(b));
+            float ms = 0;
+            ZK_CUDA(cudaEventElapsedTime(&ms, a, b));
+            ms /= reps;
+            row += (row.empty() ? "" : ",") + std::string("\"") + std::to_string(c) + "\":" + std::to_string(ms);
+            if (ms < best) {
+                best = ms;
+                best_c = c;
+            }
+        }
+        e.tuning.window_table[{CurveTraits<C>::id * 2 + 1, l2}] = best_c;
+        rep += (l2 == min_l2 ? "" : ",") + std::string("\"") + std::to_string(l2) + "\":{\"best\":" +
+               std::to_string(best_c) + ",\"model\":" + std::to_string(c0) + ",\"ms\":{" + row + "}}";
+    }
+    rep += "}";
+    e.tuning.window_bits = saved_w;
+    e.tuning.version++;
+    e.profile = saved_prof;
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    ZK_CUDA(cudaStreamSynchronize(e.stream));
+    return rep;
 }
 
 }  // namespace zkmsm
@@ -366,10 +450,10 @@ ZkMetalStatus zkmsm_batch_commit(ZkMetalMSMEngine engine, ZkMsmTable table, cons
         std::vector<uint8_t> out((size_t)n_msms * 3 * fb);
         if (t.curve == ZKMSM_BN254) {
             Plan& pl = e.get_plan<Bn254>(cnt, boff, fmt);
-            e.run_device<Bn254>(pl, t.points.as<uint32_t>(), t.phi.as<uint32_t>(), sc, out.data());
+            e.run_device_graph<Bn254>(pl, t.points.as<uint32_t>(), t.phi.as<uint32_t>(), sc, out.data());
         } else {
             Plan& pl = e.get_plan<Bls381>(cnt, boff, fmt);
-            e.run_device<Bls381>(pl, t.points.as<uint32_t>(), t.phi.as<uint32_t>(), sc, out.data());
+            e.run_device_graph<Bls381>(pl, t.points.as<uint32_t>(), t.phi.as<uint32_t>(), sc, out.data());
         }
         for (uint32_t m = 0; m < n_msms; m++) {
             uint8_t* dst = results + (size_t)m * 3 * fb;
@@ -380,6 +464,59 @@ ZkMetalStatus zkmsm_batch_commit(ZkMetalMSMEngine engine, ZkMsmTable table, cons
     });
 }
 
+ZkMetalStatus zkmsm_autotune(ZkMetalMSMEngine engine, int curve, int min_log2n, int max_log2n, char* report,
+                             uint64_t report_len) {
+    if (!engine || min_log2n < 4 || max_log2n > 26 || min_log2n > max_log2n) return ZKMETAL_ERR_INVALID_INPUT;
+    if (curve != ZKMSM_BN254 && curve != ZKMSM_BLS12_381) return ZKMETAL_ERR_INVALID_INPUT;
+    return guarded([&] {
+        std::string r = curve == ZKMSM_BN254 ? autotune<Bn254>(ENG(engine), min_log2n, max_log2n)
+                                             : autotune<Bls381>(ENG(engine), min_log2n, max_log2n);
+        if (report && report_len) {
+            size_t k = std::min<size_t>(r.size(), report_len - 1);
+            memcpy(report, r.data(), k);
+            report[k] = 0;
+        }
+        return ZKMETAL_SUCCESS;
+    });
+}
+
+ZkMetalStatus zkmsm_tuning_save(ZkMetalMSMEngine engine, const char* path) {
+    if (!engine || !path) return ZKMETAL_ERR_INVALID_INPUT;
+    FILE* f = fopen(path, "w");
+    if (!f) {
+        set_error(std::string("cannot write ") + path);
+        return ZKMETAL_ERR_INVALID_INPUT;
+    }
+    fprintf(f, "zkmsm-tuning 1\n");
+    for (auto& kv : ENG(engine).tuning.window_table)
+        fprintf(f, "%d %d %d\n", kv.first.first, kv.first.second, kv.second);
+    fclose(f);
+    return ZKMETAL_SUCCESS;
+}
+
+ZkMetalStatus zkmsm_tuning_load(ZkMetalMSMEngine engine, const char* path) {
+    if (!engine || !path) return ZKMETAL_ERR_INVALID_INPUT;
+    FILE* f = fopen(path, "r");
+    if (!f) {
+        set_error(std::string("cannot read ") + path);
+        return ZKMETAL_ERR_INVALID_INPUT;
+    }
+    char head[32] = {0};
+    int ver = 0;
+    if (fscanf(f, "%31s %d", head, &ver) != 2 || std::string(head) != "zkmsm-tuning" || ver != 1) {
+        fclose(f);
+        set_error("not a zkmsm tuning file");
+        return ZKMETAL_ERR_INVALID_INPUT;
+    }
+    Engine& e = ENG(engine);
+    int k, l2, c;
+    while (fscanf(f, "%d %d %d", &k, &l2, &c) == 3)
+        if (k >= 0 && k < 4 && l2 >= 0 && l2 < 40 && c >= 2 && c <= 24) e.tuning.window_table[{k, l2}] = c;
+    fclose(f);
+    e.tuning.version++;
+    return ZKMETAL_SUCCESS;
+}
+
 ZkMetalStatus zkmsm_engine_set_tuning(ZkMetalMSMEngine engine, int window_bits, int chunk, int glv) {
     if (!engine || window_bits < 0 || window_bits > 24 || window_bits == 1 || chunk < 0 || chunk > 4096)
         return ZKMETAL_ERR_INVALID_INPUT;
@@ -387,6 +524,7 @@ ZkMetalStatus zkmsm_engine_set_tuning(ZkMetalMSMEngine engine, int window_bits, 
     e.tuning.window_bits = window_bits;
     e.tuning.chunk = chunk;
     e.tuning.glv = glv < 0 ? -1 : (glv ? 1 : 0);
+    e.tuning.version++;
     return ZKMETAL_SUCCESS;
 }
 

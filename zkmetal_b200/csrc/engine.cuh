@@ -40,14 +40,15 @@ struct CudaError {
 struct DevBuf {
     void* p = nullptr;
     size_t cap = 0;
-    void ensure(size_t bytes) {
-        if (bytes <= cap) return;
+    bool ensure(size_t bytes) {  // true when it had to reallocate
+        if (bytes <= cap) return false;
         if (p) cudaFree(p);
         p = nullptr;
         cap = 0;
         size_t want = bytes + bytes / 8 + 256;
         ZK_CUDA(cudaMalloc(&p, want));
         cap = want;
+        return true;
     }
     template <class T>
     T* as() const { return static_cast<T*>(p); }
@@ -63,9 +64,13 @@ struct DevBuf {
 };
 
 struct Tuning {
-    int window_bits = 0;  // 0: cost model
+    int window_bits = 0;  // 0: autotuned table if present, else cost model
     int chunk = 0;        // level-1 chunk length, 0: automatic
     int glv = -1;         // -1: automatic (on), 0 off, 1 on
+    // autotuned window width per (curve*2 + glv, nearest log2 n); filled by
+    // zkmsm_autotune or zkmsm_tuning_load
+    std::map<std::pair<int, int>, int> window_table;
+    uint64_t version = 0;  // bumped whenever the table changes
 };
 
 // Host description of one batch run.
@@ -87,6 +92,14 @@ struct Plan {
     DevBuf d_descs, d_tasks;
     std::vector<size_t> task_level_off;
 };
+
+// Nearest power-of-two exponent of n (n >= 1).
+inline int nearest_log2(uint64_t n) {
+    int l2 = 0;
+    while ((1ull << (l2 + 1)) <= n) l2++;
+    if (n - (1ull << l2) > (1ull << l2) / 2) l2++;
+    return l2;
+}
 
 // Signed windows a half-scalar of `bits` bits needs at width c.
 inline uint32_t windows_for(uint32_t bits, uint32_t c) { return (bits + 1 + c - 1) / c; }
@@ -182,6 +195,7 @@ class Engine {
         ZK_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
     }
     ~Engine() {
+        drop_graphs();
         if (stream) cudaStreamDestroy(stream);
         if (h_results) cudaFreeHost(h_results);
     }
@@ -212,6 +226,10 @@ class Engine {
             uint32_t bits = small ? scalar_bits : (d.glv ? CurveTraits<C>::half_bits : CurveTraits<C>::fr_bits);
             uint64_t epw = (uint64_t)d.n * (d.glv ? 2 : 1);
             uint32_t c = tuning.window_bits > 0 ? (uint32_t)tuning.window_bits : choose_window(epw, bits);
+            if (tuning.window_bits == 0 && d.n && !small) {
+                auto it = tuning.window_table.find({CurveTraits<C>::id * 2 + (int)d.glv, nearest_log2(d.n)});
+                if (it != tuning.window_table.end()) c = (uint32_t)it->second;
+            }
             if (c > bits + 1) c = bits + 1 < 2 ? 2 : bits + 1;
             if (c < 2) c = 2;
             d.c = c;
@@ -303,11 +321,15 @@ class Engine {
         put(scalar_bits);
         put((uint64_t)(uint32_t)tuning.window_bits << 32 | (uint32_t)tuning.chunk);
         put((uint64_t)(int64_t)tuning.glv);
+        put(tuning.version);
         for (auto c : counts) put(c);
         for (auto b : base_offs) put(b);
         auto it = plan_cache.find(key);
         if (it != plan_cache.end()) return *it->second;
-        if (plan_cache.size() >= 256) plan_cache.clear();  // cudaFree in ~DevBuf waits for the device
+        if (plan_cache.size() >= 256) {  // cudaFree in ~DevBuf waits for the device
+            drop_graphs();                 // graphs are keyed by plan address
+            plan_cache.clear();
+        }
         std::unique_ptr<Plan> pl(new Plan());
         make_plan<C>(*pl, counts, base_offs, fmt, scalar_bits);
         std::vector<RedTask> blob;
@@ -329,26 +351,44 @@ class Engine {
     void ensure_workspace(const Plan& pl) {
         using P = typename C::Fp;
         const size_t xs = sizeof(Xyzz<P>);
-        w_counts.ensure(((size_t)pl.nbuckets + 1) * 4);
-        w_cursor.ensure(((size_t)pl.nbuckets + 1) * 4);
-        w_ents.ensure(pl.entry_bound * 8 + 16);
-        w_buckets.ensure((size_t)pl.nbuckets * xs + xs);
+        bool grew = false;
+        grew |= w_counts.ensure(((size_t)pl.nbuckets + 1) * 4);
+        grew |= w_cursor.ensure(((size_t)pl.nbuckets + 1) * 4);
+        grew |= w_ents.ensure(pl.entry_bound * 8 + 16);
+        grew |= w_buckets.ensure((size_t)pl.nbuckets * xs + xs);
         uint64_t tmax = 1, m2 = 1, m3 = 1;
         for (size_t l = 0; l < pl.acc_T.size(); l++) tmax = std::max<uint64_t>(tmax, pl.acc_T[l]);
         if (pl.acc_Mbound.size() > 1) m2 = pl.acc_Mbound[1];
         for (size_t l = 2; l < pl.acc_Mbound.size(); l++) m3 = std::max<uint64_t>(m3, pl.acc_Mbound[l]);
-        w_cnt.ensure(tmax * 4 + 16);
-        w_pkeys[0].ensure(m2 * 4 + 16);
-        w_pvals[0].ensure(m2 * xs + xs);
-        w_pkeys[1].ensure(m3 * 4 + 16);
-        w_pvals[1].ensure(m3 * xs + xs);
-        w_totals.ensure(64 * 4);
+        grew |= w_cnt.ensure(tmax * 4 + 16);
+        grew |= w_pkeys[0].ensure(m2 * 4 + 16);
+        grew |= w_pvals[0].ensure(m2 * xs + xs);
+        grew |= w_pkeys[1].ensure(m3 * 4 + 16);
+        grew |= w_pvals[1].ensure(m3 * xs + xs);
+        grew |= w_totals.ensure(64 * 4);
         size_t r0 = pl.red_nout.empty() ? 1 : pl.red_nout[0];
         for (int i = 0; i < 2; i++) {
-            w_redS[i].ensure(r0 * xs + xs);
-            w_redW[i].ensure(r0 * xs + xs);
+            grew |= w_redS[i].ensure(r0 * xs + xs);
+            grew |= w_redW[i].ensure(r0 * xs + xs);
         }
-        w_results.ensure((pl.descs.size() + 1) * 3 * P::N * 4);
+        grew |= w_results.ensure((pl.descs.size() + 1) * 3 * P::N * 4);
+        // scan tile sums for the longest scanned array (no allocation inside enqueue)
+        grew |= w_tiles.ensure(((std::max<uint64_t>(pl.nbuckets, tmax) + 2047) / 2048 + 2) * 4);
+        if (grew) drop_graphs();  // captured graphs hold the old addresses
+    }
+
+    // ------------------------------------------------------------ graphs
+    // A batch shape that repeats is captured once into a CUDA graph and then
+    // replayed with one launch.  Graphs are keyed by plan and buffer
+    // addresses and dropped whenever the workspace is reallocated.
+    struct GraphEntry {
+        cudaGraphExec_t exec = nullptr;
+        uint64_t kernels = 0;
+    };
+    std::map<std::string, GraphEntry> graphs;
+    void drop_graphs() {
+        for (auto& kv : graphs) cudaGraphExecDestroy(kv.second.exec);
+        graphs.clear();
     }
 
     // Curve-specific device work: defined in engine_impl.cuh and instantiated
@@ -362,6 +402,52 @@ class Engine {
     void gen_bases(uint64_t seed, uint64_t index0, uint64_t n, uint32_t* d_out);
     template <class C>
     void gen_scalars(uint64_t seed, uint64_t index0, uint64_t n, int dist, int fmt, uint32_t* d_out);
+
+    // Same as run_device, through a cached CUDA graph of the whole pipeline.
+    template <class C>
+    void run_device_graph(const Plan& pl, const uint32_t* d_bases, const uint32_t* d_phi,
+                          const uint32_t* d_scalars, uint8_t* out) {
+        using P = typename C::Fp;
+        ensure_workspace<C>(pl);
+        std::string key;
+        auto put = [&](const void* v) { key.append(reinterpret_cast<const char*>(&v), sizeof v); };
+        put(&pl);
+        put(d_bases);
+        put(d_phi);
+        put(d_scalars);
+        put(stream);
+        auto it = graphs.find(key);
+        if (it == graphs.end()) {
+            if (graphs.size() >= 64) drop_graphs();
+            bool prof = profile;
+            profile = false;
+            uint64_t l0 = launches;
+            cudaGraph_t g = nullptr;
+            ZK_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+            try {
+                enqueue<C>(pl, d_bases, d_phi, d_scalars, w_results.as<uint32_t>());
+            } catch (...) {
+                cudaStreamEndCapture(stream, &g);
+                if (g) cudaGraphDestroy(g);
+                profile = prof;
+                throw;
+            }
+            ZK_CUDA(cudaStreamEndCapture(stream, &g));
+            profile = prof;
+            GraphEntry ge;
+            ge.kernels = launches - l0;
+            launches = l0;
+            cudaError_t ie = cudaGraphInstantiate(&ge.exec, g, 0);
+            cudaGraphDestroy(g);
+            ZK_CUDA(ie);
+            it = graphs.emplace(key, ge).first;
+        }
+        ZK_CUDA(cudaGraphLaunch(it->second.exec, stream));
+        launches += it->second.kernels;
+        size_t bytes = pl.descs.size() * 3 * P::N * 4;
+        ZK_CUDA(cudaMemcpyAsync(out, w_results.p, bytes, cudaMemcpyDeviceToHost, stream));
+        ZK_CUDA(cudaStreamSynchronize(stream));
+    }
 
     // Full MSM batch from device inputs: results copied to host `out`
     // (n_msms x 3 x fp_bytes).

@@ -1,0 +1,345 @@
+// Commitment server: continuous batching of MSM requests over resident base
+// tables (one per curve).
+//
+// The reference has no concurrent or persistent batching: its "async" batch
+// runs MSMs one after another (Sources/zkMetal/MSM/MultiMSM.swift:175-238).
+// Here a request (curve, n scalars over a prefix of that curve's table) is
+// queued by zkmsm_server_submit.  W worker threads each own an Engine (its
+// own CUDA stream and resident scratch).  A free worker takes the oldest
+// pending request's curve and admits, in arrival order, every pending
+// request of that curve that fits the batch limits and the HBM budget, runs
+// them as one batch, and hands the results back.  Requests that arrive while
+// batches are on the GPU wait only for the next free worker, and batches of
+// different workers overlap on the device.  Admission charges each request
+// an estimate of the device memory it needs; a request larger than the whole
+// budget is refused with ZKMETAL_ERR_BUSY at submit time.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <condition_variable>
+#include <deque>
+#include <memory>
+#include <mutex>
+#include <stdexcept>
+#include <thread>
+#include <unordered_map>
+
+#include "../../include/zkmsm.h"
+#include "engine.cuh"
+
+namespace zkmsm {
+
+struct TableView {  // the parts of a resident table the server needs
+    int curve;
+    uint64_t n;
+    const uint32_t* points;
+    const uint32_t* phi;
+};
+// defined in capi.cu
+bool table_view(ZkMsmTable t, TableView* out);
+
+namespace {
+
+using Clock = std::chrono::steady_clock;
+
+struct Request {
+    uint64_t id;
+    int curve;
+    int fmt;
+    uint32_t n;
+    const uint8_t* scalars;  // caller keeps it valid until the request completes
+    uint64_t bytes;          // admission charge
+    Clock::time_point t_submit, t_start, t_done;
+    int status = 1;          // 1 pending, 2 running, 0 done ok, < 0 error
+    uint8_t result[3 * 48];
+};
+
+struct Server {
+    TableView tables[2];
+    bool has_table[2] = {false, false};
+    uint64_t budget, in_use = 0;
+    uint64_t max_batch_points;
+    std::mutex mu;
+    std::condition_variable cv_work, cv_done;
+    std::deque<std::shared_ptr<Request>> pending;
+    std::unordered_map<uint64_t, std::shared_ptr<Request>> all;
+    std::atomic<uint64_t> next_id{1};
+    bool stop = false;
+    std::vector<std::thread> workers;
+    // stats
+    uint64_t batches = 0, completed = 0, failed = 0, max_batch = 0;
+    std::vector<double> latencies_ms;
+    int device = 0;
+    // host-side fault injection for tests: fail the next k batches
+    std::atomic<int> inject_failures{0};
+
+    static uint64_t estimate(int curve, uint32_t n) {
+        // scalars + sorted entries (2 halves x up to 8 windows x 8 B) + buckets
+        // and partial sums; generous so admission errs on the safe side
+        const uint64_t per_point = 32 + 2 * 8 * 8 + (curve == ZKMSM_BN254 ? 64 : 96);
+        return (uint64_t)n * per_point + (64ull << 20);
+    }
+
+    void worker_main(int w) {
+        cudaSetDevice(device);
+        std::unique_ptr<Engine> eng;
+        try {
+            eng.reset(new Engine());
+        } catch (...) {
+            return;
+        }
+        uint32_t* d_scalars = nullptr;
+        size_t d_cap = 0;
+        for (;;) {
+            std::vector<std::shared_ptr<Request>> batch;
+            uint64_t charged = 0;
+            int curve = 0;
+            {
+                std::unique_lock<std::mutex> lk(mu);
+                cv_work.wait(lk, [&] { return stop || !pending.empty(); });
+                if (stop && pending.empty()) break;
+                curve = pending.front()->curve;
+                const int fmt0 = pending.front()->fmt;
+                uint64_t pts = 0;
+                for (auto it = pending.begin(); it != pending.end();) {
+                    auto& r = *it;
+                    if (r->curve != curve || r->fmt != fmt0) {
+                        ++it;
+                        continue;
+                    }
+                    bool first = batch.empty();
+                    bool fits_mem = in_use + charged + r->bytes <= budget;
+                    bool fits_pts = pts + r->n <= max_batch_points;
+                    // the oldest request runs once memory frees up; later ones only if they fit
+                    if (!(fits_mem && (fits_pts || first))) {
+                        if (first) break;  // wait for memory
+                        ++it;
+                        continue;
+                    }
+                    pts += r->n;
+                    charged += r->bytes;
+                    r->status = 2;
+                    r->t_start = Clock::now();
+                    batch.push_back(r);
+                    it = pending.erase(it);
+                }
+                if (batch.empty()) {
+                    // nothing admissible now: wait for a completion to release memory
+                    cv_done.wait_for(lk, std::chrono::milliseconds(5));
+                    continue;
+                }
+                in_use += charged;
+            }
+            // run the batch outside the lock
+            int st = ZKMETAL_SUCCESS;
+            std::vector<uint8_t> out;
+            try {
+                if (inject_failures.load() > 0 && inject_failures.fetch_sub(1) > 0)
+                    throw std::runtime_error("injected batch failure");
+                const TableView& tv = tables[curve];
+                std::vector<uint32_t> counts, boffs;
+                uint64_t total = 0;
+                for (auto& r : batch) {
+                    counts.push_back(r->n);
+                    boffs.push_back(0);
+                    total += r->n;
+                }
+                if (total * 32 > d_cap) {
+                    if (d_scalars) cudaFree(d_scalars);
+                    d_scalars = nullptr;
+                    d_cap = 0;
+                    ZK_CUDA(cudaMalloc(&d_scalars, total * 32 + total * 4));
+                    d_cap = total * 32 + total * 4;
+                }
+                // one host-to-device copy per request into the batch's scalar array
+                uint64_t off = 0;
+                int fmt = batch[0]->fmt;
+                for (auto& r : batch) {
+                    ZK_CUDA(cudaMemcpyAsync(reinterpret_cast<uint8_t*>(d_scalars) + off * 32, r->scalars,
+                                            (size_t)r->n * 32, cudaMemcpyHostToDevice, eng->stream));
+                    off += r->n;
+                    if (r->fmt != fmt) fmt = -1;
+                }
+                if (fmt < 0) throw std::runtime_error("mixed scalar formats in one batch");
+                int fb = curve == ZKMSM_BN254 ? 32 : 48;
+                out.resize(batch.size() * 3 * fb);
+                if (curve == ZKMSM_BN254) {
+                    Plan& pl = eng->get_plan<Bn254>(counts, boffs, fmt);
+                    eng->run_device<Bn254>(pl, tv.points, tv.phi, d_scalars, out.data());
+                } else {
+                    Plan& pl = eng->get_plan<Bls381>(counts, boffs, fmt);
+                    eng->run_device<Bls381>(pl, tv.points, tv.phi, d_scalars, out.data());
+                }
+                for (size_t i = 0; i < batch.size(); i++) memcpy(batch[i]->result, out.data() + i * 3 * fb, 3 * fb);
+            } catch (const CudaError& e) {
+                set_error(std::string("server batch: ") + e.where + ": " + cudaGetErrorString(e.code));
+                cudaGetLastError();
+                st = ZKMETAL_ERR_GPU_ERROR;
+            } catch (const std::exception& e) {
+                set_error(std::string("server batch: ") + e.what());
+                st = ZKMETAL_ERR_GPU_ERROR;
+            }
+            {
+                std::lock_guard<std::mutex> lk(mu);
+                auto now = Clock::now();
+                for (auto& r : batch) {
+                    r->t_done = now;
+                    r->status = st;
+                    if (st == ZKMETAL_SUCCESS) {
+                        completed++;
+                        latencies_ms.push_back(std::chrono::duration<double, std::milli>(now - r->t_submit).count());
+                    } else {
+                        failed++;
+                    }
+                }
+                in_use -= charged;
+                batches++;
+                max_batch = std::max<uint64_t>(max_batch, batch.size());
+            }
+            cv_done.notify_all();
+            cv_work.notify_all();
+        }
+        if (d_scalars) cudaFree(d_scalars);
+        (void)w;
+    }
+};
+
+}  // namespace
+}  // namespace zkmsm
+
+using namespace zkmsm;
+
+extern "C" {
+
+ZkMetalStatus zkmsm_server_create(ZkMsmTable bn254_table, ZkMsmTable bls12_381_table, uint64_t hbm_budget_bytes,
+                                  int workers, uint64_t max_batch_points, ZkMsmServer* out) {
+    if (!out || (!bn254_table && !bls12_381_table) || workers < 1 || workers > 16) return ZKMETAL_ERR_INVALID_INPUT;
+    std::unique_ptr<Server> s(new Server());
+    if (bn254_table) {
+        if (!table_view(bn254_table, &s->tables[0]) || s->tables[0].curve != ZKMSM_BN254)
+            return ZKMETAL_ERR_INVALID_INPUT;
+        s->has_table[0] = true;
+    }
+    if (bls12_381_table) {
+        if (!table_view(bls12_381_table, &s->tables[1]) || s->tables[1].curve != ZKMSM_BLS12_381)
+            return ZKMETAL_ERR_INVALID_INPUT;
+        s->has_table[1] = true;
+    }
+    cudaGetDevice(&s->device);
+    if (hbm_budget_bytes == 0) {
+        size_t fr = 0, tot = 0;
+        if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) return ZKMETAL_ERR_GPU_ERROR;
+        hbm_budget_bytes = fr / 10 * 7;  // leave room for the engines' own growth
+    }
+    s->budget = hbm_budget_bytes;
+    s->max_batch_points = max_batch_points ? max_batch_points : (1ull << 24);
+    Server* sp = s.get();
+    for (int w = 0; w < workers; w++) s->workers.emplace_back([sp, w] { sp->worker_main(w); });
+    *out = s.release();
+    return ZKMETAL_SUCCESS;
+}
+
+ZkMetalStatus zkmsm_server_submit(ZkMsmServer server, int curve, const void* scalars, int scalar_fmt,
+                                  uint32_t n_points, uint64_t* request_id) {
+    if (!server || !scalars || !request_id || n_points == 0) return ZKMETAL_ERR_INVALID_INPUT;
+    if (curve != ZKMSM_BN254 && curve != ZKMSM_BLS12_381) return ZKMETAL_ERR_INVALID_INPUT;
+    if (scalar_fmt != ZKMSM_SCALAR_INT && scalar_fmt != ZKMSM_SCALAR_MONT) return ZKMETAL_ERR_INVALID_INPUT;
+    Server& s = *static_cast<Server*>(server);
+    if (!s.has_table[curve] || n_points > s.tables[curve].n) return ZKMETAL_ERR_INVALID_INPUT;
+    auto r = std::make_shared<Request>();
+    r->curve = curve;
+    r->fmt = scalar_fmt;
+    r->n = n_points;
+    r->scalars = static_cast<const uint8_t*>(scalars);
+    r->bytes = Server::estimate(curve, n_points);
+    if (r->bytes > s.budget) {
+        set_error("request needs more device memory than the server's budget");
+        return ZKMETAL_ERR_BUSY;
+    }
+    r->t_submit = Clock::now();
+    {
+        std::lock_guard<std::mutex> lk(s.mu);
+        if (s.stop) return ZKMETAL_ERR_BUSY;
+        r->id = s.next_id++;
+        s.all[r->id] = r;
+        s.pending.push_back(r);
+    }
+    s.cv_work.notify_one();
+    *request_id = r->id;
+    return ZKMETAL_SUCCESS;
+}
+
+ZkMetalStatus zkmsm_server_cancel(ZkMsmServer server, uint64_t request_id) {
+    if (!server) return ZKMETAL_ERR_INVALID_INPUT;
+    Server& s = *static_cast<Server*>(server);
+    std::lock_guard<std::mutex> lk(s.mu);
+    auto it = s.all.find(request_id);
+    if (it == s.all.end()) return ZKMETAL_ERR_INVALID_INPUT;
+    auto& r = it->second;
+    if (r->status != 1) return ZKMETAL_ERR_BUSY;  // already running or done
+    s.pending.erase(std::remove(s.pending.begin(), s.pending.end(), r), s.pending.end());
+    r->status = ZKMETAL_ERR_BUSY;
+    r->t_done = Clock::now();
+    s.cv_done.notify_all();
+    return ZKMETAL_SUCCESS;
+}
+
+ZkMetalStatus zkmsm_server_wait(ZkMsmServer server, uint64_t request_id, int timeout_ms, uint8_t* result,
+                                double* latency_ms) {
+    if (!server) return ZKMETAL_ERR_INVALID_INPUT;
+    Server& s = *static_cast<Server*>(server);
+    std::unique_lock<std::mutex> lk(s.mu);
+    auto it = s.all.find(request_id);
+    if (it == s.all.end()) return ZKMETAL_ERR_INVALID_INPUT;
+    auto r = it->second;
+    auto done = [&] { return r->status <= 0; };
+    if (timeout_ms < 0) s.cv_done.wait(lk, done);
+    else if (!s.cv_done.wait_for(lk, std::chrono::milliseconds(timeout_ms), done)) return ZKMETAL_ERR_BUSY;
+    int st = r->status;
+    if (st == ZKMETAL_SUCCESS && result) memcpy(result, r->result, 3 * (r->curve == ZKMSM_BN254 ? 32 : 48));
+    if (latency_ms) *latency_ms = std::chrono::duration<double, std::milli>(r->t_done - r->t_submit).count();
+    s.all.erase(it);
+    return st;
+}
+
+ZkMetalStatus zkmsm_server_stats(ZkMsmServer server, char* buf, uint64_t buflen) {
+    if (!server || !buf || !buflen) return ZKMETAL_ERR_INVALID_INPUT;
+    Server& s = *static_cast<Server*>(server);
+    std::lock_guard<std::mutex> lk(s.mu);
+    std::vector<double> v = s.latencies_ms;
+    std::sort(v.begin(), v.end());
+    auto pct = [&](double q) { return v.empty() ? 0.0 : v[std::min(v.size() - 1, (size_t)(q * (v.size() - 1) + 0.5))]; };
+    char tmp[512];
+    snprintf(tmp, sizeof tmp,
+             "{\"completed\":%llu,\"failed\":%llu,\"batches\":%llu,\"max_batch\":%llu,\"pending\":%zu,"
+             "\"p50_ms\":%.3f,\"p99_ms\":%.3f,\"max_ms\":%.3f,\"budget_bytes\":%llu,\"in_use_bytes\":%llu}",
+             (unsigned long long)s.completed, (unsigned long long)s.failed, (unsigned long long)s.batches,
+             (unsigned long long)s.max_batch, s.pending.size(), pct(0.5), pct(0.99), v.empty() ? 0.0 : v.back(),
+             (unsigned long long)s.budget, (unsigned long long)s.in_use);
+    size_t k = std::min<size_t>(strlen(tmp), buflen - 1);
+    memcpy(buf, tmp, k);
+    buf[k] = 0;
+    return ZKMETAL_SUCCESS;
+}
+
+ZkMetalStatus zkmsm_server_inject_failures(ZkMsmServer server, int batches) {
+    if (!server || batches < 0) return ZKMETAL_ERR_INVALID_INPUT;
+    static_cast<Server*>(server)->inject_failures.store(batches);
+    return ZKMETAL_SUCCESS;
+}
+
+void zkmsm_server_destroy(ZkMsmServer server) {
+    if (!server) return;
+    Server* s = static_cast<Server*>(server);
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        s->stop = true;
+    }
+    s->cv_work.notify_all();
+    for (auto& t : s->workers) t.join();
+    delete s;
+}
+
+}  // extern "C"

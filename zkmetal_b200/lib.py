@@ -72,6 +72,16 @@ _SIGS = {
     "zkmsm_table_device_points": (c_vp, [c_vp]),
     "zkmsm_batch_commit": (c_i32, [c_vp, c_vp, c_vp, c_int, c_int, c_vp, c_u32, c_u8p]),
     "zkmsm_engine_set_tuning": (c_i32, [c_vp, c_int, c_int, c_int]),
+    "zkmsm_server_create": (c_i32, [c_vp, c_vp, c_u64, c_int, c_u64, ctypes.POINTER(c_vp)]),
+    "zkmsm_server_submit": (c_i32, [c_vp, c_int, c_vp, c_int, c_u32, ctypes.POINTER(c_u64)]),
+    "zkmsm_server_cancel": (c_i32, [c_vp, c_u64]),
+    "zkmsm_server_wait": (c_i32, [c_vp, c_u64, c_int, c_vp, ctypes.POINTER(ctypes.c_double)]),
+    "zkmsm_server_stats": (c_i32, [c_vp, ctypes.c_char_p, c_u64]),
+    "zkmsm_server_inject_failures": (c_i32, [c_vp, c_int]),
+    "zkmsm_server_destroy": (None, [c_vp]),
+    "zkmsm_autotune": (c_i32, [c_vp, c_int, c_int, c_int, ctypes.c_char_p, c_u64]),
+    "zkmsm_tuning_save": (c_i32, [c_vp, ctypes.c_char_p]),
+    "zkmsm_tuning_load": (c_i32, [c_vp, ctypes.c_char_p]),
     "zkmsm_gen_bases": (c_i32, [c_vp, c_int, c_u64, c_u64, c_u64, c_vp]),
     "zkmsm_gen_scalars": (c_i32, [c_vp, c_int, c_u64, c_u64, c_u64, c_int, c_int, c_vp]),
     "zkmsm_engine_launch_count": (c_u64, [c_vp]),

@@ -224,3 +224,67 @@ class CommitmentTable:
         raw = out.raw
         return [PointProjective(raw[i * 3 * fb:i * 3 * fb + fb], raw[i * 3 * fb + fb:i * 3 * fb + 2 * fb],
                                 raw[i * 3 * fb + 2 * fb:(i + 1) * 3 * fb]) for i in range(len(counts))]
+
+
+class CommitmentServer:
+    """Continuous-batching commitment server over resident tables (new API).
+
+    ``submit`` returns a request id; ``wait`` returns (PointProjective,
+    latency_ms).  Scalar arrays passed to ``submit`` are kept referenced here
+    until their request completes, as the server reads them asynchronously.
+    """
+
+    def __init__(self, bn254_table=None, bls12_381_table=None, hbm_budget_bytes=0, workers=2,
+                 max_batch_points=0):
+        h = ctypes.c_void_p()
+        _raise_for(_l.lib().zkmsm_server_create(bn254_table._h if bn254_table else None,
+                                                bls12_381_table._h if bls12_381_table else None,
+                                                hbm_budget_bytes, workers, max_batch_points, ctypes.byref(h)))
+        self._h = h
+        self._keep = {}
+        self._curve = {}
+
+    def submit(self, curve, scalars, fmt=_l.SCALAR_INT):
+        s = as_bytes_array(scalars, 32)
+        rid = ctypes.c_uint64()
+        st = _l.lib().zkmsm_server_submit(self._h, curve, s.ctypes.data, fmt, s.size // 32, ctypes.byref(rid))
+        _raise_for(st)
+        self._keep[rid.value] = s
+        self._curve[rid.value] = curve
+        return rid.value
+
+    def cancel(self, rid):
+        return _l.lib().zkmsm_server_cancel(self._h, rid)
+
+    def wait(self, rid, timeout_ms=-1):
+        fb = _l.FP_BYTES[self._curve[rid]]
+        out = ctypes.create_string_buffer(3 * fb)
+        lat = ctypes.c_double()
+        st = _l.lib().zkmsm_server_wait(self._h, rid, timeout_ms, out, ctypes.byref(lat))
+        if st != _l.ERR_BUSY or timeout_ms < 0:
+            self._keep.pop(rid, None)
+            self._curve.pop(rid, None)
+        _raise_for(st)
+        raw = out.raw
+        return PointProjective(raw[:fb], raw[fb:2 * fb], raw[2 * fb:3 * fb]), lat.value
+
+    def stats(self):
+        import json
+        buf = ctypes.create_string_buffer(1024)
+        _raise_for(_l.lib().zkmsm_server_stats(self._h, buf, len(buf)))
+        return json.loads(buf.value.decode())
+
+    def inject_failures(self, batches):
+        _raise_for(_l.lib().zkmsm_server_inject_failures(self._h, batches))
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _l.lib().zkmsm_server_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
