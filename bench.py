@@ -310,6 +310,14 @@ def run_serve_config(duration_s=60.0, rate=200.0, seed=0x5EED0004, table_log2=22
     th.join()
     wall = time.perf_counter() - start
     st = srv.stats()
+    # capacity: the same stream submitted at once (closed loop)
+    k_sat = min(len(reqs), 400)
+    t0 = time.perf_counter()
+    sat_ids = [srv.submit(c, pools[(c, dist)][off * 32:(off + n) * 32], zl.SCALAR_MONT)
+               for (ta, c, n, dist, off) in reqs[:k_sat]]
+    for i in sat_ids:
+        srv.wait(i)
+    t_sat = time.perf_counter() - t0
     srv.close()
     # back-to-back plain drop-in calls on the first requests of the same stream
     k = min(plain_sample, len(reqs))
@@ -331,9 +339,77 @@ def run_serve_config(duration_s=60.0, rate=200.0, seed=0x5EED0004, table_log2=22
             "requests": len(reqs), "completed": st["completed"], "failed": st["failed"], "batches": st["batches"],
             "max_batch": st["max_batch"], "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"],
             "served_commits_per_s": round(st["completed"] / wall, 1),
+            "saturated_commits_per_s": round(k_sat / t_sat, 1),
             "plain_dropin_commits_per_s": round(k / t_plain, 1),
             "speedup_vs_plain_dropin": round((st["completed"] / wall) / (k / t_plain), 2),
+            "capacity_vs_plain_dropin": round((k_sat / t_sat) / (k / t_plain), 2),
             "bit_exact_vs_plain": served[:k] == plain}
+
+
+def run_bls_config(seed=0x5EED0003, log2n=22, n_batch=8, lo=14, hi=22):
+    """BLS12-381 G1: one plain 2^22 MSM (device-resident) and a batch of 8 MSMs
+    with sizes log-uniform in [2^14, 2^22] against back-to-back plain calls."""
+    import numpy as np
+    import torch
+    from zkmetal_b200 import BLS12381MSM, CommitmentTable
+    from zkmetal_b200 import lib as zl
+    L = zl.lib()
+    T = 1 << log2n
+    e = BLS12381MSM()
+    pts = _dev(torch, T * 96)
+    torch.cuda.synchronize()
+    assert L.zkmsm_gen_bases(e.handle, 1, seed, 0, T, pts.data_ptr()) == 0
+    rng = np.random.default_rng(seed)
+    counts = [int(round(2 ** u)) for u in rng.uniform(lo, hi, n_batch)]
+    total = max(sum(counts), T)
+    sc = _dev(torch, total * 32)
+    assert L.zkmsm_gen_scalars(e.handle, 1, seed + 1, 0, total, 0, 1, sc.data_ptr()) == 0
+    stream = torch.cuda.Stream()
+    res = _dev(torch, 144)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with torch.cuda.stream(stream):
+        for _ in range(2):
+            assert L.zkmsm_msm_device_async(e.handle, 1, pts.data_ptr(), None, sc.data_ptr(), 1, T, res.data_ptr(),
+                                            stream.cuda_stream) == 0
+        ev0.record(stream)
+        for _ in range(3):
+            assert L.zkmsm_msm_device_async(e.handle, 1, pts.data_ptr(), None, sc.data_ptr(), 1, T, res.data_ptr(),
+                                            stream.cuda_stream) == 0
+        ev1.record(stream)
+    torch.cuda.synchronize()
+    plain_ms = ev0.elapsed_time(ev1) / 3
+    table = CommitmentTable(e, pts.data_ptr(), on_device=True, n=T)
+    sc_h = _pinned(torch, sc)
+    out = ctypes.create_string_buffer(144)
+
+    def plain_device():
+        r, off = [], 0
+        for n in counts:
+            assert L.zkmsm_msm_device(e.handle, 1, pts.data_ptr(), sc.data_ptr() + off * 32, 1, n, out, None) == 0
+            r.append(out.raw)
+            off += n
+        return r
+
+    def batched():
+        return [p.x + p.y + p.z for p in table.batch_commit(sc_h.numpy()[:sum(counts) * 32], counts,
+                                                              fmt=zl.SCALAR_MONT)]
+    plain_device()
+    batched()
+    t0 = time.perf_counter()
+    r_dev = plain_device()
+    t_dev = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    r_bat = batched()
+    t_bat = time.perf_counter() - t0
+    table.close()
+    e.close()
+    return {"plain_2p22_ms": round(plain_ms, 3),
+            "plain_2p22_points_per_s": round(T / (plain_ms * 1e-3)),
+            "batch_workload": "8 MSMs, sizes 2^U (U ~ uniform[14,22]), prefixes of the 2^22 table",
+            "batch_points": sum(counts), "batched_ms": round(t_bat * 1e3, 2),
+            "plain_device_back_to_back_ms": round(t_dev * 1e3, 2),
+            "speedup_vs_plain_device": round(t_dev / t_bat, 2),
+            "bit_exact_vs_plain": r_bat == r_dev}
 
 
 # --------------------------------------------------------------- GPU arm
@@ -355,21 +431,23 @@ def run_ours(args):
     eng = MetalMSM()
     if args.window:
         assert L.zkmsm_engine_set_tuning(eng.handle, args.window, args.chunk, -1) == 0
-    # inputs: this rank's shard [rank*n, (rank+1)*n) of the N*n-point MSM
+    # inputs: this rank's shard of the N*n-point MSM
+    from zkmetal_b200.shard import gather_partials, shard_range
+    shard0, shard1 = shard_range(n * world, world, rank)
+    assert shard1 - shard0 == n
     pts = torch.empty(n * 64, dtype=torch.uint8, device="cuda")
     sc = torch.empty(n * 32, dtype=torch.uint8, device="cuda")
     res = torch.empty(3 * 32, dtype=torch.uint8, device="cuda")
     torch.cuda.synchronize()
     t0 = time.time()
-    assert L.zkmsm_gen_bases(eng.handle, 0, args.seed, rank * n, n, pts.data_ptr()) == 0
-    assert L.zkmsm_gen_scalars(eng.handle, 0, args.seed, rank * n, n, 0 if args.dist == "uniform" else 1, 1,
+    assert L.zkmsm_gen_bases(eng.handle, 0, args.seed, shard0, n, pts.data_ptr()) == 0
+    assert L.zkmsm_gen_scalars(eng.handle, 0, args.seed, shard0, n, 0 if args.dist == "uniform" else 1, 1,
                                sc.data_ptr()) == 0
     log("rank %d: inputs generated in %.1f s" % (rank, time.time() - t0))
     # a dedicated stream: torch's default stream has handle 0, which the
     # library reads as "use the engine's own stream"
     stream = torch.cuda.Stream()
     torch.cuda.set_stream(stream)
-    gathered = torch.empty(world * 96, dtype=torch.uint8, device="cuda")
     final = torch.empty(96, dtype=torch.uint8, device="cuda")
 
     def step():
@@ -377,7 +455,7 @@ def run_ours(args):
                                       stream.cuda_stream)
         assert st == 0, zl.last_error()
         if world > 1:
-            dist.all_gather_into_tensor(gathered, res)
+            gathered = gather_partials(res, world)
             assert L.zkmsm_sum_results_device(0, gathered.data_ptr(), world, final.data_ptr(),
                                               stream.cuda_stream) == 0
 
@@ -430,9 +508,7 @@ def run_ours(args):
             assert st == 0, zl.last_error()
             if world > 1:
                 mine = torch.frombuffer(bytearray(rx.raw + ry.raw + rz.raw), dtype=torch.uint8).cuda()
-                g = torch.empty(world * 96, dtype=torch.uint8, device="cuda")
-                dist.all_gather_into_tensor(g, mine)
-                out_all.copy_(g.cpu())
+                out_all.copy_(gather_partials(mine, world).cpu())
                 fin = ctypes.create_string_buffer(96)
                 assert L.zkmsm_sum_results(0, out_all.numpy().ctypes.data, world, fin) == 0
             dt = (time.perf_counter() - t0) * 1e3
@@ -510,6 +586,10 @@ def run_ours(args):
             line["batch"] = run_batch_config()
         except Exception as exc:  # reported, not hidden
             line["batch"] = {"error": repr(exc)}
+        try:
+            line["bls12_381"] = run_bls_config()
+        except Exception as exc:
+            line["bls12_381"] = {"error": repr(exc)}
         try:
             line["serve"] = run_serve_config(duration_s=args.serve_seconds, plain_sample=40)
         except Exception as exc:
