@@ -594,7 +594,9 @@ ZkMetalStatus zkmsm_plan_describe(int curve, const uint32_t* counts, uint32_t n_
                  std::to_string(d.win_off) + "]";
         }
         s += "],\"entry_bound\":" + std::to_string(pl.entry_bound) + ",\"nbuckets\":" + std::to_string(pl.nbuckets) +
-             ",\"acc\":[";
+             ",\"sort\":[" + std::to_string(pl.sort_maxd) + "," + std::to_string(pl.sort_spb) + "," +
+             std::to_string(pl.sort_passes) + "," + std::to_string(pl.sort_bits) + "," +
+             std::to_string(pl.sort_tiles) + "],\"acc\":[";
         for (size_t l = 0; l < pl.acc_K.size(); l++)
             s += (l ? "," : "") + std::string("[") + std::to_string(pl.acc_K[l]) + "," + std::to_string(pl.acc_T[l]) +
                  "," + std::to_string(pl.acc_Mbound[l]) + "]";

@@ -81,6 +81,10 @@ struct Plan {
     uint64_t entry_bound = 0;
     uint32_t nbuckets = 0;
     uint32_t nwin_total = 0;
+    // radix sort of the entries (msm_kernels.cuh): at most sort_maxd digits
+    // per scalar, sort_spb scalars per digit block, sort_passes passes of
+    // sort_bits-bit digits over sort_tiles tiles of SORT_ETILE entries
+    uint32_t sort_maxd = 0, sort_spb = 0, sort_passes = 0, sort_bits = 0, sort_tiles = 0;
     // segmented-sum levels: chunk length and chunk-count bound per level
     std::vector<uint32_t> acc_K, acc_T;
     std::vector<uint64_t> acc_Mbound;
@@ -184,6 +188,7 @@ class Engine {
 
     // workspace
     DevBuf w_points, w_phi, w_scalars, w_counts, w_offsets, w_cursor, w_ents, w_buckets;
+    DevBuf w_ents2, w_thist;
     DevBuf w_cnt, w_pos, w_tiles, w_totals, w_pkeys[2], w_pvals[2], w_redS[2], w_redW[2];
     DevBuf w_results, w_comb;
     bool comb_ready[2] = {false, false};
@@ -245,6 +250,20 @@ class Engine {
         pl.total_scalars = soff;
         pl.nbuckets = boff;
         pl.nwin_total = woff;
+        {
+            uint32_t maxd = 1;
+            for (auto& d : pl.descs) maxd = std::max(maxd, (d.glv ? 2u : 1u) * d.nwin);
+            uint32_t spb = SORT_DBUF / maxd;
+            if (spb >= SORT_DTHREADS) spb -= spb % SORT_DTHREADS;
+            uint32_t kb = 0;
+            while (kb < 32 && (1ull << kb) < (uint64_t)boff) kb++;
+            uint32_t passes = (kb + 7) / 8;
+            pl.sort_maxd = maxd;
+            pl.sort_spb = std::max<uint32_t>(spb, 1);
+            pl.sort_passes = passes;
+            pl.sort_bits = passes ? (kb + passes - 1) / passes : 0;
+            pl.sort_tiles = (uint32_t)std::max<uint64_t>((pl.entry_bound + SORT_ETILE - 1) / SORT_ETILE, 1);
+        }
         // segmented-sum levels
         uint64_t M = pl.entry_bound;
         uint32_t K1 = tuning.chunk > 0 ? (uint32_t)tuning.chunk : 0;
@@ -355,6 +374,9 @@ class Engine {
         grew |= w_counts.ensure(((size_t)pl.nbuckets + 1) * 4);
         grew |= w_cursor.ensure(((size_t)pl.nbuckets + 1) * 4);
         grew |= w_ents.ensure(pl.entry_bound * 8 + 16);
+        const uint64_t hsz = (uint64_t)(1u << pl.sort_bits) * pl.sort_tiles;
+        grew |= w_ents2.ensure(pl.entry_bound * 8 + 16);
+        grew |= w_thist.ensure(hsz * 4 + 16);
         grew |= w_buckets.ensure((size_t)pl.nbuckets * xs + xs);
         uint64_t tmax = 1, m2 = 1, m3 = 1;
         for (size_t l = 0; l < pl.acc_T.size(); l++) tmax = std::max<uint64_t>(tmax, pl.acc_T[l]);
@@ -373,7 +395,8 @@ class Engine {
         }
         grew |= w_results.ensure((pl.descs.size() + 1) * 3 * P::N * 4);
         // scan tile sums for the longest scanned array (no allocation inside enqueue)
-        grew |= w_tiles.ensure(((std::max<uint64_t>(pl.nbuckets, tmax) + 2047) / 2048 + 2) * 4);
+        grew |= w_tiles.ensure(((std::max<uint64_t>(std::max<uint64_t>(pl.nbuckets, tmax), hsz) + 2047) / 2048 + 2) *
+                               4);
         if (grew) drop_graphs();  // captured graphs hold the old addresses
     }
 

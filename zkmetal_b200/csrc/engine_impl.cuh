@@ -4,6 +4,9 @@
 #include "engine.cuh"
 #include "msm_kernels.cuh"
 
+#include <stdexcept>
+#include <utility>
+
 namespace zkmsm {
 
 // Exclusive scan of n u32 in place; total to d_total; optional copy.
@@ -32,23 +35,41 @@ void Engine::enqueue(const Plan& pl, const uint32_t* d_bases, const uint32_t* d_
     uint32_t* tot = w_totals.as<uint32_t>();
     auto ev = prof_begin();
     prof_mark(ev, 0);
-    ZK_CUDA(cudaMemsetAsync(w_counts.p, 0, ((size_t)pl.nbuckets + 1) * 4, stream));
     ZK_CUDA(cudaMemsetAsync(w_buckets.p, 0, (size_t)pl.nbuckets * sizeof(Xyzz<P>), stream));
+    // radix sort of the entries by bucket id; tot[0] = number of entries.
+    // The digit pass writes to whichever buffer makes the last pass land in
+    // w_ents; slot 63 of w_totals takes the (unused) totals of the scans.
+    ZK_CUDA(cudaMemsetAsync(tot, 0, 4, stream));
+    uint2* bufA = (pl.sort_passes & 1) ? w_ents2.as<uint2>() : w_ents.as<uint2>();
+    uint2* bufB = (pl.sort_passes & 1) ? w_ents.as<uint2>() : w_ents2.as<uint2>();
     if (pl.total_scalars) {
-        uint64_t g = (pl.total_scalars + 255) / 256;
-        k_digit_hist<C><<<(unsigned)g, 256, 0, stream>>>(d_scalars, dd, nd, pl.total_scalars,
-                                                        w_counts.as<uint32_t>());
+        const uint64_t g = (pl.total_scalars + pl.sort_spb - 1) / pl.sort_spb;
+        k_radix_digits<C><<<(unsigned)g, SORT_DTHREADS, 0, stream>>>(d_scalars, dd, nd, pl.total_scalars,
+                                                                    pl.sort_spb, bufA, tot + 0);
         launches++;
         ZK_CUDA(cudaGetLastError());
     }
-    // bucket offsets (exclusive) -> counts array in place, copy to cursor
-    scan_u32(*this, w_counts.as<uint32_t>(), pl.nbuckets, tot + 0, w_cursor.as<uint32_t>());
-    if (pl.total_scalars) {
-        uint64_t g = (pl.total_scalars + 255) / 256;
-        k_digit_scatter<C><<<(unsigned)g, 256, 0, stream>>>(d_scalars, dd, nd, pl.total_scalars,
-                                                           w_cursor.as<uint32_t>(), w_ents.as<uint2>());
+    for (uint32_t ps = 0; ps < pl.sort_passes; ps++) {
+        const uint32_t shift = ps * pl.sort_bits, nt = pl.sort_tiles;
+        k_radix_hist<<<nt, SORT_ETHREADS, 0, stream>>>(bufA, tot + 0, shift, pl.sort_bits, nt,
+                                                        w_thist.as<uint32_t>());
         launches++;
         ZK_CUDA(cudaGetLastError());
+        scan_u32(*this, w_thist.as<uint32_t>(), (1u << pl.sort_bits) * nt, tot + 63, nullptr);
+        switch (pl.sort_bits) {
+#define ZK_SCATTER(B)                                                                                     \
+    case B:                                                                                              \
+        k_radix_scatter<B><<<nt, SORT_ETHREADS, 0, stream>>>(bufA, tot + 0, shift, nt, w_thist.as<uint32_t>(), \
+                                                             bufB);                                      \
+        break;
+            ZK_SCATTER(1) ZK_SCATTER(2) ZK_SCATTER(3) ZK_SCATTER(4)
+            ZK_SCATTER(5) ZK_SCATTER(6) ZK_SCATTER(7) ZK_SCATTER(8)
+#undef ZK_SCATTER
+            default: throw std::runtime_error("radix digit width out of range");
+        }
+        launches++;
+        ZK_CUDA(cudaGetLastError());
+        std::swap(bufA, bufB);
     }
     prof_mark(ev, 1);
     // segmented sums

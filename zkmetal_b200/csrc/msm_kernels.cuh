@@ -4,14 +4,17 @@
 // batch of one).  Reference counterparts (Shaders/msm/*.metal and the Swift
 // engine MSM/MSMEngine.swift) are cited per kernel.
 //
-//  1. k_digit_hist    scalar -> integer (Montgomery reduce or mod r), GLV
-//                     split, signed c-bit digits; histogram of global bucket
-//                     ids.          [glv_kernels.metal:172-256,
-//                     msm_kernels.metal:399-439, MSMEngine.swift:595-661]
-//  2. scan            exclusive prefix sum of the histogram (bucket offsets)
-//  3. k_digit_scatter recompute digits, place (bucket, point|endo|sign) at
-//                     the bucket's cursor: a counting sort by bucket.
-//                     [msm_kernels.metal:279-397 (GPU sort, disabled there)]
+//  1. k_radix_digits  scalar -> integer (Montgomery reduce or mod r), GLV
+//                     split, signed c-bit digits; entries (bucket id,
+//                     point|endo|sign) appended densely, unsorted.
+//                     [glv_kernels.metal:172-256, msm_kernels.metal:399-439]
+//  2. k_radix_hist /  LSD radix sort of the entries by bucket id, 7-8 bits
+//     k_radix_scatter per pass: per-tile digit counts, scan, stable
+//                     tile-local ranking staged in shared memory and written
+//                     as contiguous runs.  [MSMEngine.swift:595-661 (CPU
+//                     counting sort per window)]
+//     (k_digit_hist / k_digit_scatter: the earlier one-pass counting sort
+//     with global atomics, kept for the allocation-free entry point.)
 //  4. k_acc_l1        bucket accumulation: each thread sums a fixed-length
 //                     chunk of the sorted list with mixed XYZZ additions;
 //                     runs wholly inside a chunk are final buckets, runs cut
@@ -300,6 +303,231 @@ __global__ void __launch_bounds__(256) k_digit_scatter(const uint32_t* __restric
             uint32_t pos = a[s].grp ? b + __popc(a[s].same & ((1u << lane) - 1)) : base[s];
             if (valid[s]) ents[pos] = make_uint2(gb[s], val[s]);
         }
+    }
+}
+
+// ------------------------------------------------------------ radix sort
+// Entries (bucket id, point | endo | sign) are sorted by bucket id with an
+// LSD radix sort, without global atomics on the data path:
+//  k_radix_digits   digits of SORT_DTILE-ish scalars per block, buffered in
+//                   shared memory and appended densely to A (one atomic per
+//                   block claims the range; the order of blocks is free);
+//  per pass (RBITS-bit digit at `shift`), over tiles of SORT_ETILE entries:
+//  k_radix_hist     per-tile digit counts, stored digit-major [digit][tile];
+//  scan             exclusive, so [digit][tile] holds the tile's first slot;
+//  k_radix_scatter  stable rank inside the tile (warp ballots per digit bit,
+//                   per-warp counters), staged in shared memory in digit
+//                   order, then written out as one contiguous run per digit.
+// Passes after the first are stable, so the result is sorted by the whole
+// key; the order inside a bucket comes from the first pass and is not
+// fixed (bucket sums do not depend on it).
+
+// Lanes of the warp whose BITS-bit digit equals this lane's (valid lanes
+// only; `vmask` = ballot of valid): one ballot per digit bit.
+template <int BITS>
+ZK_DEV uint32_t digit_peers(uint32_t d, uint32_t vmask) {
+    uint32_t peers = vmask;
+#pragma unroll
+    for (int b = 0; b < BITS; b++) {
+        const bool bit = (d >> b) & 1u;
+        const uint32_t bal = __ballot_sync(0xffffffffu, bit);
+        peers &= bit ? bal : ~bal;
+    }
+    return peers;
+}
+
+// Shared-memory counter bump with the hot-key case aggregated: lanes whose
+// key equals the first valid lane's key share one atomic (all lanes of a
+// warp hitting one bin, e.g. many scalars equal to 1, cost one atomic, not
+// 32 serialised ones); other valid lanes add 1 each.  All 32 lanes of the
+// warp call it together.
+ZK_DEV void warp_count(uint32_t* __restrict__ ctr, bool valid, uint32_t key) {
+    const uint32_t lane = threadIdx.x & 31;
+    const uint32_t m = __ballot_sync(0xffffffffu, valid);
+    if (!m) return;
+    const uint32_t leader = __ffs(m) - 1;
+    const uint32_t lk = __shfl_sync(0xffffffffu, key, leader);
+    const bool grp = valid && key == lk;
+    const uint32_t same = __ballot_sync(0xffffffffu, grp);
+    if (lane == leader) atomicAdd(ctr + lk, (uint32_t)__popc(same));
+    else if (valid && !grp) atomicAdd(ctr + key, 1u);
+}
+
+template <class C>
+__global__ void __launch_bounds__(SORT_DTHREADS) k_radix_digits(const uint32_t* __restrict__ scalars,
+                                                                const MsmDesc* __restrict__ descs, int nd,
+                                                                uint64_t total, uint32_t scalars_per_block,
+                                                                uint2* __restrict__ A,
+                                                                uint32_t* __restrict__ d_count) {
+    __shared__ uint2 buf[SORT_DBUF];
+    __shared__ uint32_t cur, base_s;
+    const uint32_t tid = threadIdx.x, lane = tid & 31;
+    if (tid == 0) cur = 0;
+    __syncthreads();
+#pragma unroll 1
+    for (uint32_t k = 0; k < scalars_per_block; k += SORT_DTHREADS) {
+        const uint64_t gi = (uint64_t)blockIdx.x * scalars_per_block + k + tid;
+        Halves h;
+        h.count = 0;
+        MsmDesc d{};
+        d.c = 2;
+        uint32_t idx = 0;
+        DigitGen g{0, 0, 0};
+        if (k + tid < scalars_per_block && gi < total) {
+            d = descs[find_msm(descs, nd, gi)];
+            prepare_scalar<C>(h, scalars + gi * 8, d.fmt, d.glv);
+            idx = d.base_off + (uint32_t)(gi - d.scalar_off);
+            if (d.nwin == 0) g.j = (uint32_t)h.count;
+        }
+        bool valid[DBATCH];
+        uint32_t gb[DBATCH], val[DBATCH];
+#pragma unroll 1
+        while (__any_sync(0xffffffffu, g.j < (uint32_t)h.count)) {
+            next_digits(g, h, d, idx, valid, gb, val);
+            uint32_t nv = 0;
+#pragma unroll
+            for (int s = 0; s < DBATCH; s++) nv += valid[s] ? 1u : 0u;
+            uint32_t incl = nv;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= (uint32_t)o) incl += t;
+            }
+            uint32_t base = 0;
+            if (lane == 31 && incl) base = atomicAdd(&cur, incl);
+            base = __shfl_sync(0xffffffffu, base, 31) + incl - nv;
+            // valid slots form a prefix of the batch; the buffer holds every
+            // digit of the block's scalars (scalars_per_block * max digits)
+#pragma unroll
+            for (int s = 0; s < DBATCH; s++)
+                if (valid[s]) buf[base + s] = make_uint2(gb[s], val[s]);
+        }
+    }
+    __syncthreads();
+    const uint32_t cnt = cur;
+    if (tid == 0) base_s = cnt ? atomicAdd(d_count, cnt) : 0;
+    __syncthreads();
+    const uint32_t base = base_s;
+    for (uint32_t i = tid; i < cnt; i += SORT_DTHREADS) A[(size_t)base + i] = buf[i];
+}
+
+// Per-warp digit counts of the warp's SORT_ETILE / SORT_WARPS entries of a
+// tile (blocked: warp w owns entries [w*PER, (w+1)*PER)); also each entry's
+// rank among the warp's earlier entries with the same digit.
+constexpr uint32_t SORT_WARPS = SORT_ETHREADS / 32;
+constexpr uint32_t SORT_PER_WARP = SORT_ETILE / SORT_WARPS;
+constexpr uint32_t SORT_ROUNDS = SORT_PER_WARP / 32;
+
+static __global__ void __launch_bounds__(SORT_ETHREADS) k_radix_hist(const uint2* __restrict__ A,
+                                                                     const uint32_t* __restrict__ d_total,
+                                                                     uint32_t shift, uint32_t bits,
+                                                                     uint32_t ntiles, uint32_t* __restrict__ hist) {
+    __shared__ uint32_t cnt[SORT_MAX_BINS];
+    const uint32_t tid = threadIdx.x;
+    const uint32_t nb = 1u << bits, mask = nb - 1;
+    for (uint32_t i = tid; i < SORT_MAX_BINS; i += SORT_ETHREADS) cnt[i] = 0;
+    __syncthreads();
+    const uint64_t total = *d_total;
+    const uint64_t tbase = (uint64_t)blockIdx.x * SORT_ETILE;
+    constexpr uint32_t R = SORT_ETILE / SORT_ETHREADS;
+    uint32_t key[R];
+#pragma unroll
+    for (uint32_t r = 0; r < R; r++) {
+        const uint64_t i = tbase + r * SORT_ETHREADS + tid;
+        key[r] = i < total ? (A[i].x >> shift) & mask : 0xffffffffu;
+    }
+#pragma unroll
+    for (uint32_t r = 0; r < R; r++) warp_count(cnt, key[r] != 0xffffffffu, key[r]);
+    __syncthreads();
+    for (uint32_t dg = tid; dg < nb; dg += SORT_ETHREADS) hist[(size_t)dg * ntiles + blockIdx.x] = cnt[dg];
+}
+
+template <int BITS>
+__global__ void __launch_bounds__(SORT_ETHREADS, 4) k_radix_scatter(const uint2* __restrict__ A,
+                                                                 const uint32_t* __restrict__ d_total,
+                                                                 uint32_t shift, uint32_t ntiles,
+                                                                 const uint32_t* __restrict__ hoff,
+                                                                 uint2* __restrict__ B) {
+    constexpr uint32_t NB = 1u << BITS, MASK = NB - 1;
+    __shared__ uint32_t wcnt[SORT_WARPS][SORT_MAX_BINS];
+    __shared__ uint32_t loff[SORT_MAX_BINS], goff[SORT_MAX_BINS], wtot[SORT_ETHREADS / 32];
+    __shared__ uint2 stage[SORT_ETILE];
+    const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    for (uint32_t i = tid; i < SORT_WARPS * SORT_MAX_BINS; i += SORT_ETHREADS) (&wcnt[0][0])[i] = 0;
+    __syncthreads();
+    const uint64_t total = *d_total;
+    const uint64_t tbase = (uint64_t)blockIdx.x * SORT_ETILE;
+    const uint32_t n_tile = tbase >= total ? 0u : total - tbase < SORT_ETILE ? (uint32_t)(total - tbase) : SORT_ETILE;
+    const uint64_t t0 = tbase + (uint64_t)warp * SORT_PER_WARP;
+    // pass 1: stable rank of each entry among the warp's earlier entries
+    // with its digit (warp w owns entries [w*PER, (w+1)*PER) of the tile)
+    // kr[r] = digit | rank << 16 (rank < SORT_PER_WARP)
+    uint32_t kr[SORT_ROUNDS];
+#pragma unroll
+    for (uint32_t r = 0; r < SORT_ROUNDS; r++) {
+        const uint64_t i = t0 + r * 32 + lane;
+        kr[r] = i < total ? (A[i].x >> shift) & MASK : 0;
+    }
+#pragma unroll
+    for (uint32_t r = 0; r < SORT_ROUNDS; r++) {
+        const uint64_t i = t0 + r * 32 + lane;
+        const bool v = i < total;
+        const uint32_t vm = __ballot_sync(0xffffffffu, v);
+        if (vm) {
+            const uint32_t d = kr[r];
+            const uint32_t peers = digit_peers<BITS>(d, vm);
+            const uint32_t before = v ? wcnt[warp][d] : 0;
+            kr[r] = d | (before + __popc(peers & ((1u << lane) - 1))) << 16;
+            __syncwarp();
+            if (v && lane == 31 - __clz(peers)) wcnt[warp][d] = before + __popc(peers);
+            __syncwarp();
+        }
+    }
+    __syncthreads();
+    // per digit: warps' counts -> warp offsets inside the digit; digit totals
+    for (uint32_t dg = tid; dg < SORT_MAX_BINS; dg += SORT_ETHREADS) {
+        uint32_t run = 0;
+#pragma unroll
+        for (uint32_t w = 0; w < SORT_WARPS; w++) {
+            const uint32_t c = wcnt[w][dg];
+            wcnt[w][dg] = run;
+            run += c;
+        }
+        loff[dg] = dg < NB ? run : 0;
+        goff[dg] = dg < NB ? hoff[(size_t)dg * ntiles + blockIdx.x] : 0;
+    }
+    __syncthreads();
+    // exclusive scan of the digit totals (SORT_MAX_BINS == SORT_ETHREADS)
+    {
+        const uint32_t c = loff[tid];
+        uint32_t incl = c;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= (uint32_t)o) incl += t;
+        }
+        if (lane == 31) wtot[warp] = incl;
+        __syncthreads();
+        uint32_t add = 0;
+        for (uint32_t w = 0; w < warp; w++) add += wtot[w];
+        __syncthreads();
+        loff[tid] = add + incl - c;
+    }
+    __syncthreads();
+    // pass 2: re-read the tile (it is in L2) and stage it in digit order
+#pragma unroll
+    for (uint32_t r = 0; r < SORT_ROUNDS; r++) {
+        const uint64_t i = t0 + r * 32 + lane;
+        if (i < total) {
+            const uint32_t d = kr[r] & 0xffffu;
+            stage[loff[d] + wcnt[warp][d] + (kr[r] >> 16)] = A[i];
+        }
+    }
+    __syncthreads();
+    for (uint32_t i = tid; i < n_tile; i += SORT_ETHREADS) {
+        const uint2 v = stage[i];
+        const uint32_t d = (v.x >> shift) & MASK;
+        B[(size_t)goff[d] + (i - loff[d])] = v;
     }
 }
 

@@ -3,9 +3,13 @@
 // k_imad_peak: the denominator of the MSM roofline -- the sustained rate of
 // 32x32->64-bit word products (one mad.lo + one mad.hi with carry, the unit
 // the CIOS multiply is counted in) with every SM fully occupied and eight
-// independent carry chains per thread.
+// independent carry chains per thread.  On sm_100a a carry-chained lo/hi
+// pair issues as one instruction on the heavy FMA pipe, which accepts one
+// such 64-bit product every 4 cycles per scheduler (a 32-bit low product
+// every 2); k_imad_wide_peak (mad.wide.u32) measures the same rate.
 // k_fe_mul_peak: independent BN254 / BLS12-381 Montgomery products per
-// second (the field-multiply ceiling of this implementation).
+// second with per-thread operands (the field-multiply ceiling of this
+// implementation).
 // k_sum_results: adds a list of library results (reference Jacobian layout
 // with Z = 1 or the identity) into one, for combining per-GPU partial MSMs.
 #include <cuda_runtime.h>
@@ -41,14 +45,18 @@ __global__ void __launch_bounds__(256) k_imad_peak(uint32_t iters, uint32_t seed
     if (x == 0x12345678u) sink[0] = x;  // keep the work observable
 }
 
-// 64-bit multiply-add form of the same work: one mad.wide.u32 per product
+// 64-bit multiply-add form of the same work: one mad.wide.u32 per product.
+// The multiplier is the high word of the chain's own accumulator, so no two
+// products are alike and the compiler cannot fold repeated ones into adds
+// (with a loop-invariant multiplier it does, and the probe then times 64-bit
+// additions instead of products).
 __global__ void __launch_bounds__(256) k_imad_wide_peak(uint32_t iters, uint32_t seed, uint32_t* sink) {
     uint32_t a[8], b = seed ^ threadIdx.x;
     uint64_t acc[8];
 #pragma unroll
     for (int j = 0; j < 8; j++) {
         a[j] = seed * (j + 3) + threadIdx.x;
-        acc[j] = j;
+        acc[j] = ((uint64_t)(b * (j + 1)) << 32) | j;
     }
 #pragma unroll 1
     for (uint32_t it = 0; it < iters; it++) {
@@ -56,7 +64,9 @@ __global__ void __launch_bounds__(256) k_imad_wide_peak(uint32_t iters, uint32_t
         for (int r = 0; r < 8; r++) {
 #pragma unroll
             for (int j = 0; j < 8; j++) {
-                asm volatile("mad.wide.u32 %0, %1, %2, %0;" : "+l"(acc[j]) : "r"(a[j]), "r"(b));
+                asm volatile("{\n\t.reg .u32 h;\n\tmov.b64 {_, h}, %0;\n\tmad.wide.u32 %0, %1, h, %0;\n\t}"
+                             : "+l"(acc[j])
+                             : "r"(a[j]));
             }
         }
     }
@@ -73,10 +83,11 @@ __global__ void __launch_bounds__(256) k_fe_mul_peak(uint32_t iters, uint32_t* s
     for (int i = 0; i < P::N; i++) {
         x[0].v[i] = P::ONE(i) ^ threadIdx.x;
         x[1].v[i] = P::R2(i) ^ blockIdx.x;
-        y.v[i] = P::ONE(i);
+        y.v[i] = P::R2(i) ^ (threadIdx.x * 0x9e3779b9u) ^ blockIdx.x;  // per-thread multiplier
     }
     x[0].v[P::N - 1] &= 0x0fffffffu;
     x[1].v[P::N - 1] &= 0x0fffffffu;
+    y.v[P::N - 1] &= 0x0fffffffu;
 #pragma unroll 1
     for (uint32_t it = 0; it < iters; it++) {
         fe_mul(x[0], x[0], y);

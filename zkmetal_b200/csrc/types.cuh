@@ -30,6 +30,16 @@ struct MsmDesc {
 // Sorted-entry value: base index (30 bits) | endo << 30 | negate << 31
 constexpr uint32_t VAL_IDX_MASK = 0x3fffffffu;
 
+// Radix sort of the entries (k_radix_digits / k_radix_hist /
+// k_radix_scatter): digit-extraction block size and its shared buffer of
+// entries, entries per sort tile and threads per sort block, and the widest
+// digit (2^8 bins; one bin per sort thread).
+constexpr uint32_t SORT_DTHREADS = 256;
+constexpr uint32_t SORT_DBUF = 4096;
+constexpr uint32_t SORT_ETILE = 4096;
+constexpr uint32_t SORT_ETHREADS = 256;
+constexpr uint32_t SORT_MAX_BINS = 256;
+
 struct RedTask {
     uint32_t in_off;   // first child node
     uint32_t n_in;     // children
