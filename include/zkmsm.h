@@ -206,6 +206,12 @@ void zkmsm_server_destroy(ZkMsmServer server);
 
 /* Tuning overrides (0 = automatic): window bits, chunk length, GLV on/off. */
 ZkMetalStatus zkmsm_engine_set_tuning(ZkMetalMSMEngine engine, int window_bits, int chunk, int glv);
+/* NEW: host-buffer MSMs (zkmetal_*_msm and their _fr forms) of at least two
+ * stripes of 2^stripe_log2 points are streamed: they run as independent MSMs
+ * over consecutive point ranges, each stripe's host-to-device copy overlapping
+ * the previous stripe's computation, and the stripe results are added on the
+ * device (the same point).  Default 22; 0 turns striping off. */
+ZkMetalStatus zkmsm_engine_set_stripe(ZkMetalMSMEngine engine, int stripe_log2);
 
 /* Synthetic inputs on the device (seeded, counter based):
  * bases[i] = k_i * G with k_i uniform in [1, r); scalars uniform in Fr
@@ -248,6 +254,14 @@ double zkmsm_wide_products_per_s(void);
 ZkMetalStatus zkmsm_sum_results(int curve, const uint8_t* results, uint32_t count, uint8_t* out);
 /* Same on device buffers, enqueued on `stream` (cudaStream_t) without waiting. */
 ZkMetalStatus zkmsm_sum_results_device(int curve, const void* d_results, uint32_t count, void* d_out, void* stream);
+
+/* NEW (test helper, no counterpart in the reference): element-wise base-field
+ * operation on n device operands of N little-endian u32 limbs (N = 8 BN254,
+ * 12 BLS12-381), Montgomery form, each operand below 2p: op 0 r = a*b/R (the
+ * product the MSM kernels use), 1 r = a^2/R (their square), 2 r = a*b/R by a
+ * second implementation of the product.  Results are canonical (below p); the call
+ * waits for the device. */
+ZkMetalStatus zkmsm_field_op(int curve, int op, const void* d_a, const void* d_b, void* d_out, uint32_t n);
 
 /* NEW, with no counterpart in the reference: a BN254 G1 MSM that allocates no
  * device memory, for callers that cannot call cudaMalloc -- e.g. a framework

@@ -200,6 +200,36 @@ def test_small_scalar_variants(eng):
 
 
 @pytest.mark.parametrize("curve", ["bn254", "bls12_381"])
+@pytest.mark.parametrize("dist", ["uniform", "witness"])
+def test_striped_host_msm_matches_unstriped(eng, oracles, curve, dist):
+    """Host-buffer MSMs streamed in stripes (independent MSMs over consecutive
+    point ranges, the copy of stripe s overlapping the work on stripe s-1, the
+    stripe results added on the device) give the same point as the unstriped
+    MSM and as the oracle; n is no multiple of the stripe, so the last stripe
+    is shorter."""
+    C = R.CURVES[curve]
+    E = ENGINES[curve]()
+    L = zl.lib()
+    n = 3 * 4096 + 777
+    p, s = gen_inputs(E, curve, 901, n, dist, zl.SCALAR_MONT)
+    pb = np.frombuffer(to_host(p), dtype=np.uint8).copy()
+    sb = np.frombuffer(to_host(s), dtype=np.uint8).copy()
+    fn = L.zkmetal_bn254_msm_fr if curve == "bn254" else L.zkmetal_bls12_381_g1_msm_fr
+    outs = []
+    for stripe_log2 in (0, 12, 11, 12):
+        check(L.zkmsm_engine_set_stripe(E.handle, stripe_log2))
+        rx, ry, rz = (ctypes.create_string_buffer(C.fp_bytes) for _ in range(3))
+        check(fn(E.handle, pb.ctypes.data, sb.ctypes.data, n, rx, ry, rz))
+        outs.append(rx.raw + ry.raw + rz.raw)
+    assert outs[0] == outs[1] == outs[2] == outs[3]
+    ref, cm = oracles
+    orc = ref if ref is not None else cm
+    assert jac_to_affine_bytes(C, outs[0]) == oracle_msm(orc, curve, pb.tobytes(), sb.tobytes(), n, zl.SCALAR_MONT)
+    assert L.zkmsm_engine_set_stripe(E.handle, 40) == zl.ERR_INVALID_INPUT
+    E.close()
+
+
+@pytest.mark.parametrize("curve", ["bn254", "bls12_381"])
 def test_batch_entry_point_matches_plain(eng, curve):
     """zkmetal_*_msm_batch: concatenated inputs, count 0 -> 96/144 zero bytes
     (zkMetal_ffi.swift:1260-1264); each result equals its own plain call."""

@@ -8,6 +8,7 @@
 #include <memory>
 #include <mutex>
 #include <new>
+#include <stdexcept>
 
 #include "../../include/zkmsm.h"
 #include "engine.cuh"
@@ -57,12 +58,84 @@ static void h2d(Engine& e, DevBuf& buf, const void* src, size_t bytes) {
     if (bytes) ZK_CUDA(cudaMemcpyAsync(buf.p, src, bytes, cudaMemcpyHostToDevice, e.stream));
 }
 
+// Host-buffer MSMs of at least two stripes of 2^stripe_log2 points (engine
+// setting, default 2^22, zkmsm_engine_set_stripe) run as that many
+// independent MSMs over consecutive point ranges: stripe s is copied on the
+// engine's copy stream while stripe s-1 is computed on its compute stream,
+// each stripe picks its own window width, and the stripe results are added on
+// the device.  The sum is the same point as the unstriped MSM.
+static uint32_t stripe_count(const Engine& e, uint32_t n) {
+    if (e.stripe_log2 == 0 || e.stripe_log2 > 31) return 1;
+    uint32_t s = n >> e.stripe_log2;
+    return s < 2 ? 1 : (s > 16 ? 16 : s);
+}
+
+template <class C>
+static void msm_host_striped(Engine& e, const uint8_t* points, const uint8_t* scalars, uint32_t n, int fmt,
+                             uint32_t scalar_bits, uint32_t S, uint8_t* out) {
+    using P = typename C::Fp;
+    const size_t pb = (size_t)2 * P::N * 4, rw = (size_t)3 * P::N;  // bytes per point, words per result
+    const uint32_t ns = (n + S - 1) / S;
+    const uint32_t nl = n - (S - 1) * ns;
+    // (a lookup may evict the cache: fetch the first plan again after the second)
+    Plan* pa = &e.get_plan<C>({ns}, {0}, fmt, scalar_bits);
+    Plan* pz = &e.get_plan<C>({nl}, {0}, fmt, scalar_bits);
+    pa = &e.get_plan<C>({ns}, {0}, fmt, scalar_bits);
+    const bool glv = pa->descs[0].glv;
+    bool grew = e.w_points.ensure((size_t)n * pb + 16);
+    grew |= e.w_scalars.ensure((size_t)n * 32 + 16);
+    if (glv) grew |= e.w_phi.ensure((size_t)n * pb + 16);
+    if (grew) e.drop_graphs();
+    e.ensure_workspace<C>(*pa);
+    e.ensure_workspace<C>(*pz);
+    e.w_stripe_results.ensure((S + 1) * rw * 4);
+    e.ensure_copy_resources(S + 1);
+    // buffers (re)allocated in the compute stream's order: the copies wait for that
+    ZK_CUDA(cudaEventRecord(e.copy_events[S], e.stream));
+    ZK_CUDA(cudaStreamWaitEvent(e.copy_stream, e.copy_events[S], 0));
+    uint8_t* dp = static_cast<uint8_t*>(e.w_points.p);
+    uint8_t* ds = static_cast<uint8_t*>(e.w_scalars.p);
+    uint8_t* dphi = glv ? static_cast<uint8_t*>(e.w_phi.p) : dp;
+    uint32_t* res = e.w_stripe_results.as<uint32_t>();
+    for (uint32_t s = 0; s < S; s++) {
+        const size_t off = (size_t)s * ns;
+        const uint32_t cnt = s + 1 < S ? ns : nl;
+        ZK_CUDA(cudaMemcpyAsync(ds + off * 32, scalars + off * 32, (size_t)cnt * 32, cudaMemcpyHostToDevice,
+                                e.copy_stream));
+        ZK_CUDA(cudaMemcpyAsync(dp + off * pb, points + off * pb, (size_t)cnt * pb, cudaMemcpyHostToDevice,
+                                e.copy_stream));
+        ZK_CUDA(cudaEventRecord(e.copy_events[s], e.copy_stream));
+        ZK_CUDA(cudaStreamWaitEvent(e.stream, e.copy_events[s], 0));
+        const uint32_t* sp = reinterpret_cast<const uint32_t*>(dp + off * pb);
+        uint32_t* sphi = reinterpret_cast<uint32_t*>(dphi + off * pb);
+        if (glv) e.make_phi<C>(sp, cnt, sphi);
+        e.enqueue<C>(s + 1 < S ? *pa : *pz, sp, sphi, reinterpret_cast<const uint32_t*>(ds + off * 32),
+                     res + s * rw);
+    }
+    const ZkMetalStatus st =
+            zkmsm_sum_results_device(CurveTraits<C>::id == 0 ? ZKMSM_BN254 : ZKMSM_BLS12_381, res, S, res + S * rw,
+                                     e.stream);
+    if (st != ZKMETAL_SUCCESS) throw std::runtime_error("adding the stripe results failed");
+    e.launches++;
+    ZK_CUDA(cudaMemcpyAsync(out, res + S * rw, rw * 4, cudaMemcpyDeviceToHost, e.stream));
+    ZK_CUDA(cudaStreamSynchronize(e.stream));
+}
+
 template <class C>
 static ZkMetalStatus msm_host(Engine& e, const uint8_t* points, const uint8_t* scalars, uint32_t n, int fmt,
                               uint32_t scalar_bits, uint8_t* rx, uint8_t* ry, uint8_t* rz) {
     using P = typename C::Fp;
     const int fb = P::N * 4;
     if (n == 0 || !points || !scalars || !rx || !ry || !rz) return ZKMETAL_ERR_INVALID_INPUT;
+    const uint32_t S = stripe_count(e, n);
+    if (S > 1) {
+        uint8_t out[3 * 48];
+        msm_host_striped<C>(e, points, scalars, n, fmt, scalar_bits, S, out);
+        memcpy(rx, out, fb);
+        memcpy(ry, out + fb, fb);
+        memcpy(rz, out + 2 * fb, fb);
+        return ZKMETAL_SUCCESS;
+    }
     h2d(e, e.w_points, points, (size_t)n * 2 * fb);
     h2d(e, e.w_scalars, scalars, (size_t)n * 32);
     Plan& pl = e.get_plan<C>({n}, {0}, fmt, scalar_bits);
@@ -525,6 +598,12 @@ ZkMetalStatus zkmsm_engine_set_tuning(ZkMetalMSMEngine engine, int window_bits, 
     e.tuning.chunk = chunk;
     e.tuning.glv = glv < 0 ? -1 : (glv ? 1 : 0);
     e.tuning.version++;
+    return ZKMETAL_SUCCESS;
+}
+
+ZkMetalStatus zkmsm_engine_set_stripe(ZkMetalMSMEngine engine, int stripe_log2) {
+    if (!engine || stripe_log2 < 0 || stripe_log2 > 31) return ZKMETAL_ERR_INVALID_INPUT;
+    ENG(engine).stripe_log2 = (uint32_t)stripe_log2;
     return ZKMETAL_SUCCESS;
 }
 

@@ -37,16 +37,31 @@ struct CudaError {
     } while (0)
 
 // Grow-only device buffer.
+// Device buffer that only grows.  With an owner stream `s` it grows through
+// the stream-ordered allocator (the old block returns to the device's memory
+// pool once the stream's earlier work is done), so growing one engine's
+// workspace never waits for other engines' work the way cudaFree does; the
+// new block is ready for work issued on `s` (other streams must wait on s).
 struct DevBuf {
     void* p = nullptr;
     size_t cap = 0;
+    cudaStream_t s = nullptr;
     bool ensure(size_t bytes) {  // true when it had to reallocate
         if (bytes <= cap) return false;
-        if (p) cudaFree(p);
-        p = nullptr;
-        cap = 0;
-        size_t want = bytes + bytes / 8 + 256;
-        ZK_CUDA(cudaMalloc(&p, want));
+        // growth is geometric (at least 1.5x): a buffer that keeps growing is
+        // reallocated a logarithmic number of times
+        size_t want = std::max(bytes + bytes / 8 + 256, cap + cap / 2);
+        if (s) {
+            if (p) ZK_CUDA(cudaFreeAsync(p, s));
+            p = nullptr;
+            cap = 0;
+            ZK_CUDA(cudaMallocAsync(&p, want, s));
+        } else {
+            if (p) cudaFree(p);
+            p = nullptr;
+            cap = 0;
+            ZK_CUDA(cudaMalloc(&p, want));
+        }
         cap = want;
         return true;
     }
@@ -95,6 +110,19 @@ struct Plan {
     // device copies of descs and reduction tasks (uploaded once per plan)
     DevBuf d_descs, d_tasks;
     std::vector<size_t> task_level_off;
+    // forget the host-side shape (device tables are kept for reuse)
+    void clear_host() {
+        descs.clear();
+        total_scalars = entry_bound = 0;
+        nbuckets = nwin_total = 0;
+        sort_maxd = sort_spb = sort_passes = sort_bits = sort_tiles = 0;
+        acc_K.clear();
+        acc_T.clear();
+        acc_Mbound.clear();
+        red_tasks.clear();
+        red_nout.clear();
+        task_level_off.clear();
+    }
 };
 
 // Nearest power-of-two exponent of n (n >= 1).
@@ -188,19 +216,52 @@ class Engine {
 
     // workspace
     DevBuf w_points, w_phi, w_scalars, w_counts, w_offsets, w_cursor, w_ents, w_buckets;
-    DevBuf w_ents2, w_thist;
+    DevBuf w_ents2, w_thist, w_stripe_results;
     DevBuf w_cnt, w_pos, w_tiles, w_totals, w_pkeys[2], w_pvals[2], w_redS[2], w_redW[2];
     DevBuf w_results, w_comb;
     bool comb_ready[2] = {false, false};
     uint32_t* h_results = nullptr;  // pinned
     size_t h_results_cap = 0;
 
+    // Workspace buffers grow on the engine stream; the device's default
+    // memory pool keeps up to 4 GiB of freed blocks for reuse.
+    void bind_workspace_stream() {
+        DevBuf* bufs[] = {&w_points, &w_phi, &w_scalars, &w_counts, &w_offsets, &w_cursor, &w_ents, &w_buckets,
+                          &w_ents2, &w_thist, &w_stripe_results, &w_cnt, &w_pos, &w_tiles, &w_totals,
+                          &w_pkeys[0], &w_pkeys[1], &w_pvals[0], &w_pvals[1], &w_redS[0], &w_redS[1],
+                          &w_redW[0], &w_redW[1], &w_results, &w_comb, &transient.d_descs, &transient.d_tasks};
+        for (DevBuf* b : bufs) b->s = stream;
+        cudaMemPool_t pool;
+        if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+            uint64_t keep = 4ull << 30;
+            cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+        }
+        cudaGetLastError();
+    }
+
     Engine() {
         ZK_CUDA(cudaGetDevice(&device));
         ZK_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+        bind_workspace_stream();
+    }
+    // Second stream and events for host-to-device copies that overlap the
+    // compute stream (striped MSMs from host buffers).
+    cudaStream_t copy_stream = nullptr;
+    std::vector<cudaEvent_t> copy_events;
+    // points per stripe of host-buffer MSMs = 2^stripe_log2 (0: no striping)
+    uint32_t stripe_log2 = 22;
+    void ensure_copy_resources(size_t n_events) {
+        if (!copy_stream) ZK_CUDA(cudaStreamCreateWithFlags(&copy_stream, cudaStreamNonBlocking));
+        while (copy_events.size() < n_events) {
+            cudaEvent_t ev;
+            ZK_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+            copy_events.push_back(ev);
+        }
     }
     ~Engine() {
         drop_graphs();
+        for (auto ev : copy_events) cudaEventDestroy(ev);
+        if (copy_stream) cudaStreamDestroy(copy_stream);
         if (stream) cudaStreamDestroy(stream);
         if (h_results) cudaFreeHost(h_results);
     }
@@ -351,19 +412,46 @@ class Engine {
         }
         std::unique_ptr<Plan> pl(new Plan());
         make_plan<C>(*pl, counts, base_offs, fmt, scalar_bits);
-        std::vector<RedTask> blob;
-        for (auto& v : pl->red_tasks) {
-            pl->task_level_off.push_back(blob.size());
-            blob.insert(blob.end(), v.begin(), v.end());
-        }
-        pl->d_tasks.ensure((blob.size() + 1) * sizeof(RedTask));
-        pl->d_descs.ensure((pl->descs.size() + 1) * sizeof(MsmDesc));
-        ZK_CUDA(cudaMemcpy(pl->d_tasks.p, blob.data(), blob.size() * sizeof(RedTask), cudaMemcpyHostToDevice));
-        ZK_CUDA(cudaMemcpy(pl->d_descs.p, pl->descs.data(), pl->descs.size() * sizeof(MsmDesc),
-                           cudaMemcpyHostToDevice));
+        upload_plan(*pl, false);
         Plan& ref = *pl;
         plan_cache.emplace(key, std::move(pl));
         return ref;
+    }
+
+    // Device tables of a plan (MSM descriptors, reduction tasks); `async`
+    // copies on the engine stream (the host vectors are pageable, so the
+    // copy has left them when the call returns).
+    void upload_plan(Plan& pl, bool async) {
+        std::vector<RedTask> blob;
+        pl.task_level_off.clear();
+        for (auto& v : pl.red_tasks) {
+            pl.task_level_off.push_back(blob.size());
+            blob.insert(blob.end(), v.begin(), v.end());
+        }
+        pl.d_tasks.ensure((blob.size() + 1) * sizeof(RedTask));
+        pl.d_descs.ensure((pl.descs.size() + 1) * sizeof(MsmDesc));
+        if (async) {
+            ZK_CUDA(cudaMemcpyAsync(pl.d_tasks.p, blob.data(), blob.size() * sizeof(RedTask), cudaMemcpyHostToDevice,
+                                    stream));
+            ZK_CUDA(cudaMemcpyAsync(pl.d_descs.p, pl.descs.data(), pl.descs.size() * sizeof(MsmDesc),
+                                    cudaMemcpyHostToDevice, stream));
+        } else {
+            ZK_CUDA(cudaMemcpy(pl.d_tasks.p, blob.data(), blob.size() * sizeof(RedTask), cudaMemcpyHostToDevice));
+            ZK_CUDA(cudaMemcpy(pl.d_descs.p, pl.descs.data(), pl.descs.size() * sizeof(MsmDesc),
+                               cudaMemcpyHostToDevice));
+        }
+    }
+
+    // An uncached plan for shapes that rarely repeat (served batches): built
+    // again in place on every call, its device tables only grow, so steady
+    // state serving neither allocates nor frees.  Valid until the next call.
+    Plan transient;
+    template <class C>
+    Plan& transient_plan(const std::vector<uint32_t>& counts, const std::vector<uint32_t>& base_offs, int fmt) {
+        transient.clear_host();
+        make_plan<C>(transient, counts, base_offs, fmt, 0);
+        upload_plan(transient, true);
+        return transient;
     }
 
     template <class C>

@@ -279,6 +279,9 @@ ZK_DEV void fe_mul(Fe<P>& r, const Fe<P>& a, const Fe<P>& b) {
 #endif
 }
 
+// A square is a product: with 32-bit limbs the CIOS form cannot use the
+// symmetry, and separating product and reduction (to use it) breaks the
+// register pairing that lets each lo/hi pair issue as one instruction.
 template <class P>
 ZK_DEV void fe_sqr(Fe<P>& r, const Fe<P>& a) { fe_mul(r, a, a); }
 

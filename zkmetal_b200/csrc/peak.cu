@@ -99,6 +99,28 @@ __global__ void __launch_bounds__(256) k_fe_mul_peak(uint32_t iters, uint32_t* s
     if (s == 0x12345678u) sink[0] = s;
 }
 
+// Element-wise field operation on n operands (limbs little endian, N words
+// each): op 0 r = a*b (the library's product), 1 r = a^2 (its square),
+// 2 r = a*b by the straight CIOS product (a second implementation).
+template <class P>
+__global__ void __launch_bounds__(128) k_field_op(int op, const uint32_t* __restrict__ a,
+                                                  const uint32_t* __restrict__ b, uint32_t* __restrict__ out,
+                                                  uint32_t n) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    Fe<P> x, y, z;
+#pragma unroll
+    for (int l = 0; l < P::N; l++) {
+        x.v[l] = a[(size_t)i * P::N + l];
+        y.v[l] = b[(size_t)i * P::N + l];
+    }
+    if (op == 0) fe_mul(z, x, y);
+    else if (op == 1) fe_sqr(z, x);
+    else fe_mul_body(z, x, y);
+#pragma unroll
+    for (int l = 0; l < P::N; l++) out[(size_t)i * P::N + l] = z.v[l];
+}
+
 template <class C>
 __global__ void k_sum_results(const uint32_t* __restrict__ in, uint32_t count, uint32_t* __restrict__ out) {
     using P = typename C::Fp;
@@ -199,6 +221,21 @@ extern "C" ZkMetalStatus zkmsm_sum_results_device(int curve, const void* d_resul
     else if (curve == ZKMSM_BLS12_381) k_sum_results<Bls381><<<1, 32, 0, s>>>(in, count, out);
     else return ZKMETAL_ERR_INVALID_INPUT;
     return cudaGetLastError() == cudaSuccess ? ZKMETAL_SUCCESS : ZKMETAL_ERR_GPU_ERROR;
+}
+
+extern "C" ZkMetalStatus zkmsm_field_op(int curve, int op, const void* d_a, const void* d_b, void* d_out,
+                                        uint32_t n) {
+    if (!d_a || !d_b || !d_out || op < 0 || op > 2) return ZKMETAL_ERR_INVALID_INPUT;
+    if (n == 0) return ZKMETAL_SUCCESS;
+    const uint32_t* a = static_cast<const uint32_t*>(d_a);
+    const uint32_t* b = static_cast<const uint32_t*>(d_b);
+    uint32_t* o = static_cast<uint32_t*>(d_out);
+    const unsigned g = (n + 127) / 128;
+    if (curve == ZKMSM_BN254) k_field_op<Bn254Fp><<<g, 128>>>(op, a, b, o, n);
+    else if (curve == ZKMSM_BLS12_381) k_field_op<Bls381Fp><<<g, 128>>>(op, a, b, o, n);
+    else return ZKMETAL_ERR_INVALID_INPUT;
+    if (cudaGetLastError() != cudaSuccess || cudaDeviceSynchronize() != cudaSuccess) return ZKMETAL_ERR_GPU_ERROR;
+    return ZKMETAL_SUCCESS;
 }
 
 extern "C" ZkMetalStatus zkmsm_sum_results(int curve, const uint8_t* results, uint32_t count, uint8_t* out) {

@@ -16,6 +16,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdio>
 #include <atomic>
 #include <chrono>
 #include <condition_variable>
@@ -135,6 +136,9 @@ struct Server {
             // run the batch outside the lock
             int st = ZKMETAL_SUCCESS;
             std::vector<uint8_t> out;
+#ifdef ZKMSM_SERVER_TRACE
+            const auto t_b0 = Clock::now();
+#endif
             try {
                 if (inject_failures.load() > 0 && inject_failures.fetch_sub(1) > 0)
                     throw std::runtime_error("injected batch failure");
@@ -146,12 +150,13 @@ struct Server {
                     boffs.push_back(0);
                     total += r->n;
                 }
-                if (total * 32 > d_cap) {
-                    if (d_scalars) cudaFree(d_scalars);
+                if (total * 32 > d_cap) {  // grows geometrically, in stream order (no device-wide wait)
+                    const uint64_t want = std::max<uint64_t>(total * 36, d_cap + d_cap / 2);
+                    if (d_scalars) ZK_CUDA(cudaFreeAsync(d_scalars, eng->stream));
                     d_scalars = nullptr;
                     d_cap = 0;
-                    ZK_CUDA(cudaMalloc(&d_scalars, total * 32 + total * 4));
-                    d_cap = total * 32 + total * 4;
+                    ZK_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&d_scalars), want, eng->stream));
+                    d_cap = want;
                 }
                 // one host-to-device copy per request into the batch's scalar array
                 uint64_t off = 0;
@@ -166,13 +171,24 @@ struct Server {
                 int fb = curve == ZKMSM_BN254 ? 32 : 48;
                 out.resize(batch.size() * 3 * fb);
                 if (curve == ZKMSM_BN254) {
-                    Plan& pl = eng->get_plan<Bn254>(counts, boffs, fmt);
+                    Plan& pl = eng->transient_plan<Bn254>(counts, boffs, fmt);
                     eng->run_device<Bn254>(pl, tv.points, tv.phi, d_scalars, out.data());
                 } else {
-                    Plan& pl = eng->get_plan<Bls381>(counts, boffs, fmt);
+                    Plan& pl = eng->transient_plan<Bls381>(counts, boffs, fmt);
                     eng->run_device<Bls381>(pl, tv.points, tv.phi, d_scalars, out.data());
                 }
                 for (size_t i = 0; i < batch.size(); i++) memcpy(batch[i]->result, out.data() + i * 3 * fb, 3 * fb);
+#ifdef ZKMSM_SERVER_TRACE
+                {
+                    const auto t_b1 = Clock::now();
+                    double oldest = 0;
+                    for (auto& r : batch)
+                        oldest = std::max(oldest, std::chrono::duration<double, std::milli>(t_b0 - r->t_submit).count());
+                    fprintf(stderr, "trace worker %p curve %d reqs %zu points %llu run %.2f ms oldest wait %.2f ms\n",
+                            (void*)eng.get(), curve, batch.size(), (unsigned long long)total,
+                            std::chrono::duration<double, std::milli>(t_b1 - t_b0).count(), oldest);
+                }
+#endif
             } catch (const CudaError& e) {
                 set_error(std::string("server batch: ") + e.where + ": " + cudaGetErrorString(e.code));
                 cudaGetLastError();

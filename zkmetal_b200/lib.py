@@ -93,6 +93,8 @@ _SIGS = {
     "zkmsm_sum_results": (c_i32, [c_int, c_vp, c_u32, c_vp]),
     "zkmsm_wide_products_per_s": (ctypes.c_double, []),
     "zkmsm_sum_results_device": (c_i32, [c_int, c_vp, c_u32, c_vp, c_vp]),
+    "zkmsm_field_op": (c_i32, [c_int, c_int, c_vp, c_vp, c_vp, c_u32]),
+    "zkmsm_engine_set_stripe": (c_i32, [c_vp, c_int]),
     "zkmsm_bn254_msm_noalloc": (c_i32, [c_vp, c_vp, c_int, c_u32, c_vp, c_vp]),
     "zkmsm_device_alloc": (c_vp, [c_u64]),
     "zkmsm_device_free": (None, [c_vp]),
