@@ -207,10 +207,11 @@ void zkmsm_server_destroy(ZkMsmServer server);
 /* Tuning overrides (0 = automatic): window bits, chunk length, GLV on/off. */
 ZkMetalStatus zkmsm_engine_set_tuning(ZkMetalMSMEngine engine, int window_bits, int chunk, int glv);
 /* NEW: host-buffer MSMs (zkmetal_*_msm and their _fr forms) of at least two
- * stripes of 2^stripe_log2 points are streamed: they run as independent MSMs
- * over consecutive point ranges, each stripe's host-to-device copy overlapping
- * the previous stripe's computation, and the stripe results are added on the
- * device (the same point).  Default 22; 0 turns striping off. */
+ * stripes of 2^stripe_log2 points are streamed: each stripe's host-to-device
+ * copy overlaps the previous stripe's sort and accumulation, every stripe
+ * fills its own bucket array in the whole MSM's window layout, and the arrays
+ * are added and reduced once (the same point).  Default 22; 0 turns striping
+ * off. */
 ZkMetalStatus zkmsm_engine_set_stripe(ZkMetalMSMEngine engine, int stripe_log2);
 
 /* Synthetic inputs on the device (seeded, counter based):

@@ -202,11 +202,11 @@ def test_small_scalar_variants(eng):
 @pytest.mark.parametrize("curve", ["bn254", "bls12_381"])
 @pytest.mark.parametrize("dist", ["uniform", "witness"])
 def test_striped_host_msm_matches_unstriped(eng, oracles, curve, dist):
-    """Host-buffer MSMs streamed in stripes (independent MSMs over consecutive
-    point ranges, the copy of stripe s overlapping the work on stripe s-1, the
-    stripe results added on the device) give the same point as the unstriped
-    MSM and as the oracle; n is no multiple of the stripe, so the last stripe
-    is shorter."""
+    """Host-buffer MSMs streamed in stripes (consecutive point ranges, the
+    copy of stripe s overlapping the work on stripe s-1, one bucket array per
+    stripe, the arrays added and reduced once) give the same point as the
+    unstriped MSM and as the oracle; n is no multiple of the stripe, so the
+    last stripe is shorter."""
     C = R.CURVES[curve]
     E = ENGINES[curve]()
     L = zl.lib()

@@ -59,11 +59,12 @@ static void h2d(Engine& e, DevBuf& buf, const void* src, size_t bytes) {
 }
 
 // Host-buffer MSMs of at least two stripes of 2^stripe_log2 points (engine
-// setting, default 2^22, zkmsm_engine_set_stripe) run as that many
-// independent MSMs over consecutive point ranges: stripe s is copied on the
-// engine's copy stream while stripe s-1 is computed on its compute stream,
-// each stripe picks its own window width, and the stripe results are added on
-// the device.  The sum is the same point as the unstriped MSM.
+// setting, default 2^22, zkmsm_engine_set_stripe) are streamed: stripe s
+// (a consecutive point range) is copied on the engine's copy stream while
+// stripe s-1 is sorted and accumulated on the compute stream.  Every stripe
+// uses the window layout of the whole MSM and fills its own bucket array;
+// the arrays are then added bucket by bucket and reduced once, so the result
+// is the same point as the unstriped MSM.
 static uint32_t stripe_count(const Engine& e, uint32_t n) {
     if (e.stripe_log2 == 0 || e.stripe_log2 > 31) return 1;
     uint32_t s = n >> e.stripe_log2;
@@ -74,21 +75,24 @@ template <class C>
 static void msm_host_striped(Engine& e, const uint8_t* points, const uint8_t* scalars, uint32_t n, int fmt,
                              uint32_t scalar_bits, uint32_t S, uint8_t* out) {
     using P = typename C::Fp;
-    const size_t pb = (size_t)2 * P::N * 4, rw = (size_t)3 * P::N;  // bytes per point, words per result
+    const size_t pb = (size_t)2 * P::N * 4, xs = (size_t)4 * P::N * 4;  // bytes per point, per XYZZ bucket
+    const uint32_t c = e.get_plan<C>({n}, {0}, fmt, scalar_bits).descs[0].c;
     const uint32_t ns = (n + S - 1) / S;
     const uint32_t nl = n - (S - 1) * ns;
     // (a lookup may evict the cache: fetch the first plan again after the second)
-    Plan* pa = &e.get_plan<C>({ns}, {0}, fmt, scalar_bits);
-    Plan* pz = &e.get_plan<C>({nl}, {0}, fmt, scalar_bits);
-    pa = &e.get_plan<C>({ns}, {0}, fmt, scalar_bits);
+    Plan* pa = &e.get_plan<C>({ns}, {0}, fmt, scalar_bits, c);
+    Plan* pz = &e.get_plan<C>({nl}, {0}, fmt, scalar_bits, c);
+    pa = &e.get_plan<C>({ns}, {0}, fmt, scalar_bits, c);
     const bool glv = pa->descs[0].glv;
+    const size_t nb = pa->nbuckets;
+    if (pz->nbuckets != nb) throw std::runtime_error("stripe bucket layouts differ");
     bool grew = e.w_points.ensure((size_t)n * pb + 16);
     grew |= e.w_scalars.ensure((size_t)n * 32 + 16);
     if (glv) grew |= e.w_phi.ensure((size_t)n * pb + 16);
     if (grew) e.drop_graphs();
     e.ensure_workspace<C>(*pa);
     e.ensure_workspace<C>(*pz);
-    e.w_stripe_results.ensure((S + 1) * rw * 4);
+    e.w_stripe_buckets.ensure(S * nb * xs + 16);
     e.ensure_copy_resources(S + 1);
     // buffers (re)allocated in the compute stream's order: the copies wait for that
     ZK_CUDA(cudaEventRecord(e.copy_events[S], e.stream));
@@ -96,7 +100,7 @@ static void msm_host_striped(Engine& e, const uint8_t* points, const uint8_t* sc
     uint8_t* dp = static_cast<uint8_t*>(e.w_points.p);
     uint8_t* ds = static_cast<uint8_t*>(e.w_scalars.p);
     uint8_t* dphi = glv ? static_cast<uint8_t*>(e.w_phi.p) : dp;
-    uint32_t* res = e.w_stripe_results.as<uint32_t>();
+    uint8_t* bk = static_cast<uint8_t*>(e.w_stripe_buckets.p);
     for (uint32_t s = 0; s < S; s++) {
         const size_t off = (size_t)s * ns;
         const uint32_t cnt = s + 1 < S ? ns : nl;
@@ -109,15 +113,12 @@ static void msm_host_striped(Engine& e, const uint8_t* points, const uint8_t* sc
         const uint32_t* sp = reinterpret_cast<const uint32_t*>(dp + off * pb);
         uint32_t* sphi = reinterpret_cast<uint32_t*>(dphi + off * pb);
         if (glv) e.make_phi<C>(sp, cnt, sphi);
-        e.enqueue<C>(s + 1 < S ? *pa : *pz, sp, sphi, reinterpret_cast<const uint32_t*>(ds + off * 32),
-                     res + s * rw);
+        e.enqueue<C>(s + 1 < S ? *pa : *pz, sp, sphi, reinterpret_cast<const uint32_t*>(ds + off * 32), nullptr,
+                     Engine::ENQ_ACC_ONLY, bk + s * nb * xs);
     }
-    const ZkMetalStatus st =
-            zkmsm_sum_results_device(CurveTraits<C>::id == 0 ? ZKMSM_BN254 : ZKMSM_BLS12_381, res, S, res + S * rw,
-                                     e.stream);
-    if (st != ZKMETAL_SUCCESS) throw std::runtime_error("adding the stripe results failed");
-    e.launches++;
-    ZK_CUDA(cudaMemcpyAsync(out, res + S * rw, rw * 4, cudaMemcpyDeviceToHost, e.stream));
+    e.fold_buckets<C>(bk, (uint32_t)nb, S);
+    e.enqueue_reduce<C>(*pz, bk, e.w_results.as<uint32_t>());
+    ZK_CUDA(cudaMemcpyAsync(out, e.w_results.p, 3 * P::N * 4, cudaMemcpyDeviceToHost, e.stream));
     ZK_CUDA(cudaStreamSynchronize(e.stream));
 }
 

@@ -216,7 +216,7 @@ class Engine {
 
     // workspace
     DevBuf w_points, w_phi, w_scalars, w_counts, w_offsets, w_cursor, w_ents, w_buckets;
-    DevBuf w_ents2, w_thist, w_stripe_results;
+    DevBuf w_ents2, w_thist, w_stripe_buckets;
     DevBuf w_cnt, w_pos, w_tiles, w_totals, w_pkeys[2], w_pvals[2], w_redS[2], w_redW[2];
     DevBuf w_results, w_comb;
     bool comb_ready[2] = {false, false};
@@ -227,7 +227,7 @@ class Engine {
     // memory pool keeps up to 4 GiB of freed blocks for reuse.
     void bind_workspace_stream() {
         DevBuf* bufs[] = {&w_points, &w_phi, &w_scalars, &w_counts, &w_offsets, &w_cursor, &w_ents, &w_buckets,
-                          &w_ents2, &w_thist, &w_stripe_results, &w_cnt, &w_pos, &w_tiles, &w_totals,
+                          &w_ents2, &w_thist, &w_stripe_buckets, &w_cnt, &w_pos, &w_tiles, &w_totals,
                           &w_pkeys[0], &w_pkeys[1], &w_pvals[0], &w_pvals[1], &w_redS[0], &w_redS[1],
                           &w_redW[0], &w_redW[1], &w_results, &w_comb, &transient.d_descs, &transient.d_tasks};
         for (DevBuf* b : bufs) b->s = stream;
@@ -269,15 +269,18 @@ class Engine {
     // ------------------------------------------------------------ planning
     template <class C>
     void make_plan(Plan& pl, const std::vector<uint32_t>& counts, const std::vector<uint32_t>& base_offs,
-                   int fmt, uint32_t scalar_bits) const {
-        plan_shape<C>(pl, tuning, counts, base_offs, fmt, scalar_bits);
+                   int fmt, uint32_t scalar_bits, uint32_t window_override = 0) const {
+        plan_shape<C>(pl, tuning, counts, base_offs, fmt, scalar_bits, window_override);
     }
 
     // Pure host planning (no device needed): window widths, bucket layout,
     // chunking of the segmented sums and the reduction tree.
     template <class C>
+    // window_override > 0 fixes every MSM's window width (the stripes of one
+    // striped MSM share one bucket layout).
     static void plan_shape(Plan& pl, const Tuning& tuning, const std::vector<uint32_t>& counts,
-                           const std::vector<uint32_t>& base_offs, int fmt, uint32_t scalar_bits) {
+                           const std::vector<uint32_t>& base_offs, int fmt, uint32_t scalar_bits,
+                           uint32_t window_override = 0) {
         pl.curve = CurveTraits<C>::id;
         uint64_t soff = 0;
         uint32_t boff = 0, woff = 0;
@@ -292,7 +295,8 @@ class Engine {
             uint32_t bits = small ? scalar_bits : (d.glv ? CurveTraits<C>::half_bits : CurveTraits<C>::fr_bits);
             uint64_t epw = (uint64_t)d.n * (d.glv ? 2 : 1);
             uint32_t c = tuning.window_bits > 0 ? (uint32_t)tuning.window_bits : choose_window(epw, bits);
-            if (tuning.window_bits == 0 && d.n && !small) {
+            if (window_override) c = window_override;
+            else if (tuning.window_bits == 0 && d.n && !small) {
                 auto it = tuning.window_table.find({CurveTraits<C>::id * 2 + (int)d.glv, nearest_log2(d.n)});
                 if (it != tuning.window_table.end()) c = (uint32_t)it->second;
             }
@@ -393,12 +397,13 @@ class Engine {
 
     template <class C>
     Plan& get_plan(const std::vector<uint32_t>& counts, const std::vector<uint32_t>& base_offs, int fmt,
-                   uint32_t scalar_bits = 0) {
+                   uint32_t scalar_bits = 0, uint32_t window_override = 0) {
         std::string key;
         auto put = [&](uint64_t v) { key.append(reinterpret_cast<const char*>(&v), sizeof v); };
         put(CurveTraits<C>::id);
         put(fmt);
         put(scalar_bits);
+        put(window_override);
         put((uint64_t)(uint32_t)tuning.window_bits << 32 | (uint32_t)tuning.chunk);
         put((uint64_t)(int64_t)tuning.glv);
         put(tuning.version);
@@ -411,7 +416,7 @@ class Engine {
             plan_cache.clear();
         }
         std::unique_ptr<Plan> pl(new Plan());
-        make_plan<C>(*pl, counts, base_offs, fmt, scalar_bits);
+        make_plan<C>(*pl, counts, base_offs, fmt, scalar_bits, window_override);
         upload_plan(*pl, false);
         Plan& ref = *pl;
         plan_cache.emplace(key, std::move(pl));
@@ -504,9 +509,18 @@ class Engine {
 
     // Curve-specific device work: defined in engine_impl.cuh and instantiated
     // once per curve (inst_bn254.cu, inst_bls381.cu).
+    // flags: ENQ_ACC_ONLY stops after the bucket sums (no window sums, no
+    // result).  bucket_base (default: the engine's bucket array) receives the
+    // bucket sums.
+    static constexpr int ENQ_ACC_ONLY = 1;
     template <class C>
     void enqueue(const Plan& pl, const uint32_t* d_bases, const uint32_t* d_phi, const uint32_t* d_scalars,
-                 uint32_t* d_results);
+                 uint32_t* d_results, int flags = 0, void* bucket_base = nullptr);
+    template <class C>
+    void enqueue_reduce(const Plan& pl, const void* bucket_base, uint32_t* d_results,
+                        std::vector<cudaEvent_t>* ev = nullptr);
+    template <class C>
+    void fold_buckets(void* base, uint32_t nb, uint32_t S);
     template <class C>
     void make_phi(const uint32_t* d_bases, uint64_t n, uint32_t* d_phi);
     template <class C>
@@ -579,7 +593,10 @@ class Engine {
 // (inst_bn254.cu, inst_bls381.cu) so the two curves compile in parallel.
 #define ZKMSM_ENGINE_TEMPLATES(EXT, C)                                                                  \
     EXT template void Engine::enqueue<C>(const Plan&, const uint32_t*, const uint32_t*, const uint32_t*, \
-                                         uint32_t*);                                                    \
+                                         uint32_t*, int, void*);                                        \
+    EXT template void Engine::enqueue_reduce<C>(const Plan&, const void*, uint32_t*,                     \
+                                                std::vector<cudaEvent_t>*);                             \
+    EXT template void Engine::fold_buckets<C>(void*, uint32_t, uint32_t);                               \
     EXT template void Engine::make_phi<C>(const uint32_t*, uint64_t, uint32_t*);                        \
     EXT template void Engine::gen_bases<C>(uint64_t, uint64_t, uint64_t, uint32_t*);                    \
     EXT template void Engine::gen_scalars<C>(uint64_t, uint64_t, uint64_t, int, int, uint32_t*);

@@ -28,14 +28,15 @@ static void scan_u32(Engine& e, uint32_t* d_in_out, uint32_t n, uint32_t* d_tota
 // d_results.  No host synchronisation inside (graph capturable).
 template <class C>
 void Engine::enqueue(const Plan& pl, const uint32_t* d_bases, const uint32_t* d_phi, const uint32_t* d_scalars,
-             uint32_t* d_results) {
+             uint32_t* d_results, int flags, void* bucket_base) {
     using P = typename C::Fp;
     const int nd = (int)pl.descs.size();
     const MsmDesc* dd = pl.d_descs.as<MsmDesc>();
     uint32_t* tot = w_totals.as<uint32_t>();
     auto ev = prof_begin();
     prof_mark(ev, 0);
-    ZK_CUDA(cudaMemsetAsync(w_buckets.p, 0, (size_t)pl.nbuckets * sizeof(Xyzz<P>), stream));
+    Xyzz<P>* buckets = bucket_base ? static_cast<Xyzz<P>*>(bucket_base) : w_buckets.as<Xyzz<P>>();
+    ZK_CUDA(cudaMemsetAsync(buckets, 0, (size_t)pl.nbuckets * sizeof(Xyzz<P>), stream));
     // radix sort of the entries by bucket id; tot[0] = number of entries.
     // The digit pass writes to whichever buffer makes the last pass land in
     // w_ents; slot 63 of w_totals takes the (unused) totals of the scans.
@@ -90,12 +91,12 @@ void Engine::enqueue(const Plan& pl, const uint32_t* d_bases, const uint32_t* d_
             k_acc_l1<C><<<(T + ZKMSM_ACC_THREADS - 1) / ZKMSM_ACC_THREADS, ZKMSM_ACC_THREADS, 0, stream>>>(
                     w_ents.as<uint2>(), d_len, K, d_bases,
                                                              d_phi, w_cnt.as<uint32_t>(),
-                                                             w_buckets.as<Xyzz<P>>(), okeys, ovals);
+                                                             buckets, okeys, ovals);
             launches++;
         } else {
             const Xyzz<P>* ivals = w_pvals[cur ^ 1].as<Xyzz<P>>();
             k_acc_lj<C><<<(T + 255) / 256, 256, 0, stream>>>(keys, ivals, d_len, K, w_cnt.as<uint32_t>(),
-                                                             w_buckets.as<Xyzz<P>>(), okeys, ovals);
+                                                             buckets, okeys, ovals);
             launches++;
         }
         ZK_CUDA(cudaGetLastError());
@@ -105,8 +106,19 @@ void Engine::enqueue(const Plan& pl, const uint32_t* d_bases, const uint32_t* d_
         if (l == 0) prof_mark(ev, 2);
     }
     prof_mark(ev, 3);
-    // bucket reduction
-    const Xyzz<P>* inS = w_buckets.as<Xyzz<P>>();
+    if (!(flags & ENQ_ACC_ONLY)) enqueue_reduce<C>(pl, buckets, d_results, &ev);
+    prof_end(ev);
+}
+
+// Window sums from the buckets by a tree of running sums, then Horner over
+// the windows and affine normalisation into d_results.
+template <class C>
+void Engine::enqueue_reduce(const Plan& pl, const void* bucket_base, uint32_t* d_results,
+                            std::vector<cudaEvent_t>* ev) {
+    using P = typename C::Fp;
+    const int nd = (int)pl.descs.size();
+    const MsmDesc* dd = pl.d_descs.as<MsmDesc>();
+    const Xyzz<P>* inS = static_cast<const Xyzz<P>*>(bucket_base);
     const Xyzz<P>* inW = nullptr;
     int rc = 0;
     for (size_t l = 0; l < pl.red_tasks.size(); l++) {
@@ -123,12 +135,21 @@ void Engine::enqueue(const Plan& pl, const uint32_t* d_bases, const uint32_t* d_
         inW = oW;
         rc ^= 1;
     }
-    prof_mark(ev, 4);
+    if (ev) prof_mark(*ev, 4);
     k_combine<C><<<(nd + 31) / 32, 32, 0, stream>>>(inS, inW, dd, nd, d_results);
     launches++;
     ZK_CUDA(cudaGetLastError());
-    prof_mark(ev, 5);
-    prof_end(ev);
+    if (ev) prof_mark(*ev, 5);
+}
+
+template <class C>
+void Engine::fold_buckets(void* base, uint32_t nb, uint32_t S) {
+    using P = typename C::Fp;
+    if (S > 1 && nb) {
+        k_bucket_fold<C><<<(nb + 127) / 128, 128, 0, stream>>>(static_cast<Xyzz<P>*>(base), nb, S);
+        launches++;
+        ZK_CUDA(cudaGetLastError());
+    }
 }
 
 // endomorphism table for a base array

@@ -678,6 +678,25 @@ __global__ void __launch_bounds__(ZKMSM_ACC_THREADS, ZKMSM_ACC_MINBLOCKS) k_acc_
     }
 }
 
+// Stripes of one MSM (same window layout, S bucket arrays of nb buckets one
+// after another): bucket i of array 0 becomes the sum of bucket i of all S.
+template <class C>
+__global__ void __launch_bounds__(128) k_bucket_fold(Xyzz<typename C::Fp>* __restrict__ b, uint32_t nb,
+                                                     uint32_t S) {
+    using P = typename C::Fp;
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nb) return;
+    Xyzz<P> acc;
+    load_xyzz(acc, b + i);
+#pragma unroll 1
+    for (uint32_t s = 1; s < S; s++) {
+        Xyzz<P> q;
+        load_xyzz(q, b + (size_t)s * nb + i);
+        xyzz_add_ni(acc, q);
+    }
+    store_xyzz(b + i, acc);
+}
+
 // Level >= 2: the same over partial sums (XYZZ + XYZZ additions).
 template <class C>
 __global__ void __launch_bounds__(256) k_acc_lj(const uint32_t* __restrict__ keys,
