@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdio>
+#include <map>
 #include <memory>
 #include <mutex>
 #include <new>
@@ -58,40 +59,53 @@ static void h2d(Engine& e, DevBuf& buf, const void* src, size_t bytes) {
     if (bytes) ZK_CUDA(cudaMemcpyAsync(buf.p, src, bytes, cudaMemcpyHostToDevice, e.stream));
 }
 
-// Host-buffer MSMs of at least two stripes of 2^stripe_log2 points (engine
-// setting, default 2^22, zkmsm_engine_set_stripe) are streamed: stripe s
-// (a consecutive point range) is copied on the engine's copy stream while
-// stripe s-1 is sorted and accumulated on the compute stream.  Every stripe
-// uses the window layout of the whole MSM and fills its own bucket array;
-// the arrays are then added bucket by bucket and reduced once, so the result
-// is the same point as the unstriped MSM.
-static uint32_t stripe_count(const Engine& e, uint32_t n) {
-    if (e.stripe_log2 == 0 || e.stripe_log2 > 31) return 1;
-    uint32_t s = n >> e.stripe_log2;
-    return s < 2 ? 1 : (s > 16 ? 16 : s);
+// Host-buffer MSMs of at least two stripes of f = 2^stripe_log2 points
+// (engine setting, default 2^22, zkmsm_engine_set_stripe) are streamed: the
+// point range is cut into stripes of f/2, f, f, ..., f, rest points (the
+// first one short, so that little of the copy is exposed before work
+// starts); stripe s is copied on the engine's copy stream while stripe s-1 is
+// sorted and accumulated on the compute stream.  Every stripe uses the window
+// layout of the whole MSM and fills its own bucket array; the arrays are then
+// added bucket by bucket and reduced once, so the result is the same point as
+// the unstriped MSM.
+static std::vector<std::pair<uint32_t, uint32_t>> stripe_ranges(const Engine& e, uint32_t n) {
+    std::vector<std::pair<uint32_t, uint32_t>> r;
+    if (e.stripe_log2 < 2 || e.stripe_log2 > 30 || (n >> e.stripe_log2) < 2) return r;
+    const uint32_t f = 1u << e.stripe_log2;
+    uint32_t off = 0, len = f / 2;
+    while (off < n) {
+        uint32_t cnt = std::min(len, n - off);
+        if (r.size() == 15) cnt = n - off;  // at most 16 stripes
+        r.push_back({off, cnt});
+        off += cnt;
+        len = f;
+    }
+    return r;
 }
 
 template <class C>
 static void msm_host_striped(Engine& e, const uint8_t* points, const uint8_t* scalars, uint32_t n, int fmt,
-                             uint32_t scalar_bits, uint32_t S, uint8_t* out) {
+                             uint32_t scalar_bits, const std::vector<std::pair<uint32_t, uint32_t>>& rg,
+                             uint8_t* out) {
     using P = typename C::Fp;
     const size_t pb = (size_t)2 * P::N * 4, xs = (size_t)4 * P::N * 4;  // bytes per point, per XYZZ bucket
+    const uint32_t S = (uint32_t)rg.size();
     const uint32_t c = e.get_plan<C>({n}, {0}, fmt, scalar_bits).descs[0].c;
-    const uint32_t ns = (n + S - 1) / S;
-    const uint32_t nl = n - (S - 1) * ns;
-    // (a lookup may evict the cache: fetch the first plan again after the second)
-    Plan* pa = &e.get_plan<C>({ns}, {0}, fmt, scalar_bits, c);
-    Plan* pz = &e.get_plan<C>({nl}, {0}, fmt, scalar_bits, c);
-    pa = &e.get_plan<C>({ns}, {0}, fmt, scalar_bits, c);
-    const bool glv = pa->descs[0].glv;
-    const size_t nb = pa->nbuckets;
-    if (pz->nbuckets != nb) throw std::runtime_error("stripe bucket layouts differ");
+    // one plan per distinct stripe length; a lookup may evict the cache, so
+    // all are fetched a second time before any is used
+    std::map<uint32_t, Plan*> plans;
+    for (int pass = 0; pass < 2; pass++)
+        for (auto& q : rg) plans[q.second] = &e.get_plan<C>({q.second}, {0}, fmt, scalar_bits, c);
+    const Plan& p0 = *plans[rg[0].second];
+    const bool glv = p0.descs[0].glv;
+    const size_t nb = p0.nbuckets;
+    for (auto& kv : plans)
+        if (kv.second->nbuckets != nb) throw std::runtime_error("stripe bucket layouts differ");
     bool grew = e.w_points.ensure((size_t)n * pb + 16);
     grew |= e.w_scalars.ensure((size_t)n * 32 + 16);
     if (glv) grew |= e.w_phi.ensure((size_t)n * pb + 16);
     if (grew) e.drop_graphs();
-    e.ensure_workspace<C>(*pa);
-    e.ensure_workspace<C>(*pz);
+    for (auto& kv : plans) e.ensure_workspace<C>(*kv.second);
     e.w_stripe_buckets.ensure(S * nb * xs + 16);
     e.ensure_copy_resources(S + 1);
     // buffers (re)allocated in the compute stream's order: the copies wait for that
@@ -102,8 +116,8 @@ static void msm_host_striped(Engine& e, const uint8_t* points, const uint8_t* sc
     uint8_t* dphi = glv ? static_cast<uint8_t*>(e.w_phi.p) : dp;
     uint8_t* bk = static_cast<uint8_t*>(e.w_stripe_buckets.p);
     for (uint32_t s = 0; s < S; s++) {
-        const size_t off = (size_t)s * ns;
-        const uint32_t cnt = s + 1 < S ? ns : nl;
+        const size_t off = rg[s].first;
+        const uint32_t cnt = rg[s].second;
         ZK_CUDA(cudaMemcpyAsync(ds + off * 32, scalars + off * 32, (size_t)cnt * 32, cudaMemcpyHostToDevice,
                                 e.copy_stream));
         ZK_CUDA(cudaMemcpyAsync(dp + off * pb, points + off * pb, (size_t)cnt * pb, cudaMemcpyHostToDevice,
@@ -113,11 +127,11 @@ static void msm_host_striped(Engine& e, const uint8_t* points, const uint8_t* sc
         const uint32_t* sp = reinterpret_cast<const uint32_t*>(dp + off * pb);
         uint32_t* sphi = reinterpret_cast<uint32_t*>(dphi + off * pb);
         if (glv) e.make_phi<C>(sp, cnt, sphi);
-        e.enqueue<C>(s + 1 < S ? *pa : *pz, sp, sphi, reinterpret_cast<const uint32_t*>(ds + off * 32), nullptr,
+        e.enqueue<C>(*plans[cnt], sp, sphi, reinterpret_cast<const uint32_t*>(ds + off * 32), nullptr,
                      Engine::ENQ_ACC_ONLY, bk + s * nb * xs);
     }
     e.fold_buckets<C>(bk, (uint32_t)nb, S);
-    e.enqueue_reduce<C>(*pz, bk, e.w_results.as<uint32_t>());
+    e.enqueue_reduce<C>(p0, bk, e.w_results.as<uint32_t>());
     ZK_CUDA(cudaMemcpyAsync(out, e.w_results.p, 3 * P::N * 4, cudaMemcpyDeviceToHost, e.stream));
     ZK_CUDA(cudaStreamSynchronize(e.stream));
 }
@@ -128,10 +142,10 @@ static ZkMetalStatus msm_host(Engine& e, const uint8_t* points, const uint8_t* s
     using P = typename C::Fp;
     const int fb = P::N * 4;
     if (n == 0 || !points || !scalars || !rx || !ry || !rz) return ZKMETAL_ERR_INVALID_INPUT;
-    const uint32_t S = stripe_count(e, n);
-    if (S > 1) {
+    const auto rg = stripe_ranges(e, n);
+    if (rg.size() > 1) {
         uint8_t out[3 * 48];
-        msm_host_striped<C>(e, points, scalars, n, fmt, scalar_bits, S, out);
+        msm_host_striped<C>(e, points, scalars, n, fmt, scalar_bits, rg, out);
         memcpy(rx, out, fb);
         memcpy(ry, out + fb, fb);
         memcpy(rz, out + 2 * fb, fb);
