@@ -480,7 +480,10 @@ class Engine {
         grew |= w_pvals[0].ensure(m2 * xs + xs);
         grew |= w_pkeys[1].ensure(m3 * 4 + 16);
         grew |= w_pvals[1].ensure(m3 * xs + xs);
-        grew |= w_totals.ensure(64 * 4);
+        if (w_totals.ensure(64 * 4)) {  // new memory holds anything: start the counters at zero
+            grew = true;
+            ZK_CUDA(cudaMemsetAsync(w_totals.p, 0, 64 * 4, stream));
+        }
         size_t r0 = pl.red_nout.empty() ? 1 : pl.red_nout[0];
         for (int i = 0; i < 2; i++) {
             grew |= w_redS[i].ensure(r0 * xs + xs);
