@@ -37,25 +37,27 @@ struct CudaError {
     } while (0)
 
 // Grow-only device buffer.
-// Device buffer that only grows.  With an owner stream `s` it grows through
-// the stream-ordered allocator (the old block returns to the device's memory
-// pool once the stream's earlier work is done), so growing one engine's
-// workspace never waits for other engines' work the way cudaFree does; the
-// new block is ready for work issued on `s` (other streams must wait on s).
+// Device buffer that only grows.  Bound to an owner's stream variable `sp`
+// (the engine's current stream, which follows a caller's stream during
+// calls on it), it grows through the stream-ordered allocator: the old block
+// returns to the device's memory pool once the work already issued on that
+// stream is done, so growing one engine's workspace never waits for other
+// engines' work the way cudaFree does, and the new block is ready for work
+// issued on the same stream (other streams must wait on it).
 struct DevBuf {
     void* p = nullptr;
     size_t cap = 0;
-    cudaStream_t s = nullptr;
+    cudaStream_t* sp = nullptr;
     bool ensure(size_t bytes) {  // true when it had to reallocate
         if (bytes <= cap) return false;
         // growth is geometric (at least 1.5x): a buffer that keeps growing is
         // reallocated a logarithmic number of times
         size_t want = std::max(bytes + bytes / 8 + 256, cap + cap / 2);
-        if (s) {
-            if (p) ZK_CUDA(cudaFreeAsync(p, s));
+        if (sp) {
+            if (p) ZK_CUDA(cudaFreeAsync(p, *sp));
             p = nullptr;
             cap = 0;
-            ZK_CUDA(cudaMallocAsync(&p, want, s));
+            ZK_CUDA(cudaMallocAsync(&p, want, *sp));
         } else {
             if (p) cudaFree(p);
             p = nullptr;
@@ -230,7 +232,7 @@ class Engine {
                           &w_ents2, &w_thist, &w_stripe_buckets, &w_cnt, &w_pos, &w_tiles, &w_totals,
                           &w_pkeys[0], &w_pkeys[1], &w_pvals[0], &w_pvals[1], &w_redS[0], &w_redS[1],
                           &w_redW[0], &w_redW[1], &w_results, &w_comb, &transient.d_descs, &transient.d_tasks};
-        for (DevBuf* b : bufs) b->s = stream;
+        for (DevBuf* b : bufs) b->sp = &stream;
         cudaMemPool_t pool;
         if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
             uint64_t keep = 4ull << 30;
