@@ -458,7 +458,7 @@ def run_ours(args):
     L = zl.lib()
     n = 1 << args.log2n
     eng = MetalMSM()
-    if args.window:
+    if args.window or args.chunk:
         assert L.zkmsm_engine_set_tuning(eng.handle, args.window, args.chunk, -1) == 0
     # inputs: this rank's shard of the N*n-point MSM
     from zkmetal_b200.shard import gather_partials, shard_range
