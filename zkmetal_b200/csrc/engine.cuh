@@ -88,6 +88,9 @@ struct Tuning {
     // zkmsm_autotune or zkmsm_tuning_load
     std::map<std::pair<int, int>, int> window_table;
     uint64_t version = 0;  // bumped whenever the table changes
+    // threads of the level-1 accumulation kernel resident at once on the
+    // device, per curve (0: unknown; then chunks are not wave-aligned)
+    uint32_t acc_wave[2] = {0, 0};
 };
 
 // Host description of one batch run.
@@ -245,6 +248,8 @@ class Engine {
         ZK_CUDA(cudaGetDevice(&device));
         ZK_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
         bind_workspace_stream();
+        tuning.acc_wave[0] = acc_resident_threads<Bn254>();
+        tuning.acc_wave[1] = acc_resident_threads<Bls381>();
     }
     // Second stream and events for host-to-device copies that overlap the
     // compute stream (striped MSMs from host buffers).
@@ -342,6 +347,15 @@ class Engine {
             uint64_t avg = pl.nbuckets ? M / pl.nbuckets : 1;
             uint64_t k = std::min<uint64_t>(std::max<uint64_t>(8, waves8), std::max<uint64_t>(16, 2 * avg));
             K1 = (uint32_t)std::min<uint64_t>(k, 512);
+            // then round the thread count to a whole number of waves of
+            // resident threads: a last, nearly empty wave would run on an
+            // almost idle device for a full chunk time
+            const uint64_t W = tuning.acc_wave[CurveTraits<C>::id];
+            if (W) {
+                const double waves = (double)M / ((double)K1 * (double)W);
+                const uint64_t w = (uint64_t)(waves + 0.5);
+                if (waves >= 1.0 && w >= 1) K1 = (uint32_t)std::max<uint64_t>(8, (M + w * W - 1) / (w * W));
+            }
         }
         uint32_t K = K1;
         for (int lvl = 0; lvl < 40; lvl++) {
@@ -528,6 +542,9 @@ class Engine {
     void fold_buckets(void* base, uint32_t nb, uint32_t S);
     template <class C>
     void make_phi(const uint32_t* d_bases, uint64_t n, uint32_t* d_phi);
+    // resident threads of k_acc_l1<C> on this device (occupancy API)
+    template <class C>
+    uint32_t acc_resident_threads();
     template <class C>
     void gen_bases(uint64_t seed, uint64_t index0, uint64_t n, uint32_t* d_out);
     template <class C>
@@ -603,6 +620,7 @@ class Engine {
                                                 std::vector<cudaEvent_t>*);                             \
     EXT template void Engine::fold_buckets<C>(void*, uint32_t, uint32_t);                               \
     EXT template void Engine::make_phi<C>(const uint32_t*, uint64_t, uint32_t*);                        \
+    EXT template uint32_t Engine::acc_resident_threads<C>();                                              \
     EXT template void Engine::gen_bases<C>(uint64_t, uint64_t, uint64_t, uint32_t*);                    \
     EXT template void Engine::gen_scalars<C>(uint64_t, uint64_t, uint64_t, int, int, uint32_t*);
 

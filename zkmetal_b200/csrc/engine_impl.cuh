@@ -162,6 +162,17 @@ void Engine::make_phi(const uint32_t* d_bases, uint64_t n, uint32_t* d_phi) {
 }
 
 template <class C>
+uint32_t Engine::acc_resident_threads() {
+    int per_sm = 0, sms = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_acc_l1<C>, ZKMSM_ACC_THREADS, 0) != cudaSuccess ||
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return (uint32_t)(per_sm * sms * ZKMSM_ACC_THREADS);
+}
+
+template <class C>
 void Engine::gen_bases(uint64_t seed, uint64_t index0, uint64_t n, uint32_t* d_out) {
     using P = typename C::Fp;
     int ci = CurveTraits<C>::id;
