@@ -85,8 +85,8 @@ ZK_DEV void xyzz_dbl_affine(Xyzz<P>& r, const Affine<P>& a) {
     r.zzz = w;
 }
 
-// r = 2a (dbl-2008-s-1)
-template <class P>
+// r = 2a (dbl-2008-s-1); INL: products inline
+template <class P, bool INL = false>
 ZK_DEV void xyzz_dbl(Xyzz<P>& r, const Xyzz<P>& a) {
     if (xyzz_is_id(a) || fe_is_zero(a.y)) {
         xyzz_set_id(r);
@@ -94,23 +94,23 @@ ZK_DEV void xyzz_dbl(Xyzz<P>& r, const Xyzz<P>& a) {
     }
     Fe<P> u, v, w, s, m, t;
     fe_dbl(u, a.y);
-    fe_sqr(v, u);
-    fe_mul(w, u, v);
-    fe_mul(s, a.x, v);
-    fe_sqr(m, a.x);
+    fe_mul_x<INL>(v, u, u);
+    fe_mul_x<INL>(w, u, v);
+    fe_mul_x<INL>(s, a.x, v);
+    fe_mul_x<INL>(m, a.x, a.x);
     fe_dbl(t, m);
     fe_add(m, m, t);
-    fe_sqr(t, m);
+    fe_mul_x<INL>(t, m, m);
     fe_sub(t, t, s);
     Fe<P> x3;
     fe_sub(x3, t, s);
     fe_sub(t, s, x3);
-    fe_mul(t, m, t);
-    fe_mul(s, w, a.y);
+    fe_mul_x<INL>(t, m, t);
+    fe_mul_x<INL>(s, w, a.y);
     fe_sub(r.y, t, s);
     r.x = x3;
-    fe_mul(r.zz, v, a.zz);
-    fe_mul(r.zzz, w, a.zzz);
+    fe_mul_x<INL>(r.zz, v, a.zz);
+    fe_mul_x<INL>(r.zzz, w, a.zzz);
 }
 
 // acc += (x, y) with (x, y) affine and not the identity (madd-2008-s).
@@ -152,7 +152,8 @@ ZK_DEV void xyzz_add_affine(Xyzz<P>& acc, const Affine<P>& q) {
 }
 
 // acc += b, both XYZZ (add-2008-s)
-template <class P>
+// INL: products inline
+template <class P, bool INL = false>
 ZK_DEV void xyzz_add(Xyzz<P>& acc, const Xyzz<P>& b) {
     if (xyzz_is_id(b)) return;
     if (xyzz_is_id(acc)) {
@@ -160,10 +161,10 @@ ZK_DEV void xyzz_add(Xyzz<P>& acc, const Xyzz<P>& b) {
         return;
     }
     Fe<P> u1, u2, s1, s2;
-    fe_mul(u1, acc.x, b.zz);     // U1 = X1*ZZ2
-    fe_mul(u2, b.x, acc.zz);     // U2 = X2*ZZ1
-    fe_mul(s1, acc.y, b.zzz);    // S1 = Y1*ZZZ2
-    fe_mul(s2, b.y, acc.zzz);    // S2 = Y2*ZZZ1
+    fe_mul_x<INL>(u1, acc.x, b.zz);     // U1 = X1*ZZ2
+    fe_mul_x<INL>(u2, b.x, acc.zz);     // U2 = X2*ZZ1
+    fe_mul_x<INL>(s1, acc.y, b.zzz);    // S1 = Y1*ZZZ2
+    fe_mul_x<INL>(s2, b.y, acc.zzz);    // S2 = Y2*ZZZ1
     fe_sub(u2, u2, u1);          // P
     fe_sub(s2, s2, s1);          // R
     if (fe_is_zero(u2)) {
@@ -172,22 +173,22 @@ ZK_DEV void xyzz_add(Xyzz<P>& acc, const Xyzz<P>& b) {
         return;
     }
     Fe<P> pp, ppp, t;
-    fe_sqr(pp, u2);
-    fe_mul(ppp, u2, pp);
-    fe_mul(u1, u1, pp);          // Q = U1*PP
-    fe_sqr(t, s2);
+    fe_mul_x<INL>(pp, u2, u2);
+    fe_mul_x<INL>(ppp, u2, pp);
+    fe_mul_x<INL>(u1, u1, pp);          // Q = U1*PP
+    fe_mul_x<INL>(t, s2, s2);
     fe_sub(t, t, ppp);
     fe_sub(t, t, u1);
     fe_sub(t, t, u1);            // X3
     fe_sub(u1, u1, t);
-    fe_mul(u1, s2, u1);
-    fe_mul(s1, s1, ppp);
+    fe_mul_x<INL>(u1, s2, u1);
+    fe_mul_x<INL>(s1, s1, ppp);
     fe_sub(acc.y, u1, s1);       // Y3 = R(Q - X3) - S1*PPP
     acc.x = t;
-    fe_mul(acc.zz, acc.zz, b.zz);
-    fe_mul(acc.zz, acc.zz, pp);
-    fe_mul(acc.zzz, acc.zzz, b.zzz);
-    fe_mul(acc.zzz, acc.zzz, ppp);
+    fe_mul_x<INL>(acc.zz, acc.zz, b.zz);
+    fe_mul_x<INL>(acc.zz, acc.zz, pp);
+    fe_mul_x<INL>(acc.zzz, acc.zzz, b.zzz);
+    fe_mul_x<INL>(acc.zzz, acc.zzz, ppp);
 }
 
 template <class P>

@@ -126,9 +126,13 @@ void Engine::enqueue_reduce(const Plan& pl, const void* bucket_base, uint32_t* d
         const RedTask* tk = pl.d_tasks.as<RedTask>() + pl.task_level_off[l];
         Xyzz<P>* oS = w_redS[rc].as<Xyzz<P>>();
         Xyzz<P>* oW = w_redW[rc].as<Xyzz<P>>();
-        k_reduce_level<C><<<(nout + 127) / 128, 128, 0, stream>>>(inS, inW, tk, (int)pl.red_tasks[l].size(),
-                                                                 nout, pl.red_L,
-                                                                 (uint32_t)l * pl.red_log2L, oS, oW);
+        if (nout <= RED_INLINE_MAX_NODES)
+            k_reduce_level<C, true><<<(nout + 127) / 128, 128, 0, stream>>>(inS, inW, tk, (int)pl.red_tasks[l].size(),
+                                                                           nout, pl.red_L,
+                                                                           (uint32_t)l * pl.red_log2L, oS, oW);
+        else
+            k_reduce_level<C, false><<<(nout + 127) / 128, 128, 0, stream>>>(
+                    inS, inW, tk, (int)pl.red_tasks[l].size(), nout, pl.red_L, (uint32_t)l * pl.red_log2L, oS, oW);
         launches++;
         ZK_CUDA(cudaGetLastError());
         inS = oS;

@@ -279,6 +279,23 @@ ZK_DEV void fe_mul(Fe<P>& r, const Fe<P>& a, const Fe<P>& b) {
 #endif
 }
 
+// Product whose form is fixed at compile time: out of line (the default:
+// one shared copy per kernel, small code for throughput kernels) or inline
+// (the compiler may overlap independent products: for latency-bound kernels
+// that run few threads, such as the top of the bucket reduction).
+template <bool INL, class P>
+ZK_DEV void fe_mul_x(Fe<P>& r, const Fe<P>& a, const Fe<P>& b) {
+    if (INL) {
+#if ZKMSM_MUL_EO
+        fe_mul_body_eo(r, a, b);
+#else
+        fe_mul_body(r, a, b);
+#endif
+    } else {
+        fe_mul(r, a, b);
+    }
+}
+
 // A square is a product: with 32-bit limbs the CIOS form cannot use the
 // symmetry, and separating product and reduction (to use it) breaks the
 // register pairing that lets each lo/hi pair issue as one instruction.

@@ -765,7 +765,9 @@ ZK_DEV int find_task(const RedTask* __restrict__ t, int nt, uint32_t g) {
     return lo;
 }
 
-template <class C>
+// INL: inline products, for the top levels, whose few threads are
+// latency-bound (a lone thread's out-of-line products cannot overlap).
+template <class C, bool INL>
 __global__ void __launch_bounds__(128) k_reduce_level(const Xyzz<typename C::Fp>* __restrict__ inS,
                                                       const Xyzz<typename C::Fp>* __restrict__ inW,
                                                       const RedTask* __restrict__ tasks, int ntasks,
@@ -785,19 +787,19 @@ __global__ void __launch_bounds__(128) k_reduce_level(const Xyzz<typename C::Fp>
 #pragma unroll 1
     for (int s = (int)cnt - 1; s >= 1; s--) {
         load_xyzz(q, inS + c0 + s);
-        xyzz_add(run, q);
-        xyzz_add(x, run);
+        xyzz_add<P, INL>(run, q);
+        xyzz_add<P, INL>(x, run);
     }
     load_xyzz(q, inS + c0);
-    xyzz_add(run, q);
+    xyzz_add<P, INL>(run, q);
     store_xyzz(outS + g, run);
 #pragma unroll 1
-    for (uint32_t d = 0; d < log2span; d++) xyzz_dbl(x, x);
+    for (uint32_t d = 0; d < log2span; d++) xyzz_dbl<P, INL>(x, x);
     if (inW != nullptr) {
 #pragma unroll 1
         for (uint32_t s = 0; s < cnt; s++) {
             load_xyzz(q, inW + c0 + s);
-            xyzz_add(x, q);
+            xyzz_add<P, INL>(x, q);
         }
     }
     store_xyzz(outW + g, x);
@@ -826,12 +828,12 @@ __global__ void k_combine(const Xyzz<typename C::Fp>* __restrict__ rootS,
     for (int w = (int)d.nwin - 1; w >= 0; w--) {
         if (w != (int)d.nwin - 1) {
 #pragma unroll 1
-            for (uint32_t b = 0; b < d.c; b++) xyzz_dbl(acc, acc);
+            for (uint32_t b = 0; b < d.c; b++) xyzz_dbl<P, true>(acc, acc);  // one thread: inline products
         }
         load_xyzz(q, rootS + d.win_off + w);
-        xyzz_add(acc, q);
+        xyzz_add<P, true>(acc, q);
         load_xyzz(q, rootW + d.win_off + w);
-        xyzz_add(acc, q);
+        xyzz_add<P, true>(acc, q);
     }
     Affine<P> a;
     xyzz_to_affine_ni(a, acc);

@@ -213,7 +213,7 @@ extern "C" ZkMetalStatus zkmsm_bn254_msm_noalloc(const void* d_points, const voi
     for (int l = 0; l < RED_LEVELS; l++) {
         nodes = (nodes + RED_L - 1) / RED_L;
         uint32_t nout = nodes * NWIN;
-        k_reduce_level<C><<<(nout + 127) / 128, 128, 0, s>>>(inS, inW, dt + l * NWIN, NWIN, nout, RED_L,
+        k_reduce_level<C, false><<<(nout + 127) / 128, 128, 0, s>>>(inS, inW, dt + l * NWIN, NWIN, nout, RED_L,
                                                              (uint32_t)l * RED_LOG2L, rS[l & 1], rW[l & 1]);
         inS = rS[l & 1];
         inW = rW[l & 1];

@@ -40,6 +40,10 @@ constexpr uint32_t SORT_ETILE = 4096;
 constexpr uint32_t SORT_ETHREADS = 256;
 constexpr uint32_t SORT_MAX_BINS = 256;
 
+// Bucket-reduction levels with at most this many output nodes run the
+// inline-product kernel (few threads: latency-bound).
+constexpr uint32_t RED_INLINE_MAX_NODES = 32768;
+
 struct RedTask {
     uint32_t in_off;   // first child node
     uint32_t n_in;     // children
