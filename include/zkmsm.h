@@ -206,12 +206,13 @@ void zkmsm_server_destroy(ZkMsmServer server);
 
 /* Tuning overrides (0 = automatic): window bits, chunk length, GLV on/off. */
 ZkMetalStatus zkmsm_engine_set_tuning(ZkMetalMSMEngine engine, int window_bits, int chunk, int glv);
-/* NEW: host-buffer MSMs (zkmetal_*_msm and their _fr forms) of at least two
- * stripes of 2^stripe_log2 points are streamed: each stripe's host-to-device
- * copy overlaps the previous stripe's sort and accumulation, every stripe
- * fills its own bucket array in the whole MSM's window layout, and the arrays
- * are added and reduced once (the same point).  Default 22; 0 turns striping
- * off. */
+/* NEW: host-buffer MSMs (zkmetal_*_msm and their _fr forms) are streamed in
+ * stripes (consecutive point ranges growing 1.6x per stripe up to 2^stripe_log2
+ * points): each stripe's host-to-device copy overlaps the previous stripe's
+ * sort and accumulation, every stripe fills its own bucket array in the whole
+ * MSM's window layout, and the arrays are added and reduced once (the same
+ * point).  -1 (default): automatic, largest stripe half of n's next power of
+ * two, only for n >= 2^22; 0: off; 2..30: fixed. */
 ZkMetalStatus zkmsm_engine_set_stripe(ZkMetalMSMEngine engine, int stripe_log2);
 
 /* Synthetic inputs on the device (seeded, counter based):

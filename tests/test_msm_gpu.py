@@ -216,7 +216,7 @@ def test_striped_host_msm_matches_unstriped(eng, oracles, curve, dist):
     sb = np.frombuffer(to_host(s), dtype=np.uint8).copy()
     fn = L.zkmetal_bn254_msm_fr if curve == "bn254" else L.zkmetal_bls12_381_g1_msm_fr
     outs = []
-    for stripe_log2 in (0, 12, 11, 12):
+    for stripe_log2 in (0, 12, 11, 13):
         check(L.zkmsm_engine_set_stripe(E.handle, stripe_log2))
         rx, ry, rz = (ctypes.create_string_buffer(C.fp_bytes) for _ in range(3))
         check(fn(E.handle, pb.ctypes.data, sb.ctypes.data, n, rx, ry, rz))
@@ -226,6 +226,8 @@ def test_striped_host_msm_matches_unstriped(eng, oracles, curve, dist):
     orc = ref if ref is not None else cm
     assert jac_to_affine_bytes(C, outs[0]) == oracle_msm(orc, curve, pb.tobytes(), sb.tobytes(), n, zl.SCALAR_MONT)
     assert L.zkmsm_engine_set_stripe(E.handle, 40) == zl.ERR_INVALID_INPUT
+    assert L.zkmsm_engine_set_stripe(E.handle, -2) == zl.ERR_INVALID_INPUT
+    check(L.zkmsm_engine_set_stripe(E.handle, -1))
     E.close()
 
 

@@ -59,26 +59,36 @@ static void h2d(Engine& e, DevBuf& buf, const void* src, size_t bytes) {
     if (bytes) ZK_CUDA(cudaMemcpyAsync(buf.p, src, bytes, cudaMemcpyHostToDevice, e.stream));
 }
 
-// Host-buffer MSMs of at least two stripes of f = 2^stripe_log2 points
-// (engine setting, default 2^22, zkmsm_engine_set_stripe) are streamed: the
-// point range is cut into stripes of f/2, f, f, ..., f, rest points (the
-// first one short, so that little of the copy is exposed before work
-// starts); stripe s is copied on the engine's copy stream while stripe s-1 is
+// Host-buffer MSMs of at least two stripes of f points (engine setting
+// zkmsm_engine_set_stripe: f = 2^stripe_log2, or by default half of n's
+// next power of two when n >= 2^22) are streamed: the
+// point range is cut into stripes that start at f/4 points and grow by 1.6x
+// up to f (a short first stripe exposes little of the copy before work
+// starts; a stripe's compute, ~3 ns per BN254 point, covers the copy of the
+// next, 1.6x longer one at ~1.8 ns per point); stripe s is copied on the
+// engine's copy stream while stripe s-1 is
 // sorted and accumulated on the compute stream.  Every stripe uses the window
 // layout of the whole MSM and fills its own bucket array; the arrays are then
 // added bucket by bucket and reduced once, so the result is the same point as
 // the unstriped MSM.
 static std::vector<std::pair<uint32_t, uint32_t>> stripe_ranges(const Engine& e, uint32_t n) {
     std::vector<std::pair<uint32_t, uint32_t>> r;
-    if (e.stripe_log2 < 2 || e.stripe_log2 > 30 || (n >> e.stripe_log2) < 2) return r;
-    const uint32_t f = 1u << e.stripe_log2;
-    uint32_t off = 0, len = f / 2;
+    int lg = e.stripe_log2;
+    if (lg < 0) {  // automatic
+        if (n < (1u << 22)) return r;
+        lg = 0;
+        while ((1ull << lg) < n) lg++;
+        lg -= 1;
+    }
+    if (lg < 2 || lg > 30 || (n >> lg) < 1) return r;
+    const uint32_t f = 1u << lg;
+    uint32_t off = 0, len = std::max(f / 4, 1u);
     while (off < n) {
         uint32_t cnt = std::min(len, n - off);
         if (r.size() == 15) cnt = n - off;  // at most 16 stripes
         r.push_back({off, cnt});
         off += cnt;
-        len = f;
+        len = (uint32_t)std::min<uint64_t>(f, (uint64_t)len * 8 / 5 + 1);
     }
     return r;
 }
@@ -617,8 +627,8 @@ ZkMetalStatus zkmsm_engine_set_tuning(ZkMetalMSMEngine engine, int window_bits, 
 }
 
 ZkMetalStatus zkmsm_engine_set_stripe(ZkMetalMSMEngine engine, int stripe_log2) {
-    if (!engine || stripe_log2 < 0 || stripe_log2 > 31) return ZKMETAL_ERR_INVALID_INPUT;
-    ENG(engine).stripe_log2 = (uint32_t)stripe_log2;
+    if (!engine || stripe_log2 < -1 || stripe_log2 > 30) return ZKMETAL_ERR_INVALID_INPUT;
+    ENG(engine).stripe_log2 = stripe_log2;
     return ZKMETAL_SUCCESS;
 }
 

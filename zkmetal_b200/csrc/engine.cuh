@@ -255,8 +255,9 @@ class Engine {
     // compute stream (striped MSMs from host buffers).
     cudaStream_t copy_stream = nullptr;
     std::vector<cudaEvent_t> copy_events;
-    // points per stripe of host-buffer MSMs = 2^stripe_log2 (0: no striping)
-    uint32_t stripe_log2 = 22;
+    // largest stripe of streamed host-buffer MSMs: 2^stripe_log2 points;
+    // -1: automatic (half of n's next power of two, for n >= 2^22); 0: off
+    int stripe_log2 = -1;
     void ensure_copy_resources(size_t n_events) {
         if (!copy_stream) ZK_CUDA(cudaStreamCreateWithFlags(&copy_stream, cudaStreamNonBlocking));
         while (copy_events.size() < n_events) {
