@@ -182,6 +182,7 @@ class Engine {
     Tuning tuning;
     int device = 0;
     uint64_t launches = 0;  // kernels launched by this engine (for reporting)
+    uint64_t workspace_growths = 0;  // times ensure_workspace had to reallocate
 
     // Optional per-phase timing with CUDA events on the engine's stream:
     // phases 0 scalar prep + sort, 1 level-1 accumulation, 2 later
@@ -229,7 +230,8 @@ class Engine {
     size_t h_results_cap = 0;
 
     // Workspace buffers grow on the engine stream; the device's default
-    // memory pool keeps up to 4 GiB of freed blocks for reuse.
+    // memory pool keeps at least 4 GiB of freed blocks for reuse (a larger
+    // setting, e.g. a server's reservation, is left as it is).
     void bind_workspace_stream() {
         DevBuf* bufs[] = {&w_points, &w_phi, &w_scalars, &w_counts, &w_offsets, &w_cursor, &w_ents, &w_buckets,
                           &w_ents2, &w_thist, &w_stripe_buckets, &w_cnt, &w_pos, &w_tiles, &w_totals,
@@ -238,8 +240,9 @@ class Engine {
         for (DevBuf* b : bufs) b->sp = &stream;
         cudaMemPool_t pool;
         if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
-            uint64_t keep = 4ull << 30;
-            cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+            uint64_t keep = 4ull << 30, cur = 0;
+            cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &cur);
+            if (cur < keep) cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
         }
         cudaGetLastError();
     }
@@ -510,7 +513,10 @@ class Engine {
         // scan tile sums for the longest scanned array (no allocation inside enqueue)
         grew |= w_tiles.ensure(((std::max<uint64_t>(std::max<uint64_t>(pl.nbuckets, tmax), hsz) + 2047) / 2048 + 2) *
                                4);
-        if (grew) drop_graphs();  // captured graphs hold the old addresses
+        if (grew) {
+            drop_graphs();  // captured graphs hold the old addresses
+            workspace_growths++;
+        }
     }
 
     // ------------------------------------------------------------ graphs

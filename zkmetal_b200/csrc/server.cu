@@ -57,6 +57,9 @@ struct Request {
     uint8_t result[3 * 48];
 };
 
+// batches of at most this many points run on a worker's high-priority stream
+constexpr uint64_t SMALL_BATCH_POINTS = 1ull << 20;
+
 struct Server {
     TableView tables[2];
     bool has_table[2] = {false, false};
@@ -73,6 +76,7 @@ struct Server {
     uint64_t batches = 0, completed = 0, failed = 0, max_batch = 0;
     std::vector<double> latencies_ms;
     int device = 0;
+    const Clock::time_point t_created = Clock::now();
     // host-side fault injection for tests: fail the next k batches
     std::atomic<int> inject_failures{0};
 
@@ -93,6 +97,18 @@ struct Server {
         }
         uint32_t* d_scalars = nullptr;
         size_t d_cap = 0;
+        // small batches run on a high-priority stream: their blocks get SMs
+        // as soon as blocks of other workers' large batches finish, instead
+        // of queueing behind whole kernels
+        cudaStream_t own = eng->stream, hi = nullptr;
+        {
+            int lo_pri = 0, hi_pri = 0;
+            if (cudaDeviceGetStreamPriorityRange(&lo_pri, &hi_pri) != cudaSuccess ||
+                cudaStreamCreateWithPriority(&hi, cudaStreamNonBlocking, hi_pri) != cudaSuccess) {
+                cudaGetLastError();
+                hi = nullptr;
+            }
+        }
         for (;;) {
             std::vector<std::shared_ptr<Request>> batch;
             uint64_t charged = 0;
@@ -150,6 +166,8 @@ struct Server {
                     boffs.push_back(0);
                     total += r->n;
                 }
+                // the previous batch has completed on whichever stream it used
+                eng->stream = (hi && total <= SMALL_BATCH_POINTS) ? hi : own;
                 if (total * 32 > d_cap) {  // grows geometrically, in stream order (no device-wide wait)
                     const uint64_t want = std::max<uint64_t>(total * 36, d_cap + d_cap / 2);
                     if (d_scalars) ZK_CUDA(cudaFreeAsync(d_scalars, eng->stream));
@@ -184,9 +202,13 @@ struct Server {
                     double oldest = 0;
                     for (auto& r : batch)
                         oldest = std::max(oldest, std::chrono::duration<double, std::milli>(t_b0 - r->t_submit).count());
-                    fprintf(stderr, "trace worker %p curve %d reqs %zu points %llu run %.2f ms oldest wait %.2f ms\n",
-                            (void*)eng.get(), curve, batch.size(), (unsigned long long)total,
-                            std::chrono::duration<double, std::milli>(t_b1 - t_b0).count(), oldest);
+                    fprintf(stderr,
+                            "trace t %.3f worker %p curve %d reqs %zu points %llu run %.2f ms oldest wait %.2f ms "
+                            "growths %llu\n",
+                            std::chrono::duration<double>(t_b0 - t_created).count(), (void*)eng.get(), curve,
+                            batch.size(), (unsigned long long)total,
+                            std::chrono::duration<double, std::milli>(t_b1 - t_b0).count(), oldest,
+                            (unsigned long long)eng->workspace_growths);
                 }
 #endif
             } catch (const CudaError& e) {
@@ -217,7 +239,9 @@ struct Server {
             cv_done.notify_all();
             cv_work.notify_all();
         }
+        eng->stream = own;
         if (d_scalars) cudaFree(d_scalars);
+        if (hi) cudaStreamDestroy(hi);
         (void)w;
     }
 };
@@ -244,13 +268,39 @@ ZkMetalStatus zkmsm_server_create(ZkMsmTable bn254_table, ZkMsmTable bls12_381_t
         s->has_table[1] = true;
     }
     cudaGetDevice(&s->device);
+    s->max_batch_points = max_batch_points ? max_batch_points : (1ull << 24);
+    // Reserve workspace memory in the device's memory pool.  Engines grow
+    // their workspaces through the stream-ordered allocator; a growth that
+    // has to map new physical memory (gigabytes for a large batch of many
+    // medium MSMs) held up the other workers' batches for a few hundred
+    // milliseconds.  Memory reserved once and kept by the pool is handed out
+    // without mapping.
+    {
+        size_t fr = 0, tot = 0;
+        cudaMemPool_t pool;
+        if (cudaMemGetInfo(&fr, &tot) == cudaSuccess && cudaDeviceGetDefaultMemPool(&pool, s->device) == cudaSuccess) {
+            const uint64_t want =
+                    std::min<uint64_t>((uint64_t)workers * s->max_batch_points * 384 + (1ull << 30), fr / 4);
+            uint64_t thr = 0;
+            cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+            if (thr < want) {
+                thr = want;
+                cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+            }
+            void* p = nullptr;
+            if (cudaMallocAsync(&p, want, 0) == cudaSuccess) {
+                cudaFreeAsync(p, 0);
+                cudaStreamSynchronize(0);
+            }
+        }
+        cudaGetLastError();
+    }
     if (hbm_budget_bytes == 0) {
         size_t fr = 0, tot = 0;
         if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) return ZKMETAL_ERR_GPU_ERROR;
         hbm_budget_bytes = fr / 10 * 7;  // leave room for the engines' own growth
     }
     s->budget = hbm_budget_bytes;
-    s->max_batch_points = max_batch_points ? max_batch_points : (1ull << 24);
     Server* sp = s.get();
     for (int w = 0; w < workers; w++) s->workers.emplace_back([sp, w] { sp->worker_main(w); });
     *out = s.release();
