@@ -154,3 +154,22 @@ def test_server_admission_cancel_and_injected_failure(eng, tables):
         assert srv.stats()["failed"] == 1
     finally:
         srv.close()
+
+
+def test_server_large_batch_matches_plain(eng):
+    """A batch above the small-batch limit (2^20 points) runs on the worker's
+    normal-priority stream; its results match plain MSMs of the same scalars."""
+    e = eng["bn254"]
+    T = (1 << 20) + 4096
+    p, _ = gen_inputs(e, "bn254", 350, T, "uniform", zl.SCALAR_MONT)
+    table = CommitmentTable(e, p.data_ptr(), on_device=True, n=T)
+    srv = CommitmentServer(table, None, workers=1)
+    try:
+        sc = scalars_host(e, "bn254", 351, T, "witness")
+        ids = [srv.submit(zl.BN254, sc[: n * 32], zl.SCALAR_MONT) for n in (T, 1000, T - 5)]
+        res = [srv.wait(i)[0] for i in ids]
+        for (n, r) in zip((T, 1000, T - 5), res):
+            assert r.x + r.y + r.z == plain(e, "bn254", p, sc, n), n
+    finally:
+        srv.close()
+        table.close()

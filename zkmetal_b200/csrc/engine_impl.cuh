@@ -88,7 +88,8 @@ void Engine::enqueue(const Plan& pl, const uint32_t* d_bases, const uint32_t* d_
         uint32_t* okeys = w_pkeys[cur].as<uint32_t>();
         Xyzz<P>* ovals = w_pvals[cur].as<Xyzz<P>>();
         if (l == 0) {
-            k_acc_l1<C><<<(T + ZKMSM_ACC_THREADS - 1) / ZKMSM_ACC_THREADS, ZKMSM_ACC_THREADS, 0, stream>>>(
+            constexpr int AT = AccLaunch<C>::THREADS;
+            k_acc_l1<C><<<(T + AT - 1) / AT, AT, 0, stream>>>(
                     w_ents.as<uint2>(), d_len, K, d_bases,
                                                              d_phi, w_cnt.as<uint32_t>(),
                                                              buckets, okeys, ovals);
@@ -168,12 +169,13 @@ void Engine::make_phi(const uint32_t* d_bases, uint64_t n, uint32_t* d_phi) {
 template <class C>
 uint32_t Engine::acc_resident_threads() {
     int per_sm = 0, sms = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_acc_l1<C>, ZKMSM_ACC_THREADS, 0) != cudaSuccess ||
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_acc_l1<C>, AccLaunch<C>::THREADS, 0) !=
+                cudaSuccess ||
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) {
         cudaGetLastError();
         return 0;
     }
-    return (uint32_t)(per_sm * sms * ZKMSM_ACC_THREADS);
+    return (uint32_t)(per_sm * sms * AccLaunch<C>::THREADS);
 }
 
 template <class C>

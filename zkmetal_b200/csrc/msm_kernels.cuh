@@ -617,14 +617,20 @@ static __global__ void __launch_bounds__(256) k_chunk_count(const uint32_t* __re
 }
 
 // Level 1: chunks of the sorted entry list, mixed additions of gathered bases.
-#ifndef ZKMSM_ACC_MINBLOCKS
-#define ZKMSM_ACC_MINBLOCKS 1
-#endif
-#ifndef ZKMSM_ACC_THREADS
-#define ZKMSM_ACC_THREADS 256
-#endif
+// Launch shape of k_acc_l1 per curve: BN254 fits two 256-thread blocks per
+// SM at its natural 114 registers; BLS12-381 (158 registers unbounded) is
+// held to 128 registers for two blocks per SM, 8% faster despite a few
+// spilled bytes (measured at 2^22).
 template <class C>
-__global__ void __launch_bounds__(ZKMSM_ACC_THREADS, ZKMSM_ACC_MINBLOCKS) k_acc_l1(const uint2* __restrict__ ents,
+struct AccLaunch {
+    static constexpr int THREADS = 256, MIN_BLOCKS = 1;
+};
+template <>
+struct AccLaunch<Bls381> {
+    static constexpr int THREADS = 256, MIN_BLOCKS = 2;
+};
+template <class C>
+__global__ void __launch_bounds__(AccLaunch<C>::THREADS, AccLaunch<C>::MIN_BLOCKS) k_acc_l1(const uint2* __restrict__ ents,
                                                 const uint32_t* __restrict__ d_len, uint32_t K,
                                                 const uint32_t* __restrict__ bases,
                                                 const uint32_t* __restrict__ phi,

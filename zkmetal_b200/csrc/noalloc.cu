@@ -199,7 +199,7 @@ extern "C" ZkMetalStatus zkmsm_bn254_msm_noalloc(const void* d_points, const voi
         k_chunk_count<<<(Tl + 255) / 256, 256, 0, s>>>(lk, ks, tot + l, Kl, Tl, cnt);
         scan(base, cnt, Tl, tot + l + 1, nullptr, s);
         if (l == 0)
-            k_acc_l1<C><<<(Tl + ZKMSM_ACC_THREADS - 1) / ZKMSM_ACC_THREADS, ZKMSM_ACC_THREADS, 0, s>>>(ents, tot + l, Kl, pts, phi, cnt, buckets, pk[cur],
+            k_acc_l1<C><<<(Tl + AccLaunch<C>::THREADS - 1) / AccLaunch<C>::THREADS, AccLaunch<C>::THREADS, 0, s>>>(ents, tot + l, Kl, pts, phi, cnt, buckets, pk[cur],
                                                           pv[cur]);
         else
             k_acc_lj<C><<<(Tl + 255) / 256, 256, 0, s>>>(lk, pv[cur ^ 1], tot + l, Kl, cnt, buckets, pk[cur], pv[cur]);
