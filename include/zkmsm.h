@@ -151,6 +151,21 @@ ZkMetalStatus zkmsm_msm_device_async(ZkMetalMSMEngine engine, int curve, const v
 typedef void* ZkMsmTable;
 ZkMetalStatus zkmsm_table_create(ZkMetalMSMEngine engine, int curve, const void* points, uint64_t n_points,
                                  int points_on_device, ZkMsmTable* out);
+/* NEW: fixed-base precomputation for a resident table (replaces the
+ * reference's BGMW tables, Sources/zkMetal/MSM/MSMPrecomputation.swift:17-274
+ * and Sources/NeonFieldOps/bn254_msm.c:2163-2327, which store every digit
+ * multiple of every window).  Extends the table in place with its window
+ * shifts: copy k of every point is 2^(spacing_bits*k) * P_i, for
+ * k < ceil((fr_bits + 1) / spacing_bits), so memory grows by that many
+ * copies (BN254, spacing 4: 64 copies, 4 KiB per point).  MSMs over the
+ * table (zkmsm_batch_commit, the commitment server) then use window widths
+ * that are multiples of spacing_bits, add every window into one bucket set
+ * and skip the Horner chain; results are unchanged.  spacing_bits: 2..24,
+ * or 0 to drop the shifts.  Not to be called while the table is in use.
+ * ZKMETAL_ERR_INVALID_INPUT if copies * n_points reaches 2^30. */
+ZkMetalStatus zkmsm_table_precompute(ZkMsmTable table, int spacing_bits);
+/* Spacing of the table's shifts (0: none; -1: no table). */
+int zkmsm_table_shift_bits(ZkMsmTable table);
 void zkmsm_table_destroy(ZkMsmTable table);
 /* Device pointer of the table's affine points (for reading back / tests). */
 const void* zkmsm_table_device_points(ZkMsmTable table);
@@ -237,6 +252,11 @@ ZkMetalStatus zkmsm_engine_phase_times(ZkMetalMSMEngine engine, double* ms5, uin
  * buf.  Pure host computation: no device is touched. */
 ZkMetalStatus zkmsm_plan_describe(int curve, const uint32_t* counts, uint32_t n_msms, int scalar_fmt,
                                   int window_bits, int chunk, int glv, int scalar_bits, char* buf, uint64_t buflen);
+/* The same for MSMs over prefixes of a table of table_points points with
+ * window shifts of spacing shift_bits (zkmsm_table_precompute). */
+ZkMetalStatus zkmsm_plan_describe_shift(int curve, const uint32_t* counts, uint32_t n_msms, int scalar_fmt,
+                                        int window_bits, int shift_bits, uint32_t table_points, char* buf,
+                                        uint64_t buflen);
 
 /* Kernels launched so far by this engine (cumulative). */
 uint64_t zkmsm_engine_launch_count(ZkMetalMSMEngine engine);

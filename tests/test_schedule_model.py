@@ -59,7 +59,18 @@ def excl_scan(a):
     return out, run
 
 
+def plan_shift(curve, counts, shift_bits, table_points, window=0):
+    L = zl.lib()
+    arr = (ctypes.c_uint32 * len(counts))(*counts)
+    buf = ctypes.create_string_buffer(1 << 22)
+    st = L.zkmsm_plan_describe_shift(curve, arr, len(counts), 0, window, shift_bits, table_points, buf, len(buf))
+    assert st == 0, zl.last_error()
+    return json.loads(buf.value.decode())
+
+
 def run_model(C, pl, bases, scalars, seed=0):
+    """`bases`: the base table as the entries index it (for a shift-table
+    plan, copy k of the table at k * table_points + i)."""
     r = C.r
     lam = C.lam
     rng = random.Random(seed)
@@ -68,15 +79,21 @@ def run_model(C, pl, bases, scalars, seed=0):
     # 1-3: histogram, scan, scatter
     entries = []
     for d in descs:
-        soff, n, boff, c, nwin, glv, bucket_off, fmt, win_off = d
+        soff, n, boff, c, nwin, glv, bucket_off, fmt, win_off, wstep, nred = d
         B = 1 << (c - 1)
         for i in range(n):
             for j, (k, hneg) in enumerate(halves(C, scalars[soff + i], glv)):
                 for w, a, dneg in digits(k, c, nwin):
                     if a:
-                        gb = bucket_off + w * B + (a - 1)
+                        if wstep:  # shift table: one bucket set, window w reads copy w*c/s
+                            gb = bucket_off + (a - 1)
+                            idx = boff + i + w * wstep
+                            assert idx < len(bases) and idx <= 0x3FFFFFFF
+                            entries.append((gb, idx | ((hneg ^ dneg) << 31)))
+                        else:
+                            gb = bucket_off + w * B + (a - 1)
+                            entries.append((gb, (boff + i) | (j << 30) | ((hneg ^ dneg) << 31)))
                         assert gb < G
-                        entries.append((gb, (boff + i) | (j << 30) | ((hneg ^ dneg) << 31)))
     assert len(entries) <= pl["entry_bound"]
     rng.shuffle(entries)  # atomics give any order within a bucket
     entries.sort(key=lambda e: e[0])
@@ -172,9 +189,10 @@ def run_model(C, pl, bases, scalars, seed=0):
         inS, inW = outS, outW
     results = []
     for d in descs:
-        soff, n, boff, c, nwin, glv, bucket_off, fmt, win_off = d
+        soff, n, boff, c, nwin, glv, bucket_off, fmt, win_off, wstep, nred = d
+        assert nred == (1 if wstep else nwin)
         acc = 0
-        for w in range(nwin - 1, -1, -1):
+        for w in range(nred - 1, -1, -1):
             acc = acc * (1 << c) + inS[win_off + w] + inW[win_off + w]
         results.append(acc % r if n else 0)
     return results
@@ -218,6 +236,57 @@ def test_schedule_model(curve, counts, dist, window, chunk, glv, bits):
         want = sum(s * b for s, b in zip(scalars[off:off + n], bases[:n])) % C.r
         assert got[m] == want, m
         off += n
+
+
+SHIFT_CASES = [
+    # curve, counts, dist, shift spacing, table points, window override
+    ("bn254", [700], "uniform", 4, 700, 0),
+    ("bn254", [700], "witness", 4, 1000, 0),
+    ("bn254", [300, 0, 17, 1, 900], "uniform", 4, 1000, 0),
+    ("bn254", [500], "uniform", 4, 600, 10),   # 10 rounds up to a multiple of 4
+    ("bn254", [400], "witness", 8, 400, 16),
+    ("bls12_381", [600], "uniform", 6, 600, 0),
+    ("bls12_381", [250, 0, 40], "witness", 5, 300, 0),
+]
+
+
+@pytest.mark.parametrize("curve,counts,dist,s,tp,window", SHIFT_CASES)
+def test_schedule_model_shift_table(curve, counts, dist, s, tp, window):
+    """MSMs over a table with window shifts: every window's digits index
+    copy w*c/s of the table and add into one bucket set; one window sum."""
+    C = R.CURVES[curve]
+    cid = zl.BN254 if curve == "bn254" else zl.BLS12_381
+    pl = plan_shift(cid, counts, s, tp, window)
+    for d in pl["descs"]:
+        if d[1]:
+            assert d[3] % s == 0 and d[5] == 0 and d[10] == 1 and d[9] == (d[3] // s) * tp
+            if window:
+                assert d[3] == -(-window // s) * s
+    copies = -(-(C.r.bit_length() + 1) // s)
+    rng = random.Random(sum(counts) + s)
+    table = [rng.randrange(1, C.r) for _ in range(tp)]
+    ext = [p * pow(2, s * k, C.r) % C.r for k in range(copies) for p in table]
+    total = sum(counts)
+    if dist == "uniform":
+        scalars = [rng.randrange(1 << 256) for _ in range(total)]
+    else:
+        scalars = []
+        for _ in range(total):
+            u = rng.randrange(100)
+            scalars.append(0 if u < 40 else 1 if u < 60 else rng.getrandbits(32) if u < 85 else rng.randrange(C.r))
+    got = run_model(C, pl, ext, scalars, seed=len(counts))
+    off = 0
+    for m, n in enumerate(counts):
+        want = sum(sc * b for sc, b in zip(scalars[off:off + n], table[:n])) % C.r
+        assert got[m] == want, m
+        off += n
+
+
+def test_shift_plan_falls_back_outside_table():
+    """An MSM longer than the shift table's prefix uses ordinary windows."""
+    pl = plan_shift(zl.BN254, [100, 5000], 4, 1000)
+    assert pl["descs"][0][9] > 0 and pl["descs"][0][10] == 1
+    assert pl["descs"][1][9] == 0 and pl["descs"][1][10] == pl["descs"][1][4]
 
 
 def test_plan_sizes_2_24():

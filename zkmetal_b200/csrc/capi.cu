@@ -227,15 +227,12 @@ struct Table {
     int curve;
     uint64_t n;
     DevBuf points, phi;
+    // window shifts (zkmsm_table_precompute): `points` then holds `copies`
+    // copies of the n points, copy k = 2^(shift_bits*k) * P_i
+    uint32_t shift_bits = 0, copies = 1;
+    ShiftSpec shifts() const { return ShiftSpec{shift_bits, shift_bits ? (uint32_t)n : 0u}; }
 };
 
-// read-only view of a table for the commitment server (server.cu)
-struct TableView {
-    int curve;
-    uint64_t n;
-    const uint32_t* points;
-    const uint32_t* phi;
-};
 bool table_view(ZkMsmTable t, TableView* out) {
     if (!t || !out) return false;
     Table* tb = static_cast<Table*>(t);
@@ -243,6 +240,7 @@ bool table_view(ZkMsmTable t, TableView* out) {
     out->n = tb->n;
     out->points = tb->points.as<uint32_t>();
     out->phi = tb->phi.as<uint32_t>();
+    out->shifts = tb->shifts();
     return true;
 }
 
@@ -520,6 +518,38 @@ ZkMetalStatus zkmsm_table_create(ZkMetalMSMEngine engine, int curve, const void*
     });
 }
 
+ZkMetalStatus zkmsm_table_precompute(ZkMsmTable table, int spacing_bits) {
+    if (!table || spacing_bits < 0 || spacing_bits == 1 || spacing_bits > 24) return ZKMETAL_ERR_INVALID_INPUT;
+    Table& t = *static_cast<Table*>(table);
+    const uint32_t s = (uint32_t)spacing_bits;
+    const uint32_t fr_bits = t.curve == ZKMSM_BN254 ? CurveTraits<Bn254>::fr_bits : CurveTraits<Bls381>::fr_bits;
+    // a window's top digit may carry into bit fr_bits, so copies cover fr_bits + 1 bits
+    const uint32_t copies = s ? (fr_bits + 1 + s - 1) / s : 1;
+    if ((uint64_t)copies * t.n > VAL_IDX_MASK) {
+        set_error("shift table index exceeds 30 bits: use a wider spacing");
+        return ZKMETAL_ERR_INVALID_INPUT;
+    }
+    if (s == t.shift_bits) return ZKMETAL_SUCCESS;
+    return guarded([&] {
+        Engine& e = *t.engine;
+        const size_t ab = (size_t)2 * fp_bytes(t.curve);
+        DevBuf nb;
+        nb.ensure((size_t)copies * t.n * ab);
+        ZK_CUDA(cudaMemcpyAsync(nb.p, t.points.p, (size_t)t.n * ab, cudaMemcpyDeviceToDevice, e.stream));
+        if (t.curve == ZKMSM_BN254) e.make_shifts<Bn254>(nb.as<uint32_t>(), t.n, s, copies);
+        else e.make_shifts<Bls381>(nb.as<uint32_t>(), t.n, s, copies);
+        ZK_CUDA(cudaStreamSynchronize(e.stream));
+        e.drop_graphs();  // graphs captured over the old table address
+        std::swap(t.points.p, nb.p);
+        std::swap(t.points.cap, nb.cap);
+        t.shift_bits = s;
+        t.copies = copies;
+        return ZKMETAL_SUCCESS;
+    });
+}
+
+int zkmsm_table_shift_bits(ZkMsmTable table) { return table ? (int)static_cast<Table*>(table)->shift_bits : -1; }
+
 void zkmsm_table_destroy(ZkMsmTable table) { delete static_cast<Table*>(table); }
 
 const void* zkmsm_table_device_points(ZkMsmTable table) {
@@ -547,10 +577,10 @@ ZkMetalStatus zkmsm_batch_commit(ZkMetalMSMEngine engine, ZkMsmTable table, cons
         int fb = fp_bytes(t.curve);
         std::vector<uint8_t> out((size_t)n_msms * 3 * fb);
         if (t.curve == ZKMSM_BN254) {
-            Plan& pl = e.get_plan<Bn254>(cnt, boff, fmt);
+            Plan& pl = e.get_plan<Bn254>(cnt, boff, fmt, 0, 0, t.shifts());
             e.run_device_graph<Bn254>(pl, t.points.as<uint32_t>(), t.phi.as<uint32_t>(), sc, out.data());
         } else {
-            Plan& pl = e.get_plan<Bls381>(cnt, boff, fmt);
+            Plan& pl = e.get_plan<Bls381>(cnt, boff, fmt, 0, 0, t.shifts());
             e.run_device_graph<Bls381>(pl, t.points.as<uint32_t>(), t.phi.as<uint32_t>(), sc, out.data());
         }
         for (uint32_t m = 0; m < n_msms; m++) {
@@ -677,8 +707,8 @@ ZkMetalStatus zkmsm_engine_phase_times(ZkMetalMSMEngine engine, double* ms5, uin
     });
 }
 
-ZkMetalStatus zkmsm_plan_describe(int curve, const uint32_t* counts, uint32_t n_msms, int fmt, int window_bits,
-                                  int chunk, int glv, int scalar_bits, char* buf, uint64_t buflen) {
+static ZkMetalStatus plan_json(int curve, const uint32_t* counts, uint32_t n_msms, int fmt, int window_bits,
+                               int chunk, int glv, int scalar_bits, ShiftSpec sh, char* buf, uint64_t buflen) {
     if (!counts || !buf || n_msms == 0) return ZKMETAL_ERR_INVALID_INPUT;
     return guarded([&] {
         Tuning t;
@@ -687,15 +717,15 @@ ZkMetalStatus zkmsm_plan_describe(int curve, const uint32_t* counts, uint32_t n_
         t.glv = glv;
         std::vector<uint32_t> cnt(counts, counts + n_msms), boff(n_msms, 0);
         Plan pl;
-        if (curve == ZKMSM_BN254) Engine::plan_shape<Bn254>(pl, t, cnt, boff, fmt, scalar_bits);
-        else Engine::plan_shape<Bls381>(pl, t, cnt, boff, fmt, scalar_bits);
+        if (curve == ZKMSM_BN254) Engine::plan_shape<Bn254>(pl, t, cnt, boff, fmt, scalar_bits, 0, sh);
+        else Engine::plan_shape<Bls381>(pl, t, cnt, boff, fmt, scalar_bits, 0, sh);
         std::string s = "{\"descs\":[";
         for (size_t i = 0; i < pl.descs.size(); i++) {
             auto& d = pl.descs[i];
             s += (i ? "," : "") + std::string("[") + std::to_string(d.scalar_off) + "," + std::to_string(d.n) + "," +
                  std::to_string(d.base_off) + "," + std::to_string(d.c) + "," + std::to_string(d.nwin) + "," +
                  std::to_string(d.glv) + "," + std::to_string(d.bucket_off) + "," + std::to_string(d.fmt) + "," +
-                 std::to_string(d.win_off) + "]";
+                 std::to_string(d.win_off) + "," + std::to_string(d.wstep) + "," + std::to_string(d.nred) + "]";
         }
         s += "],\"entry_bound\":" + std::to_string(pl.entry_bound) + ",\"nbuckets\":" + std::to_string(pl.nbuckets) +
              ",\"sort\":[" + std::to_string(pl.sort_maxd) + "," + std::to_string(pl.sort_spb) + "," +
@@ -720,6 +750,19 @@ ZkMetalStatus zkmsm_plan_describe(int curve, const uint32_t* counts, uint32_t n_
         memcpy(buf, s.c_str(), s.size() + 1);
         return ZKMETAL_SUCCESS;
     });
+}
+
+ZkMetalStatus zkmsm_plan_describe(int curve, const uint32_t* counts, uint32_t n_msms, int fmt, int window_bits,
+                                  int chunk, int glv, int scalar_bits, char* buf, uint64_t buflen) {
+    return plan_json(curve, counts, n_msms, fmt, window_bits, chunk, glv, scalar_bits, ShiftSpec{}, buf, buflen);
+}
+
+ZkMetalStatus zkmsm_plan_describe_shift(int curve, const uint32_t* counts, uint32_t n_msms, int fmt,
+                                        int window_bits, int shift_bits, uint32_t table_points, char* buf,
+                                        uint64_t buflen) {
+    if (shift_bits < 2 || shift_bits > 24) return ZKMETAL_ERR_INVALID_INPUT;
+    return plan_json(curve, counts, n_msms, fmt, window_bits, 0, -1, 0,
+                     ShiftSpec{(uint32_t)shift_bits, table_points}, buf, buflen);
 }
 
 uint64_t zkmsm_engine_launch_count(ZkMetalMSMEngine engine) { return engine ? ENG(engine).launches : 0; }

@@ -12,6 +12,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <cstdint>
 #include <cstring>
 #include <map>
@@ -161,6 +162,51 @@ inline uint32_t choose_window(uint64_t entries_per_window, uint32_t bits) {
     return bc;
 }
 
+// Window width for an MSM over a shift table with spacing s (copy k of the
+// table holds 2^(s*k) * P_i): a multiple of s, at most 20.  All windows share
+// one bucket set and there is no Horner chain.  Cost in units of one sorted
+// entry (a mixed addition): n per window, 1.8 per bucket of the single set,
+// and latency terms for the reduction depth (per window bit) and for the
+// segmented-sum depth (log of the entries per bucket).  The coefficients are
+// a least-squares fit of measured BN254 MSM times, n = 2^8..2^16 and
+// c = 4..20 on a B200 (within 0.18 ms).
+inline uint32_t choose_window_shift(uint64_t n, uint32_t bits, uint32_t s) {
+    double best = 1e300;
+    uint32_t bc = s;
+    for (uint32_t c = s; c <= std::max<uint32_t>(s, 20); c += s) {
+        const uint32_t w = windows_for(bits, c);
+        const double add = (double)n * w;
+        const double red = 1.8 * (double)(1u << (c - 1));
+        const double per_bucket = (double)n * w / (double)(1u << (c - 1));
+        const double lat = 5.5e5 * c + 3.06e5 * std::log2(per_bucket + 1.0);
+        const double cost = add + red + lat;
+        if (cost < best) {
+            best = cost;
+            bc = c;
+        }
+        if (c > bits) break;  // wider windows only add buckets
+    }
+    return bc;
+}
+
+// The precomputed window shifts of a resident base table: `copies` copies of
+// its `points` points, copy k holding 2^(bits*k) * P_i (bits 0: none).
+struct ShiftSpec {
+    uint32_t bits = 0;
+    uint32_t points = 0;
+};
+
+// Read-only view of a resident base table (capi.cu owns tables; the
+// commitment server reads them through table_view).
+struct TableView {
+    int curve;
+    uint64_t n;
+    const uint32_t* points;
+    const uint32_t* phi;
+    ShiftSpec shifts;
+};
+bool table_view(void* table, TableView* out);
+
 template <class C>
 struct CurveTraits;
 template <>
@@ -280,18 +326,20 @@ class Engine {
     // ------------------------------------------------------------ planning
     template <class C>
     void make_plan(Plan& pl, const std::vector<uint32_t>& counts, const std::vector<uint32_t>& base_offs,
-                   int fmt, uint32_t scalar_bits, uint32_t window_override = 0) const {
-        plan_shape<C>(pl, tuning, counts, base_offs, fmt, scalar_bits, window_override);
+                   int fmt, uint32_t scalar_bits, uint32_t window_override = 0, ShiftSpec sh = {}) const {
+        plan_shape<C>(pl, tuning, counts, base_offs, fmt, scalar_bits, window_override, sh);
     }
 
     // Pure host planning (no device needed): window widths, bucket layout,
     // chunking of the segmented sums and the reduction tree.
     template <class C>
     // window_override > 0 fixes every MSM's window width (the stripes of one
-    // striped MSM share one bucket layout).
+    // striped MSM share one bucket layout).  `sh`: the bases are a shift
+    // table; an MSM whose points lie in it uses the precomputed shifts (no
+    // GLV, window width a multiple of sh.bits, one bucket set).
     static void plan_shape(Plan& pl, const Tuning& tuning, const std::vector<uint32_t>& counts,
                            const std::vector<uint32_t>& base_offs, int fmt, uint32_t scalar_bits,
-                           uint32_t window_override = 0) {
+                           uint32_t window_override = 0, ShiftSpec sh = {}) {
         pl.curve = CurveTraits<C>::id;
         uint64_t soff = 0;
         uint32_t boff = 0, woff = 0;
@@ -302,6 +350,26 @@ class Engine {
             d.base_off = base_offs[m];
             d.fmt = fmt;
             bool small = scalar_bits > 0 && scalar_bits <= 64;
+            if (sh.bits && d.n && (uint64_t)d.base_off + d.n <= sh.points) {
+                const uint32_t bits = small ? scalar_bits : CurveTraits<C>::fr_bits;
+                uint32_t c = window_override ? window_override
+                                             : tuning.window_bits > 0 ? (uint32_t)tuning.window_bits
+                                                                      : choose_window_shift(d.n, bits, sh.bits);
+                c = std::max<uint32_t>(1, (c + sh.bits - 1) / sh.bits) * sh.bits;
+                d.glv = 0;
+                d.c = c;
+                d.nwin = windows_for(bits, c);
+                d.wstep = (c / sh.bits) * sh.points;
+                d.nred = 1;
+                d.bucket_off = boff;
+                d.win_off = woff;
+                boff += 1u << (c - 1);
+                woff += 1;
+                pl.entry_bound += (uint64_t)d.n * d.nwin;
+                soff += d.n;
+                pl.descs.push_back(d);
+                continue;
+            }
             d.glv = small ? 0 : (tuning.glv == 0 ? 0 : 1);
             uint32_t bits = small ? scalar_bits : (d.glv ? CurveTraits<C>::half_bits : CurveTraits<C>::fr_bits);
             uint64_t epw = (uint64_t)d.n * (d.glv ? 2 : 1);
@@ -315,6 +383,8 @@ class Engine {
             if (c < 2) c = 2;
             d.c = c;
             d.nwin = d.n ? windows_for(bits, c) : 0;
+            d.wstep = 0;
+            d.nred = d.nwin;
             d.bucket_off = boff;
             d.win_off = woff;
             boff += d.nwin * (1u << (c - 1));
@@ -377,7 +447,7 @@ class Engine {
         uint32_t off = 0;
         for (auto& d : pl.descs) {
             uint32_t B = 1u << (d.c - 1);
-            for (uint32_t w = 0; w < d.nwin; w++) {
+            for (uint32_t w = 0; w < d.nred; w++) {
                 RedTask t;
                 t.in_off = d.bucket_off + w * B;
                 t.n_in = B;
@@ -417,13 +487,14 @@ class Engine {
 
     template <class C>
     Plan& get_plan(const std::vector<uint32_t>& counts, const std::vector<uint32_t>& base_offs, int fmt,
-                   uint32_t scalar_bits = 0, uint32_t window_override = 0) {
+                   uint32_t scalar_bits = 0, uint32_t window_override = 0, ShiftSpec sh = {}) {
         std::string key;
         auto put = [&](uint64_t v) { key.append(reinterpret_cast<const char*>(&v), sizeof v); };
         put(CurveTraits<C>::id);
         put(fmt);
         put(scalar_bits);
         put(window_override);
+        put((uint64_t)sh.bits << 32 | sh.points);
         put((uint64_t)(uint32_t)tuning.window_bits << 32 | (uint32_t)tuning.chunk);
         put((uint64_t)(int64_t)tuning.glv);
         put(tuning.version);
@@ -436,7 +507,7 @@ class Engine {
             plan_cache.clear();
         }
         std::unique_ptr<Plan> pl(new Plan());
-        make_plan<C>(*pl, counts, base_offs, fmt, scalar_bits, window_override);
+        make_plan<C>(*pl, counts, base_offs, fmt, scalar_bits, window_override, sh);
         upload_plan(*pl, false);
         Plan& ref = *pl;
         plan_cache.emplace(key, std::move(pl));
@@ -472,9 +543,10 @@ class Engine {
     // state serving neither allocates nor frees.  Valid until the next call.
     Plan transient;
     template <class C>
-    Plan& transient_plan(const std::vector<uint32_t>& counts, const std::vector<uint32_t>& base_offs, int fmt) {
+    Plan& transient_plan(const std::vector<uint32_t>& counts, const std::vector<uint32_t>& base_offs, int fmt,
+                         ShiftSpec sh = {}) {
         transient.clear_host();
-        make_plan<C>(transient, counts, base_offs, fmt, 0);
+        make_plan<C>(transient, counts, base_offs, fmt, 0, 0, sh);
         upload_plan(transient, true);
         return transient;
     }
@@ -549,6 +621,11 @@ class Engine {
     void fold_buckets(void* base, uint32_t nb, uint32_t S);
     template <class C>
     void make_phi(const uint32_t* d_bases, uint64_t n, uint32_t* d_phi);
+    // Window shifts of a table of n affine points (copy 0, at d_table):
+    // copies 1..copies-1, copy k = 2^(s*k) * P_i at d_table + k*n points.
+    // Synchronous (returns when the table is written).
+    template <class C>
+    void make_shifts(uint32_t* d_table, uint64_t n, uint32_t s, uint32_t copies);
     // resident threads of k_acc_l1<C> on this device (occupancy API)
     template <class C>
     uint32_t acc_resident_threads();
@@ -627,6 +704,7 @@ class Engine {
                                                 std::vector<cudaEvent_t>*);                             \
     EXT template void Engine::fold_buckets<C>(void*, uint32_t, uint32_t);                               \
     EXT template void Engine::make_phi<C>(const uint32_t*, uint64_t, uint32_t*);                        \
+    EXT template void Engine::make_shifts<C>(uint32_t*, uint64_t, uint32_t, uint32_t);                  \
     EXT template uint32_t Engine::acc_resident_threads<C>();                                              \
     EXT template void Engine::gen_bases<C>(uint64_t, uint64_t, uint64_t, uint32_t*);                    \
     EXT template void Engine::gen_scalars<C>(uint64_t, uint64_t, uint64_t, int, int, uint32_t*);

@@ -167,6 +167,31 @@ void Engine::make_phi(const uint32_t* d_bases, uint64_t n, uint32_t* d_phi) {
 }
 
 template <class C>
+void Engine::make_shifts(uint32_t* d_table, uint64_t n, uint32_t s, uint32_t copies) {
+    using P = typename C::Fp;
+    if (!n || copies < 2) return;
+    // points per pass: the XYZZ scratch of one pass stays near 512 MB
+    const uint64_t per_point = (uint64_t)(copies - 1) * sizeof(Xyzz<P>);
+    const uint32_t m = (uint32_t)std::min<uint64_t>(n, std::max<uint64_t>(1024, (512ull << 20) / per_point));
+    DevBuf scratch;
+    scratch.ensure((size_t)m * per_point);
+    Xyzz<P>* sc = scratch.as<Xyzz<P>>();
+    for (uint64_t i0 = 0; i0 < n; i0 += m) {
+        const uint32_t mm = (uint32_t)std::min<uint64_t>(m, n - i0);
+        k_shift_chain<C><<<(mm + 127) / 128, 128, 0, stream>>>(d_table, (uint32_t)i0, mm, s, copies, sc);
+        launches++;
+        ZK_CUDA(cudaGetLastError());
+        const uint64_t total = (uint64_t)(copies - 1) * mm;
+        const uint64_t threads = (total + SHIFT_G - 1) / SHIFT_G;
+        k_shift_affine<C><<<(unsigned)((threads + 127) / 128), 128, 0, stream>>>(sc, total, mm, (uint32_t)i0, n,
+                                                                                 d_table);
+        launches++;
+        ZK_CUDA(cudaGetLastError());
+    }
+    ZK_CUDA(cudaStreamSynchronize(stream));
+}
+
+template <class C>
 uint32_t Engine::acc_resident_threads() {
     int per_sm = 0, sms = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_acc_l1<C>, AccLaunch<C>::THREADS, 0) !=

@@ -212,8 +212,13 @@ ZK_DEV void next_digits(DigitGen& g, const Halves& h, const MsmDesc& d, uint32_t
             }
             if (a) {
                 valid[s] = true;
-                gb[s] = d.bucket_off + w * half + (a - 1);
-                val[s] = idx | (j << 30) | ((h.neg[j] ^ dn) << 31);
+                if (d.wstep) {  // shift table: window w's base is 2^(c*w)*P, one bucket set
+                    gb[s] = d.bucket_off + (a - 1);
+                    val[s] = (idx + w * d.wstep) | ((h.neg[j] ^ dn) << 31);
+                } else {
+                    gb[s] = d.bucket_off + w * half + (a - 1);
+                    val[s] = idx | (j << 30) | ((h.neg[j] ^ dn) << 31);
+                }
                 break;
             }
         }
@@ -593,6 +598,94 @@ __global__ void __launch_bounds__(256) k_endo(const uint32_t* __restrict__ bases
     store_fe(d + P::N / 4, a.y);
 }
 
+// ------------------------------------------------------------ shift tables
+//
+// A resident table of n affine points extended with window shifts: copy k
+// (0 <= k < copies) holds 2^(s*k) * P_i at index k*n + i, copy 0 being the
+// points themselves.  An MSM over the table with window width c (a multiple
+// of s) then takes window w's digit against copy w*c/s, so every window
+// adds into one bucket set and the result needs no doublings.  Replaces the
+// reference's BGMW precomputation (MSM/MSMPrecomputation.swift:17-274,
+// bn254_msm.c:2163-2230), whose tables hold every digit multiple of every
+// window shift (2^c - 1 points per window per base); here only the shifts
+// are stored and the digit multiples come from the bucket method.
+
+// Step 1, points [i0, i0 + m): the doubling chain of each point in XYZZ,
+// copy k >= 1 of point i0 + j to scratch[(k - 1) * m + j].
+template <class C>
+__global__ void __launch_bounds__(128) k_shift_chain(const uint32_t* __restrict__ pts, uint32_t i0, uint32_t m,
+                                                     uint32_t s, uint32_t copies,
+                                                     Xyzz<typename C::Fp>* __restrict__ scratch) {
+    using P = typename C::Fp;
+    const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= m) return;
+    Affine<P> a;
+    load_affine(a, pts, i0 + j);
+    Xyzz<P> acc;
+    xyzz_from_affine(acc, a);
+#pragma unroll 1
+    for (uint32_t k = 1; k < copies; k++) {
+#pragma unroll 1
+        for (uint32_t b = 0; b < s; b++) xyzz_dbl_ni(acc, acc);
+        store_xyzz(scratch + (size_t)(k - 1) * m + j, acc);
+    }
+}
+
+// Step 2: scratch element e = (k - 1) * m + j to affine at table index
+// k * n + i0 + j, SHIFT_G consecutive elements per thread sharing one
+// inversion (simultaneous inversion: prefix products forward, then one
+// inverse unwound backwards).  The identity (ZZ = 0) becomes (0, 0) and
+// contributes 1 to the products.
+constexpr uint32_t SHIFT_G = 16;
+template <class C>
+__global__ void __launch_bounds__(128) k_shift_affine(const Xyzz<typename C::Fp>* __restrict__ scratch,
+                                                      uint64_t total, uint32_t m, uint32_t i0, uint64_t n,
+                                                      uint32_t* __restrict__ table) {
+    using P = typename C::Fp;
+    const uint64_t e0 = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) * SHIFT_G;
+    if (e0 >= total) return;
+    const uint32_t cnt = (uint32_t)(total - e0 < SHIFT_G ? total - e0 : SHIFT_G);
+    Fe<P> pre[SHIFT_G];
+    Fe<P> acc, t;
+    fe_set_one(acc);
+#pragma unroll 1
+    for (uint32_t g = 0; g < cnt; g++) {
+        Xyzz<P> q;
+        load_xyzz(q, scratch + e0 + g);
+        pre[g] = acc;
+        if (!xyzz_is_id(q)) {
+            fe_mul(t, q.zz, q.zzz);
+            fe_mul(acc, acc, t);
+        }
+    }
+    Fe<P> inv;
+    fe_inv(inv, acc);
+#pragma unroll 1
+    for (int g = (int)cnt - 1; g >= 0; g--) {
+        Xyzz<P> q;
+        load_xyzz(q, scratch + e0 + g);
+        const uint64_t e = e0 + (uint32_t)g;
+        const uint64_t k = e / m + 1, j = e % m;
+        uint4* d = reinterpret_cast<uint4*>(table + (size_t)(k * n + i0 + j) * 2 * P::N);
+        Affine<P> a;
+        if (xyzz_is_id(q)) {
+            fe_set_zero(a.x);
+            fe_set_zero(a.y);
+        } else {
+            Fe<P> it, u;
+            fe_mul(it, inv, pre[g]);    // 1 / (ZZ * ZZZ)
+            fe_mul(t, q.zz, q.zzz);
+            fe_mul(inv, inv, t);        // 1 / (product of the earlier elements)
+            fe_mul(u, it, q.zzz);       // 1 / ZZ
+            fe_mul(a.x, q.x, u);
+            fe_mul(u, it, q.zz);        // 1 / ZZZ
+            fe_mul(a.y, q.y, u);
+        }
+        store_fe(d, a.x);
+        store_fe(d + P::N / 4, a.y);
+    }
+}
+
 // ------------------------------------------------------------ segmented sums
 
 // Partial-slot count of a chunk: a run touching the chunk's first entry that
@@ -811,8 +904,9 @@ __global__ void __launch_bounds__(128) k_reduce_level(const Xyzz<typename C::Fp>
     store_xyzz(outW + g, x);
 }
 
-// Horner over each MSM's windows; output reference-layout Jacobian (X, Y, Z)
-// Montgomery with Z = 1 (or the identity (1, 1, 0)).
+// Horner over each MSM's window sums (one sum, no doublings, for a
+// shift-table MSM); output reference-layout Jacobian (X, Y, Z) Montgomery
+// with Z = 1 (or the identity (1, 1, 0)).
 template <class C>
 __global__ void k_combine(const Xyzz<typename C::Fp>* __restrict__ rootS,
                           const Xyzz<typename C::Fp>* __restrict__ rootW,
@@ -831,8 +925,8 @@ __global__ void k_combine(const Xyzz<typename C::Fp>* __restrict__ rootS,
         return;
     }
 #pragma unroll 1
-    for (int w = (int)d.nwin - 1; w >= 0; w--) {
-        if (w != (int)d.nwin - 1) {
+    for (int w = (int)d.nred - 1; w >= 0; w--) {
+        if (w != (int)d.nred - 1) {
 #pragma unroll 1
             for (uint32_t b = 0; b < d.c; b++) xyzz_dbl<P, true>(acc, acc);  // one thread: inline products
         }

@@ -137,6 +137,8 @@ extern "C" ZkMetalStatus zkmsm_bn254_msm_noalloc(const void* d_points, const voi
     desc.bucket_off = 0;
     desc.fmt = (uint32_t)fmt;
     desc.win_off = 0;
+    desc.wstep = 0;
+    desc.nred = NWIN;
     RedTask tasks[RED_LEVELS * NWIN];
     uint32_t nin = BPW;
     for (int l = 0; l < RED_LEVELS; l++) {

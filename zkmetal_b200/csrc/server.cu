@@ -32,14 +32,6 @@
 
 namespace zkmsm {
 
-struct TableView {  // the parts of a resident table the server needs
-    int curve;
-    uint64_t n;
-    const uint32_t* points;
-    const uint32_t* phi;
-};
-// defined in capi.cu
-bool table_view(ZkMsmTable t, TableView* out);
 
 namespace {
 
@@ -189,10 +181,10 @@ struct Server {
                 int fb = curve == ZKMSM_BN254 ? 32 : 48;
                 out.resize(batch.size() * 3 * fb);
                 if (curve == ZKMSM_BN254) {
-                    Plan& pl = eng->transient_plan<Bn254>(counts, boffs, fmt);
+                    Plan& pl = eng->transient_plan<Bn254>(counts, boffs, fmt, tv.shifts);
                     eng->run_device<Bn254>(pl, tv.points, tv.phi, d_scalars, out.data());
                 } else {
-                    Plan& pl = eng->transient_plan<Bls381>(counts, boffs, fmt);
+                    Plan& pl = eng->transient_plan<Bls381>(counts, boffs, fmt, tv.shifts);
                     eng->run_device<Bls381>(pl, tv.points, tv.phi, d_scalars, out.data());
                 }
                 for (size_t i = 0; i < batch.size(); i++) memcpy(batch[i]->result, out.data() + i * 3 * fb, 3 * fb);

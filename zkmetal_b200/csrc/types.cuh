@@ -25,6 +25,12 @@ struct MsmDesc {
     uint32_t bucket_off;  // first global bucket id
     uint32_t fmt;         // 0: integer scalars, 1: Montgomery-form Fr
     uint32_t win_off;     // first window-sum slot
+    // Shift-table MSMs (bases 2^(c*w)*P_i precomputed for every window w):
+    // the base index of window w's digit is base_off + i + w*wstep and all
+    // windows share one bucket set (nred = 1 window sum, no doublings in the
+    // combine).  wstep = 0: ordinary windows, nred = nwin.
+    uint32_t wstep;
+    uint32_t nred;        // window sums (bucket sets) of this MSM
 };
 
 // Sorted-entry value: base index (30 bits) | endo << 30 | negate << 31

@@ -69,6 +69,8 @@ _SIGS = {
     "zkmsm_msm_device_async": (c_i32, [c_vp, c_int, c_vp, c_vp, c_vp, c_int, c_u32, c_vp, c_vp]),
     "zkmsm_table_create": (c_i32, [c_vp, c_int, c_vp, c_u64, c_int, ctypes.POINTER(c_vp)]),
     "zkmsm_table_destroy": (None, [c_vp]),
+    "zkmsm_table_precompute": (c_i32, [c_vp, c_int]),
+    "zkmsm_table_shift_bits": (c_int, [c_vp]),
     "zkmsm_table_device_points": (c_vp, [c_vp]),
     "zkmsm_batch_commit": (c_i32, [c_vp, c_vp, c_vp, c_int, c_int, c_vp, c_u32, c_u8p]),
     "zkmsm_engine_set_tuning": (c_i32, [c_vp, c_int, c_int, c_int]),
@@ -86,6 +88,7 @@ _SIGS = {
     "zkmsm_gen_scalars": (c_i32, [c_vp, c_int, c_u64, c_u64, c_u64, c_int, c_int, c_vp]),
     "zkmsm_engine_launch_count": (c_u64, [c_vp]),
     "zkmsm_plan_describe": (c_i32, [c_int, c_vp, c_u32, c_int, c_int, c_int, c_int, c_int, ctypes.c_char_p, c_u64]),
+    "zkmsm_plan_describe_shift": (c_i32, [c_int, c_vp, c_u32, c_int, c_int, c_int, c_u32, ctypes.c_char_p, c_u64]),
     "zkmsm_engine_profile": (c_i32, [c_vp, c_int]),
     "zkmsm_engine_phase_times": (c_i32, [c_vp, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(c_u64), c_int]),
     "zkmsm_measure_peaks": (c_i32, [ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double),

@@ -199,6 +199,17 @@ class CommitmentTable:
         self._h = h
         self.n = count
 
+    def precompute(self, spacing_bits=4):
+        """Extend the table with its window shifts (copy k = 2^(spacing*k) * P):
+        later MSMs over it use one bucket set and no Horner chain.  0 drops
+        the shifts.  Replaces the reference's BGMW precomputation
+        (MSM/MSMPrecomputation.swift:17-274)."""
+        _raise_for(_l.lib().zkmsm_table_precompute(self._h, int(spacing_bits)))
+
+    @property
+    def shift_bits(self):
+        return _l.lib().zkmsm_table_shift_bits(self._h)
+
     def close(self):
         if getattr(self, "_h", None):
             _l.lib().zkmsm_table_destroy(self._h)
