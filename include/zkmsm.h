@@ -179,12 +179,13 @@ ZkMetalStatus zkmsm_batch_commit(ZkMetalMSMEngine engine, ZkMsmTable table, cons
                                  int scalars_on_device, int scalar_fmt, const uint32_t* counts, uint32_t n_msms,
                                  uint8_t* results);
 
-/* Autotuner: times the MSM at window widths around the cost model's choice
- * for every power-of-two size 2^min_log2n .. 2^max_log2n on synthetic
- * inputs and keeps the fastest per size; later plans of this engine use the
- * table (MSMs matched to the nearest power of two).  A JSON summary of the
- * timings is written to `report` (may be NULL).  Replaces the reference's
- * device tuning (Sources/zkMetal/Tuning.swift:9-127). */
+/* Autotuner: times the MSM at equal window widths around the cost model's
+ * choice, and at the model's two-width layout where it picks one (reported
+ * as width 0), for every power-of-two size 2^min_log2n .. 2^max_log2n on
+ * synthetic inputs and keeps the fastest per size; later plans of this
+ * engine use the table (MSMs matched to the nearest power of two).  A JSON
+ * summary of the timings is written to `report` (may be NULL).  Replaces the
+ * reference's device tuning (Sources/zkMetal/Tuning.swift:9-127). */
 ZkMetalStatus zkmsm_autotune(ZkMetalMSMEngine engine, int curve, int min_log2n, int max_log2n, char* report,
                              uint64_t report_len);
 /* Persist / restore the autotuned table (text file). */
@@ -219,14 +220,16 @@ ZkMetalStatus zkmsm_server_stats(ZkMsmServer server, char* buf, uint64_t buflen)
 ZkMetalStatus zkmsm_server_inject_failures(ZkMsmServer server, int batches);
 void zkmsm_server_destroy(ZkMsmServer server);
 
-/* Tuning overrides (0 = automatic): window bits, chunk length, GLV on/off. */
+/* Tuning overrides (0 = automatic): window bits, chunk length, GLV on/off.
+ * window_bits >= 2^16 is a two-width layout c | nlo << 16: nlo windows of
+ * c bits, then (c + 1)-bit windows up to the scalar width. */
 ZkMetalStatus zkmsm_engine_set_tuning(ZkMetalMSMEngine engine, int window_bits, int chunk, int glv);
 /* NEW: host-buffer MSMs (zkmetal_*_msm and their _fr forms) are streamed in
- * stripes (consecutive point ranges growing 1.6x per stripe up to 2^stripe_log2
- * points): each stripe's host-to-device copy overlaps the previous stripe's
- * sort and accumulation, every stripe fills its own bucket array in the whole
- * MSM's window layout, and the arrays are added and reduced once (the same
- * point).  -1 (default): automatic, largest stripe half of n's next power of
+ * stripes (consecutive point ranges from 2^(stripe_log2-2) points, growing
+ * 1.6x per stripe up to 2^stripe_log2): each stripe's host-to-device copy
+ * overlaps the previous stripe's sort and accumulation, every stripe fills
+ * its own bucket array in the window layout of the largest stripe, and the
+ * arrays are added and reduced once (the same point).  -1 (default): automatic, largest stripe half of n's next power of
  * two, only for n >= 2^22; 0: off; 2..30: fixed. */
 ZkMetalStatus zkmsm_engine_set_stripe(ZkMetalMSMEngine engine, int stripe_log2);
 

@@ -160,7 +160,10 @@ def test_tuning_invariance(eng, oracles, curve):
     L = zl.lib()
     results = set()
     try:
-        for c, k, glv in [(0, 0, -1), (6, 8, 1), (11, 33, 1), (16, 128, 1), (21, 16, 1), (9, 8, 0), (13, 64, 0)]:
+        # c | nlo << 16: nlo windows of c bits, then c + 1-bit windows
+        for c, k, glv in [(0, 0, -1), (6, 8, 1), (11, 33, 1), (16, 128, 1), (21, 16, 1), (9, 8, 0), (13, 64, 0),
+                          (5 | 10 << 16, 8, 1), (12 | 3 << 16, 16, 1), (18 | 5 << 16, 64, 1), (21 | 4 << 16, 192, 1),
+                          (10 | 7 << 16, 24, 0)]:
             check(L.zkmsm_engine_set_tuning(e.handle, c, k, glv))
             results.add(msm_device(e, curve, p, s, zl.SCALAR_INT, n))
     finally:

@@ -38,13 +38,27 @@ def halves(C, s, glv):
     return [(abs(k1), int(k1 < 0)), (abs(k2), int(k2 < 0))]
 
 
-def digits(k, c, nwin):
-    half = 1 << (c - 1)
+def win_width(c, nlo, w):
+    return c + (1 if w >= nlo else 0)
+
+
+def win_bit(c, nlo, w):
+    return w * c + max(0, w - nlo)
+
+
+def win_bucket(c, nlo, w):
+    return (w + max(0, w - nlo)) << (c - 1)
+
+
+def digits(k, c, nwin, nlo=None):
+    """Signed digits; windows [0, nlo) are c bits, later ones c + 1 bits."""
+    nlo = nwin if nlo is None else nlo
     carry = 0
     for w in range(nwin):
-        v = ((k >> (c * w)) & ((1 << c) - 1)) + carry
-        if v > half:
-            yield w, (1 << c) - v, 1
+        cw = win_width(c, nlo, w)
+        v = ((k >> win_bit(c, nlo, w)) & ((1 << cw) - 1)) + carry
+        if v > (1 << (cw - 1)):
+            yield w, (1 << cw) - v, 1
             carry = 1
         else:
             yield w, v, 0
@@ -79,11 +93,11 @@ def run_model(C, pl, bases, scalars, seed=0):
     # 1-3: histogram, scan, scatter
     entries = []
     for d in descs:
-        soff, n, boff, c, nwin, glv, bucket_off, fmt, win_off, wstep, nred = d
-        B = 1 << (c - 1)
+        soff, n, boff, c, nwin, glv, bucket_off, fmt, win_off, wstep, nred, nlo = d
         for i in range(n):
             for j, (k, hneg) in enumerate(halves(C, scalars[soff + i], glv)):
-                for w, a, dneg in digits(k, c, nwin):
+                assert k < 1 << sum(win_width(c, nlo, w) for w in range(nwin)) - 1, "windows cover bits + 1"
+                for w, a, dneg in digits(k, c, nwin, nlo):
                     if a:
                         if wstep:  # shift table: one bucket set, window w reads copy w*c/s
                             gb = bucket_off + (a - 1)
@@ -91,7 +105,7 @@ def run_model(C, pl, bases, scalars, seed=0):
                             assert idx < len(bases) and idx <= 0x3FFFFFFF
                             entries.append((gb, idx | ((hneg ^ dneg) << 31)))
                         else:
-                            gb = bucket_off + w * B + (a - 1)
+                            gb = bucket_off + win_bucket(c, nlo, w) + (a - 1)
                             entries.append((gb, (boff + i) | (j << 30) | ((hneg ^ dneg) << 31)))
                         assert gb < G
     assert len(entries) <= pl["entry_bound"]
@@ -189,11 +203,11 @@ def run_model(C, pl, bases, scalars, seed=0):
         inS, inW = outS, outW
     results = []
     for d in descs:
-        soff, n, boff, c, nwin, glv, bucket_off, fmt, win_off, wstep, nred = d
+        soff, n, boff, c, nwin, glv, bucket_off, fmt, win_off, wstep, nred, nlo = d
         assert nred == (1 if wstep else nwin)
         acc = 0
         for w in range(nred - 1, -1, -1):
-            acc = acc * (1 << c) + inS[win_off + w] + inW[win_off + w]
+            acc = acc * (1 << win_width(c, nlo, w)) + inS[win_off + w] + inW[win_off + w]
         results.append(acc % r if n else 0)
     return results
 
@@ -234,6 +248,42 @@ def test_schedule_model(curve, counts, dist, window, chunk, glv, bits):
     for m, n in enumerate(counts):
         # the plan puts every MSM on a prefix of one base table (base_off = 0)
         want = sum(s * b for s, b in zip(scalars[off:off + n], bases[:n])) % C.r
+        assert got[m] == want, m
+        off += n
+
+
+LAYOUT_CASES = [
+    # curve, counts, dist, c, nlo (nlo windows of c bits, then c + 1-bit ones)
+    ("bn254", [700], "uniform", 5, 10),
+    ("bn254", [2000], "witness", 6, 1),
+    ("bn254", [300, 0, 17, 1, 900], "uniform", 7, 4),
+    ("bls12_381", [600], "uniform", 8, 3),
+    ("bls12_381", [250, 0, 40], "witness", 4, 20),
+]
+
+
+@pytest.mark.parametrize("curve,counts,dist,c,nlo", LAYOUT_CASES)
+def test_schedule_model_two_width(curve, counts, dist, c, nlo):
+    """Forced two-width layouts (window setting c | nlo << 16): digits,
+    bucket offsets, reduction tasks and the Horner combine per window width."""
+    C = R.CURVES[curve]
+    cid = zl.BN254 if curve == "bn254" else zl.BLS12_381
+    pl = plan(cid, counts, 0, c | (nlo << 16), 0, -1, 0)
+    for d in pl["descs"]:
+        if d[1]:
+            assert d[3] == c and d[11] == nlo < d[4]
+    rng = random.Random(sum(counts) + c)
+    total = sum(counts)
+    bases = [rng.randrange(1, C.r) for _ in range(total)]
+    if dist == "uniform":
+        scalars = [rng.randrange(1 << 256) for _ in range(total)]
+    else:
+        scalars = [0 if u < 40 else 1 if u < 60 else rng.getrandbits(32) if u < 85 else rng.randrange(C.r)
+                   for u in (rng.randrange(100) for _ in range(total))]
+    got = run_model(C, pl, bases, scalars, seed=len(counts))
+    off = 0
+    for m, n in enumerate(counts):
+        want = sum(sc * b for sc, b in zip(scalars[off:off + n], bases[:n])) % C.r
         assert got[m] == want, m
         off += n
 
@@ -294,6 +344,23 @@ def test_plan_sizes_2_24():
     window choice is the cost model's."""
     pl = plan(zl.BN254, [1 << 24])
     d = pl["descs"][0]
-    assert d[4] * (1 << (d[3] - 1)) == pl["nbuckets"]
-    assert pl["entry_bound"] == 2 * (1 << 24) * d[4] < (1 << 32)
-    assert 14 <= d[3] <= 21
+    c, nwin, nlo = d[3], d[4], d[11]
+    assert win_bucket(c, nlo, nwin) == pl["nbuckets"]
+    assert pl["entry_bound"] == 2 * (1 << 24) * nwin < (1 << 32)
+    assert 14 <= c <= 22
+    # GLV halves of 127 bits: the windows cover exactly the 128 bits of the
+    # signed recoding, the wider ones on top
+    assert sum(win_width(c, nlo, w) for w in range(nwin)) == 128 and nlo <= nwin
+
+
+@pytest.mark.parametrize("curve,n", [("bn254", 1 << 20), ("bn254", 1 << 22), ("bn254", 1 << 24),
+                                     ("bls12_381", 1 << 22)])
+def test_two_width_layout_covers_scalar(curve, n):
+    """Large plans split the signed recoding's bits + 1 bits into windows
+    whose widths differ by at most one."""
+    cid = zl.BN254 if curve == "bn254" else zl.BLS12_381
+    d = plan(cid, [n])["descs"][0]
+    c, nwin, nlo = d[3], d[4], d[11]
+    widths = [win_width(c, nlo, w) for w in range(nwin)]
+    assert max(widths) - min(widths) <= 1 and widths == sorted(widths)
+    assert sum(widths) - widths[-1] < 128 <= sum(widths)

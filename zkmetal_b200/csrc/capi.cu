@@ -21,6 +21,15 @@ void set_error(const std::string& s) { g_last_error = s; }
 
 static int fp_bytes(int curve) { return curve == ZKMSM_BLS12_381 ? 48 : 32; }
 
+// A window setting: 0 (automatic), a width 2..24, or a two-width layout
+// c | nlo << 16 (nlo >= 1 windows of c = 2..22 bits, then c + 1-bit windows).
+static bool window_setting_ok(int w) {
+    if (w < 0) return false;
+    if (w < 65536) return w != 1 && w <= 24;
+    const int c = w & 0xffff, nlo = w >> 16;
+    return c >= 2 && c <= 22 && nlo >= 1 && nlo <= 256;
+}
+
 // Map exceptions to reference status codes.
 template <class F>
 static ZkMetalStatus guarded(F&& f) {
@@ -67,10 +76,10 @@ static void h2d(Engine& e, DevBuf& buf, const void* src, size_t bytes) {
 // starts; a stripe's compute, ~3 ns per BN254 point, covers the copy of the
 // next, 1.6x longer one at ~1.8 ns per point); stripe s is copied on the
 // engine's copy stream while stripe s-1 is
-// sorted and accumulated on the compute stream.  Every stripe uses the window
-// layout of the whole MSM and fills its own bucket array; the arrays are then
-// added bucket by bucket and reduced once, so the result is the same point as
-// the unstriped MSM.
+// sorted and accumulated on the compute stream.  Every stripe uses one
+// window layout and fills its own bucket array; the arrays are then added
+// bucket by bucket and reduced once, so the result is the same point as the
+// unstriped MSM.
 static std::vector<std::pair<uint32_t, uint32_t>> stripe_ranges(const Engine& e, uint32_t n) {
     std::vector<std::pair<uint32_t, uint32_t>> r;
     int lg = e.stripe_log2;
@@ -100,12 +109,21 @@ static void msm_host_striped(Engine& e, const uint8_t* points, const uint8_t* sc
     using P = typename C::Fp;
     const size_t pb = (size_t)2 * P::N * 4, xs = (size_t)4 * P::N * 4;  // bytes per point, per XYZZ bucket
     const uint32_t S = (uint32_t)rg.size();
-    const uint32_t c = e.get_plan<C>({n}, {0}, fmt, scalar_bits).descs[0].c;
+    // every stripe takes the window layout (width c, and nlo windows of c
+    // bits before the c + 1-bit ones when the widths differ) of the largest
+    // stripe: each stripe fills its own bucket array, so the layout of the
+    // whole n (2^24: 8.4M buckets) would cost a gigabyte per stripe to fill
+    // and fold (BN254 2^24 from host buffers: 59.2 ms, against 57.0 ms with
+    // the 2^23 layout of 1.2M buckets)
+    uint32_t fmax = 0;
+    for (auto& q : rg) fmax = std::max(fmax, q.second);
+    const MsmDesc d0 = e.get_plan<C>({fmax}, {0}, fmt, scalar_bits).descs[0];
+    const uint32_t layout = d0.c | (d0.nlo < d0.nwin ? d0.nlo << 16 : 0u);
     // one plan per distinct stripe length; a lookup may evict the cache, so
     // all are fetched a second time before any is used
     std::map<uint32_t, Plan*> plans;
     for (int pass = 0; pass < 2; pass++)
-        for (auto& q : rg) plans[q.second] = &e.get_plan<C>({q.second}, {0}, fmt, scalar_bits, c);
+        for (auto& q : rg) plans[q.second] = &e.get_plan<C>({q.second}, {0}, fmt, scalar_bits, layout);
     const Plan& p0 = *plans[rg[0].second];
     const bool glv = p0.descs[0].glv;
     const size_t nb = p0.nbuckets;
@@ -281,11 +299,16 @@ static std::string autotune(Engine& e, int min_l2, int max_l2) {
         e.tuning.window_bits = 0;
         e.tuning.window_table.erase({CurveTraits<C>::id * 2 + 1, l2});
         e.tuning.version++;
-        int c0 = (int)e.get_plan<C>({n}, {0}, ZKMSM_SCALAR_MONT).descs[0].c;
+        const MsmDesc d0 = e.get_plan<C>({n}, {0}, ZKMSM_SCALAR_MONT).descs[0];
+        const int c0 = (int)d0.c;
+        // candidates: equal windows of c0 - 2 .. c0 + 2 bits, and the
+        // planner's two-width layout when it chose one (table value 0)
+        const bool two_width = d0.nlo < d0.nwin;
         int best_c = c0;
         float best = 1e30f;
         std::string row;
-        for (int c = std::max(4, c0 - 2); c <= std::min(22, c0 + 2); c++) {
+        for (int c = two_width ? 0 : std::max(4, c0 - 2); c <= std::min(22, c0 + 2); c++) {
+            if (c > 0 && c < std::max(4, c0 - 2)) continue;
             e.tuning.window_bits = c;
             Plan& pl = e.get_plan<C>({n}, {0}, ZKMSM_SCALAR_MONT);
             e.ensure_workspace<C>(pl);
@@ -307,7 +330,8 @@ static std::string autotune(Engine& e, int min_l2, int max_l2) {
         }
         e.tuning.window_table[{CurveTraits<C>::id * 2 + 1, l2}] = best_c;
         rep += (l2 == min_l2 ? "" : ",") + std::string("\"") + std::to_string(l2) + "\":{\"best\":" +
-               std::to_string(best_c) + ",\"model\":" + std::to_string(c0) + ",\"ms\":{" + row + "}}";
+               std::to_string(best_c) + ",\"model\":" + std::to_string(two_width ? 0 : c0) + ",\"ms\":{" + row +
+               "}}";
     }
     rep += "}";
     e.tuning.window_bits = saved_w;
@@ -639,15 +663,15 @@ ZkMetalStatus zkmsm_tuning_load(ZkMetalMSMEngine engine, const char* path) {
     Engine& e = ENG(engine);
     int k, l2, c;
     while (fscanf(f, "%d %d %d", &k, &l2, &c) == 3)
-        if (k >= 0 && k < 4 && l2 >= 0 && l2 < 40 && c >= 2 && c <= 24) e.tuning.window_table[{k, l2}] = c;
+        if (k >= 0 && k < 4 && l2 >= 0 && l2 < 40 && (c == 0 || (c >= 2 && c <= 24)))
+            e.tuning.window_table[{k, l2}] = c;  // 0: the planner's own layout
     fclose(f);
     e.tuning.version++;
     return ZKMETAL_SUCCESS;
 }
 
 ZkMetalStatus zkmsm_engine_set_tuning(ZkMetalMSMEngine engine, int window_bits, int chunk, int glv) {
-    if (!engine || window_bits < 0 || window_bits > 24 || window_bits == 1 || chunk < 0 || chunk > 4096)
-        return ZKMETAL_ERR_INVALID_INPUT;
+    if (!engine || !window_setting_ok(window_bits) || chunk < 0 || chunk > 4096) return ZKMETAL_ERR_INVALID_INPUT;
     Engine& e = ENG(engine);
     e.tuning.window_bits = window_bits;
     e.tuning.chunk = chunk;
@@ -709,7 +733,7 @@ ZkMetalStatus zkmsm_engine_phase_times(ZkMetalMSMEngine engine, double* ms5, uin
 
 static ZkMetalStatus plan_json(int curve, const uint32_t* counts, uint32_t n_msms, int fmt, int window_bits,
                                int chunk, int glv, int scalar_bits, ShiftSpec sh, char* buf, uint64_t buflen) {
-    if (!counts || !buf || n_msms == 0) return ZKMETAL_ERR_INVALID_INPUT;
+    if (!counts || !buf || n_msms == 0 || !window_setting_ok(window_bits)) return ZKMETAL_ERR_INVALID_INPUT;
     return guarded([&] {
         Tuning t;
         t.window_bits = window_bits;
@@ -725,7 +749,8 @@ static ZkMetalStatus plan_json(int curve, const uint32_t* counts, uint32_t n_msm
             s += (i ? "," : "") + std::string("[") + std::to_string(d.scalar_off) + "," + std::to_string(d.n) + "," +
                  std::to_string(d.base_off) + "," + std::to_string(d.c) + "," + std::to_string(d.nwin) + "," +
                  std::to_string(d.glv) + "," + std::to_string(d.bucket_off) + "," + std::to_string(d.fmt) + "," +
-                 std::to_string(d.win_off) + "," + std::to_string(d.wstep) + "," + std::to_string(d.nred) + "]";
+                 std::to_string(d.win_off) + "," + std::to_string(d.wstep) + "," + std::to_string(d.nred) + "," +
+                 std::to_string(d.nlo) + "]";
         }
         s += "],\"entry_bound\":" + std::to_string(pl.entry_bound) + ",\"nbuckets\":" + std::to_string(pl.nbuckets) +
              ",\"sort\":[" + std::to_string(pl.sort_maxd) + "," + std::to_string(pl.sort_spb) + "," +

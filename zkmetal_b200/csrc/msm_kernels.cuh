@@ -185,7 +185,6 @@ struct DigitGen {
 
 ZK_DEV void next_digits(DigitGen& g, const Halves& h, const MsmDesc& d, uint32_t idx, bool (&valid)[DBATCH],
                         uint32_t (&gb)[DBATCH], uint32_t (&val)[DBATCH]) {
-    const uint32_t half = 1u << (d.c - 1);
 #pragma unroll
     for (int s = 0; s < DBATCH; s++) {
         valid[s] = false;
@@ -193,10 +192,11 @@ ZK_DEV void next_digits(DigitGen& g, const Halves& h, const MsmDesc& d, uint32_t
         val[s] = 0;
 #pragma unroll 1
         while (g.j < (uint32_t)h.count) {
-            uint32_t v = bit_field(h.k[g.j], g.w * d.c, d.c) + g.carry;
+            const uint32_t cw = win_width(d, g.w);
+            uint32_t v = bit_field(h.k[g.j], win_bit(d, g.w), cw) + g.carry;
             uint32_t a, dn;
-            if (v > half) {
-                a = (1u << d.c) - v;
+            if (v > (1u << (cw - 1))) {
+                a = (1u << cw) - v;
                 dn = 1;
                 g.carry = 1;
             } else {
@@ -216,7 +216,7 @@ ZK_DEV void next_digits(DigitGen& g, const Halves& h, const MsmDesc& d, uint32_t
                     gb[s] = d.bucket_off + (a - 1);
                     val[s] = (idx + w * d.wstep) | ((h.neg[j] ^ dn) << 31);
                 } else {
-                    gb[s] = d.bucket_off + w * half + (a - 1);
+                    gb[s] = d.bucket_off + win_bucket(d, w) + (a - 1);
                     val[s] = idx | (j << 30) | ((h.neg[j] ^ dn) << 31);
                 }
                 break;
@@ -928,7 +928,7 @@ __global__ void k_combine(const Xyzz<typename C::Fp>* __restrict__ rootS,
     for (int w = (int)d.nred - 1; w >= 0; w--) {
         if (w != (int)d.nred - 1) {
 #pragma unroll 1
-            for (uint32_t b = 0; b < d.c; b++) xyzz_dbl<P, true>(acc, acc);  // one thread: inline products
+            for (uint32_t b = 0; b < win_width(d, w); b++) xyzz_dbl<P, true>(acc, acc);  // one thread: inline products
         }
         load_xyzz(q, rootS + d.win_off + w);
         xyzz_add<P, true>(acc, q);

@@ -139,6 +139,7 @@ extern "C" ZkMetalStatus zkmsm_bn254_msm_noalloc(const void* d_points, const voi
     desc.win_off = 0;
     desc.wstep = 0;
     desc.nred = NWIN;
+    desc.nlo = NWIN;
     RedTask tasks[RED_LEVELS * NWIN];
     uint32_t nin = BPW;
     for (int l = 0; l < RED_LEVELS; l++) {

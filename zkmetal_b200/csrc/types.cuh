@@ -31,7 +31,21 @@ struct MsmDesc {
     // combine).  wstep = 0: ordinary windows, nred = nwin.
     uint32_t wstep;
     uint32_t nred;        // window sums (bucket sets) of this MSM
+    // Window widths: windows [0, nlo) are c bits wide, windows [nlo, nwin)
+    // c + 1 bits (the bits + 1 bits a signed recoding covers, split as evenly
+    // as the window count allows); nlo = nwin: every window c bits.
+    uint32_t nlo;
 };
+
+// Width, first scalar bit and first bucket (relative to bucket_off) of
+// window w of an MSM: windows below nlo have 2^(c-1) buckets, the others 2^c.
+__host__ __device__ inline uint32_t win_width(const MsmDesc& d, uint32_t w) { return d.c + (w >= d.nlo ? 1u : 0u); }
+__host__ __device__ inline uint32_t win_bit(const MsmDesc& d, uint32_t w) {
+    return w * d.c + (w > d.nlo ? w - d.nlo : 0u);
+}
+__host__ __device__ inline uint32_t win_bucket(const MsmDesc& d, uint32_t w) {
+    return (w + (w > d.nlo ? w - d.nlo : 0u)) << (d.c - 1);
+}
 
 // Sorted-entry value: base index (30 bits) | endo << 30 | negate << 31
 constexpr uint32_t VAL_IDX_MASK = 0x3fffffffu;
