@@ -168,8 +168,15 @@ ZK_DEV void xyzz_add(Xyzz<P>& acc, const Xyzz<P>& b) {
     fe_sub(u2, u2, u1);          // P
     fe_sub(s2, s2, s1);          // R
     if (fe_is_zero(u2)) {
-        if (fe_is_zero(s2)) xyzz_dbl_ni(acc, acc);
-        else xyzz_set_id(acc);
+        // P == Q: double.  The inline form doubles inline too: a call would
+        // take acc's address and keep it in local memory for the whole
+        // kernel (twice the latency of a register-resident addition).
+        if (fe_is_zero(s2)) {
+            if (INL) xyzz_dbl<P, true>(acc, acc);
+            else xyzz_dbl_ni(acc, acc);
+        } else {
+            xyzz_set_id(acc);
+        }
         return;
     }
     Fe<P> pp, ppp, t;

@@ -436,6 +436,11 @@ class Engine {
                 d.nwin = d.n ? windows_for(bits, c) : 0;
                 d.nlo = d.nwin;
             }
+            if (d.nwin > MAX_WINDOWS) {  // too narrow for the combine: widen
+                while (windows_for(bits, c) > MAX_WINDOWS) c++;
+                d.c = c;
+                d.nwin = d.nlo = windows_for(bits, c);
+            }
             d.wstep = 0;
             d.nred = d.nwin;
             d.bucket_off = boff;

@@ -141,7 +141,8 @@ void Engine::enqueue_reduce(const Plan& pl, const void* bucket_base, uint32_t* d
         rc ^= 1;
     }
     if (ev) prof_mark(*ev, 4);
-    k_combine<C><<<(nd + 31) / 32, 32, 0, stream>>>(inS, inW, dd, nd, d_results);
+    k_combine<C><<<(nd + COMBINE_WARPS - 1) / COMBINE_WARPS, 32 * COMBINE_WARPS, 0, stream>>>(inS, inW, dd, nd,
+                                                                                              d_results);
     launches++;
     ZK_CUDA(cudaGetLastError());
     if (ev) prof_mark(*ev, 5);

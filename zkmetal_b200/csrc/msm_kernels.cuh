@@ -25,7 +25,8 @@
 //                     20% of all points in one bucket for witness scalars).
 //  6. k_reduce_level  per window sum_b b*B_b by a tree of running sums.
 //                     [msm_kernels.metal:152-248]
-//  7. k_combine       Horner over windows, normalise to affine.
+//  7. k_combine       sum of the windows shifted to their bit offsets (a
+//                     tree over one warp per MSM), normalise to affine.
 //                     [MSMEngine.swift:899-904, msm_kernels.metal:251-275]
 #pragma once
 #include "types.cuh"
@@ -904,46 +905,84 @@ __global__ void __launch_bounds__(128) k_reduce_level(const Xyzz<typename C::Fp>
     store_xyzz(outW + g, x);
 }
 
-// Horner over each MSM's window sums (one sum, no doublings, for a
-// shift-table MSM); output reference-layout Jacobian (X, Y, Z) Montgomery
-// with Z = 1 (or the identity (1, 1, 0)).
+// Window combine, one warp per MSM: R = sum_w 2^bit(w) * (S_w + W_w).  Lane
+// l forms the sums of windows 2l and 2l + 1, folds them into
+// G_l = T_2l + 2^width(2l) T_2l+1 and shifts G_l to its own bit offset,
+// 2^bit(2l) G_l: all lanes double in one converged loop, so the warp spends
+// the largest offset once (the doublings of Horner's rule, no more).  A tree
+// of warp shuffles then adds the G_l: log2(windows) + 3 additions on the
+// critical path instead of two per window.  Lane 0 normalises to affine and
+// writes the reference-layout Jacobian (X, Y, Z) Montgomery with Z = 1 (or
+// the identity (1, 1, 0)).  Up to 64 windows; a shift-table MSM has one
+// window sum and no doublings.
+constexpr uint32_t COMBINE_WARPS = 4;
+
+template <class P>
+ZK_DEV void shfl_down_xyzz(Xyzz<P>& r, const Xyzz<P>& a, uint32_t delta) {
+#pragma unroll
+    for (int i = 0; i < P::N; i++) {
+        r.x.v[i] = __shfl_down_sync(0xffffffffu, a.x.v[i], delta);
+        r.y.v[i] = __shfl_down_sync(0xffffffffu, a.y.v[i], delta);
+        r.zz.v[i] = __shfl_down_sync(0xffffffffu, a.zz.v[i], delta);
+        r.zzz.v[i] = __shfl_down_sync(0xffffffffu, a.zzz.v[i], delta);
+    }
+}
+
 template <class C>
-__global__ void k_combine(const Xyzz<typename C::Fp>* __restrict__ rootS,
-                          const Xyzz<typename C::Fp>* __restrict__ rootW,
-                          const MsmDesc* __restrict__ descs, int nd, uint32_t* __restrict__ out) {
+__global__ void __launch_bounds__(32 * COMBINE_WARPS) k_combine(const Xyzz<typename C::Fp>* __restrict__ rootS,
+                                                               const Xyzz<typename C::Fp>* __restrict__ rootW,
+                                                               const MsmDesc* __restrict__ descs, int nd,
+                                                               uint32_t* __restrict__ out) {
     using P = typename C::Fp;
-    int m = blockIdx.x * blockDim.x + threadIdx.x;
-    if (m >= nd) return;
+    const uint32_t lane = threadIdx.x & 31;
+    const int m = (int)(blockIdx.x * COMBINE_WARPS + (threadIdx.x >> 5));
+    if (m >= nd) return;  // warp-uniform
     const MsmDesc d = descs[m];
-    Xyzz<P> acc, q;
-    xyzz_set_id(acc);
     uint32_t* o = out + (size_t)m * 3 * P::N;
-    if (d.n == 0) {
-        Fe<P> one;
-        fe_set_one(one);
-        for (int l = 0; l < P::N; l++) { o[l] = one.v[l]; o[P::N + l] = one.v[l]; o[2 * P::N + l] = 0; }
-        return;
-    }
-#pragma unroll 1
-    for (int w = (int)d.nred - 1; w >= 0; w--) {
-        if (w != (int)d.nred - 1) {
-#pragma unroll 1
-            for (uint32_t b = 0; b < win_width(d, w); b++) xyzz_dbl<P, true>(acc, acc);  // one thread: inline products
-        }
-        load_xyzz(q, rootS + d.win_off + w);
-        xyzz_add<P, true>(acc, q);
-        load_xyzz(q, rootW + d.win_off + w);
-        xyzz_add<P, true>(acc, q);
-    }
-    Affine<P> a;
-    xyzz_to_affine_ni(a, acc);
     Fe<P> one;
     fe_set_one(one);
-    bool id = xyzz_is_id(acc);
-    for (int l = 0; l < P::N; l++) {
-        o[l] = id ? one.v[l] : a.x.v[l];
-        o[P::N + l] = id ? one.v[l] : a.y.v[l];
-        o[2 * P::N + l] = id ? 0u : one.v[l];
+    if (d.n == 0) {
+        if (lane == 0)
+            for (int l = 0; l < P::N; l++) { o[l] = one.v[l]; o[P::N + l] = one.v[l]; o[2 * P::N + l] = 0; }
+        return;
+    }
+    const uint32_t nw = d.nred;
+    const uint32_t w0 = 2 * lane;
+    Xyzz<P> g, q;
+    xyzz_set_id(g);
+    if (w0 + 1 < nw) {
+        load_xyzz(g, rootS + d.win_off + w0 + 1);
+        load_xyzz(q, rootW + d.win_off + w0 + 1);
+        xyzz_add<P, true>(g, q);
+#pragma unroll 1
+        for (uint32_t b = 0; b < win_width(d, w0); b++) xyzz_dbl<P, true>(g, g);
+    }
+    if (w0 < nw) {
+        load_xyzz(q, rootS + d.win_off + w0);
+        xyzz_add<P, true>(g, q);
+        load_xyzz(q, rootW + d.win_off + w0);
+        xyzz_add<P, true>(g, q);
+    }
+    const uint32_t shift = w0 < nw ? win_bit(d, w0) : 0u;
+#pragma unroll 1
+    for (uint32_t b = 0; b < shift; b++) xyzz_dbl<P, true>(g, g);
+#pragma unroll 1
+    for (uint32_t st = 1; st < 32; st <<= 1) {
+        shfl_down_xyzz(q, g, st);  // every lane takes part in the shuffle
+        if ((lane & (2 * st - 1)) == 0 && 2 * (lane + st) < nw) xyzz_add<P, true>(g, q);
+    }
+    if (lane == 0) {
+        // normalise a copy: passing g itself to the out-of-line call would
+        // take its address and keep it in local memory through the loops
+        Xyzz<P> t = g;
+        Affine<P> a;
+        xyzz_to_affine_ni(a, t);
+        const bool id = xyzz_is_id(g);
+        for (int l = 0; l < P::N; l++) {
+            o[l] = id ? one.v[l] : a.x.v[l];
+            o[P::N + l] = id ? one.v[l] : a.y.v[l];
+            o[2 * P::N + l] = id ? 0u : one.v[l];
+        }
     }
 }
 

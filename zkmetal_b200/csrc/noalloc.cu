@@ -221,7 +221,7 @@ extern "C" ZkMetalStatus zkmsm_bn254_msm_noalloc(const void* d_points, const voi
         inS = rS[l & 1];
         inW = rW[l & 1];
     }
-    k_combine<C><<<1, 32, 0, s>>>(inS, inW, dd, 1, static_cast<uint32_t*>(d_result));
+    k_combine<C><<<1, 32 * COMBINE_WARPS, 0, s>>>(inS, inW, dd, 1, static_cast<uint32_t*>(d_result));
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) {
         set_error(std::string("zkmsm_bn254_msm_noalloc: launch failed: ") + cudaGetErrorString(e));

@@ -37,6 +37,10 @@ struct MsmDesc {
     uint32_t nlo;
 };
 
+// Most window sums one MSM may have: the window combine holds two per lane
+// of one warp.
+constexpr uint32_t MAX_WINDOWS = 64;
+
 // Width, first scalar bit and first bucket (relative to bucket_off) of
 // window w of an MSM: windows below nlo have 2^(c-1) buckets, the others 2^c.
 __host__ __device__ inline uint32_t win_width(const MsmDesc& d, uint32_t w) { return d.c + (w >= d.nlo ? 1u : 0u); }
