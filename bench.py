@@ -229,6 +229,39 @@ def run_small_config(eng, pts, sc, stream, log2n=20, steps=20):
             "speedup_e2e_vs_published": round(pub / e2e, 1), "note": "published figure is other hardware"}
 
 
+def run_witness_config(eng, pts, stream, n_max, seed=0x5EED0001, steps=5):
+    """Witness-like scalars (40% zero, 20% one, 25% below 2^32, 15% uniform in
+    Fr) on the same device-resident bases, at 2^20 and at the headline size:
+    device ms per MSM (CUDA events on the library's stream)."""
+    import torch
+    from zkmetal_b200 import lib as zl
+    L = zl.lib()
+    sc = _dev(torch, n_max * 32)
+    torch.cuda.synchronize()
+    assert L.zkmsm_gen_scalars(eng.handle, 0, seed + 7, 0, n_max, 1, 1, sc.data_ptr()) == 0
+    res = torch.empty(96, dtype=torch.uint8, device="cuda")
+    out = {"distribution": "40% 0, 20% 1, 25% uniform below 2^32, 15% uniform in Fr (Montgomery form)"}
+    for lg in (20, n_max.bit_length() - 1):
+        n = 1 << lg
+
+        def step():
+            assert L.zkmsm_msm_device_async(eng.handle, 0, pts.data_ptr(), None, sc.data_ptr(), 1, n,
+                                            res.data_ptr(), stream.cuda_stream) == 0
+
+        for _ in range(3):
+            step()
+        torch.cuda.synchronize()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        for _ in range(steps):
+            step()
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        out["device_ms_2p%d" % lg] = round(ev0.elapsed_time(ev1) / steps, 3)
+    del sc
+    return out
+
+
 # Window-shift spacing of the resident tables of the batched and served
 # configurations (zkmsm_table_precompute): copy k = 2^(4k) * P.
 SHIFT_SPACING = 4
@@ -682,18 +715,34 @@ def run_ours(args):
             "sample": "one %d-point BN254 MSM (first shard of the same inputs), reference C Pippenger, "
                       "%d OpenMP threads, time x%g to 2^%d" % (n_sample, threads, scale, args.log2n)}
     if world == 1 and not args.no_extras:
+        def release():
+            # buffers of the previous configuration go back to the driver, so
+            # that the next one (the server sizes its budget from free device
+            # memory) sees the whole device
+            import gc
+            gc.collect()
+            torch.cuda.synchronize()
+            torch.cuda.empty_cache()
+
         try:
             line["bn254_2p20"] = run_small_config(eng, pts, sc, stream, log2n=20)
         except Exception as exc:  # reported, not hidden
             line["bn254_2p20"] = {"error": repr(exc)}
         try:
+            line["witness"] = run_witness_config(eng, pts, stream, n)
+        except Exception as exc:  # reported, not hidden
+            line["witness"] = {"error": repr(exc)}
+        release()
+        try:
             line["batch"] = run_batch_config()
         except Exception as exc:  # reported, not hidden
             line["batch"] = {"error": repr(exc)}
+        release()
         try:
             line["bls12_381"] = run_bls_config()
         except Exception as exc:
             line["bls12_381"] = {"error": repr(exc)}
+        release()
         try:
             line["serve"] = run_serve_config(duration_s=args.serve_seconds, plain_sample=40)
         except Exception as exc:

@@ -237,6 +237,48 @@ class CommitmentTable:
                                 raw[i * 3 * fb + 2 * fb:(i + 1) * 3 * fb]) for i in range(len(counts))]
 
 
+class KZGEngine:
+    """Polynomial commitments over a resident SRS: a mirror of the reference's
+    ``KZGEngine.commit`` / ``batchCommit`` (KZG/KZGEngine.swift:132-170) and
+    ``GPUCommitmentBatchEngine.commit`` / ``batchCommit``
+    (Commitment/GPUCommitmentBatchEngine.swift:263-300).
+
+    ``srs``: affine points (n x 64 B BN254 or n x 96 B BLS12-381, Montgomery),
+    kept resident in HBM as a ``CommitmentTable`` with its window shifts
+    (``shift_bits``, 0 = none).  ``commit(coeffs)`` takes Fr coefficients in
+    Montgomery form (n x 32 B, the memory layout of the reference's ``[Fr]``)
+    and returns ``MSM(SRS[0..n), coeffs)``; the Fr -> integer conversion runs
+    on the device.  ``batchCommit`` commits any number of polynomials of any
+    lengths in one batched launch (the reference runs uneven lengths one by
+    one).  A polynomial longer than the SRS, or an empty one, raises
+    ``MSMError("invalidInput")``."""
+
+    def __init__(self, srs, engine=None, shift_bits=4):
+        self.engine = engine if engine is not None else MetalMSM()
+        self.table = CommitmentTable(self.engine, srs)
+        if shift_bits:
+            self.table.precompute(shift_bits)
+
+    @property
+    def srs_size(self):
+        return self.table.n
+
+    def commit(self, coeffs):
+        return self.batchCommit([coeffs])[0]
+
+    def batchCommit(self, polynomials):
+        if len(polynomials) == 0:
+            return []
+        arrays = [as_bytes_array(p, 32) for p in polynomials]
+        counts = [a.size // 32 for a in arrays]
+        if min(counts) == 0 or max(counts) > self.table.n:
+            raise MSMError("invalidInput", "polynomial empty or longer than the SRS (%d points)" % self.table.n)
+        return self.table.batch_commit(np.concatenate(arrays), counts, fmt=_l.SCALAR_MONT)
+
+    def close(self):
+        self.table.close()
+
+
 class CommitmentServer:
     """Continuous-batching commitment server over resident tables (new API).
 
