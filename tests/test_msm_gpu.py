@@ -103,10 +103,17 @@ def test_edge_cases(eng, curve):
         ([P, G], [(1 << 256) - 1, (1 << 255)]),
         ([G] * 40, [1] * 40),                           # one hot bucket
     ]
-    for pts, sc in cases:
-        want = C.enc_affine(R.naive_msm(C, pts, sc))
-        got = aff(C, eng[curve].msm(R.pack_points(C, pts), R.pack_scalars_int(sc)))
-        assert got == want, (pts, sc)
+    L = zl.lib()
+    try:
+        # default plan, a two-width layout (c | nlo << 16), and no GLV
+        for window, glv in ((0, -1), (5 | 10 << 16, 1), (6 | 3 << 16, 0)):
+            check(L.zkmsm_engine_set_tuning(eng[curve].handle, window, 0, glv))
+            for pts, sc in cases:
+                want = C.enc_affine(R.naive_msm(C, pts, sc))
+                got = aff(C, eng[curve].msm(R.pack_points(C, pts), R.pack_scalars_int(sc)))
+                assert got == want, (window, glv, pts, sc)
+    finally:
+        check(L.zkmsm_engine_set_tuning(eng[curve].handle, 0, 0, -1))
 
 
 def test_invalid_inputs(eng):

@@ -166,3 +166,37 @@ def test_server_over_shift_tables(eng):
         srv.close()
         for t in tabs.values():
             t.close()
+
+
+@pytest.mark.parametrize("curve", ["bn254", "bls12_381"])
+def test_shift_edge_cases(eng, curve):
+    """Duplicate bases (the doubling path), cancellation, identity bases,
+    zero and unreduced scalars and a hot bucket, over shift tables."""
+    C = R.CURVES[curve]
+    G = (C.gx, C.gy)
+    P = R.scalar_mul(C, G, 987654321)
+    Q = R.aff_neg(C, P)
+    cases = [
+        ([P, P, P], [3, 3, 3]),
+        ([P, Q], [9, 9]),
+        ([P, Q, P], [9, 9, 2]),
+        ([None, P, None], [5, 7, 11]),
+        ([P, G], [0, 0]),
+        ([P, G], [1, 1]),
+        ([P, G, P], [C.r - 1, C.r, C.r + 5]),
+        ([P, G], [(1 << 256) - 1, (1 << 255)]),
+        ([G] * 40, [1] * 40),
+        ([P, P], [1 << 200, 1 << 200]),          # equal shifted copies in one bucket
+    ]
+    for pts, sc in cases:
+        t = CommitmentTable(eng[curve], R.pack_points(C, pts))
+        try:
+            t.precompute(4)
+            # two MSMs: the whole case, then its first point alone (one scalar each)
+            r = t.batch_commit(R.pack_scalars_int(sc + sc[:1]), [len(pts), 1], fmt=zl.SCALAR_INT)
+            assert jac_to_affine_bytes(C, r[0].x + r[0].y + r[0].z) == C.enc_affine(R.naive_msm(C, pts, sc)), \
+                (pts, sc)
+            assert jac_to_affine_bytes(C, r[1].x + r[1].y + r[1].z) == \
+                C.enc_affine(R.naive_msm(C, pts[:1], sc[:1]))
+        finally:
+            t.close()
