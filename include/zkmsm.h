@@ -110,6 +110,21 @@ ZkMetalStatus zkmetal_bls12_381_g1_msm_batch(ZkMetalMSMEngine engine, const uint
                                              const uint8_t* all_scalars, const uint32_t* counts,
                                              uint32_t n_msms, uint8_t* results);
 
+/* ---- BLS12-377 G1 MSM ---------------------------------------------------
+ * NEW symbols, the same shapes as the BLS12-381 ones (96 B points, 48 B
+ * coordinates).  They replace the Swift API BLS12377MSM.msm
+ * (MSM/BLS12377MSMEngine.swift:266) and the C g1 Pippenger
+ * (NeonFieldOps/bls12_377_ops.c:1476, GLV form :1814). */
+ZkMetalStatus zkmetal_bls12_377_g1_msm(ZkMetalMSMEngine engine, const uint8_t* points, const uint8_t* scalars,
+                                       uint32_t n_points, uint8_t* result_x, uint8_t* result_y,
+                                       uint8_t* result_z);
+ZkMetalStatus zkmetal_bls12_377_g1_msm_fr(ZkMetalMSMEngine engine, const uint8_t* points,
+                                          const uint8_t* scalars_mont, uint32_t n_points, uint8_t* result_x,
+                                          uint8_t* result_y, uint8_t* result_z);
+ZkMetalStatus zkmetal_bls12_377_g1_msm_batch(ZkMetalMSMEngine engine, const uint8_t* all_points,
+                                             const uint8_t* all_scalars, const uint32_t* counts,
+                                             uint32_t n_msms, uint8_t* results);
+
 /* ---- misc: zkmetal.h:520-530 --------------------------------------------- */
 /* replaces zkmetal_set_shader_dir (zkmetal.h:524): accepted and ignored (no shaders) */
 void zkmetal_set_shader_dir(const char* path);
@@ -123,6 +138,7 @@ const char* zkmetal_version(void);
 /* Curve selector for the entry points below. */
 #define ZKMSM_BN254 0
 #define ZKMSM_BLS12_381 1
+#define ZKMSM_BLS12_377 2
 /* Scalar encoding */
 #define ZKMSM_SCALAR_INT 0
 #define ZKMSM_SCALAR_MONT 1

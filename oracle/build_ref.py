@@ -1,17 +1,20 @@
 #!/usr/bin/env python3
 """Build recipe for the reference's own CPU Pippenger (test infrastructure only).
 
-This is the CHECKER, never the product.  It compiles the reference's two C
+This is the CHECKER, never the product.  It compiles the reference's three C
 translation units that hold the MSM path,
 
     Sources/NeonFieldOps/bn254_msm.c       (bn254_pippenger_msm, :1145-1187)
     Sources/NeonFieldOps/bls12_381_ops.c   (bls12_381_g1_pippenger_msm, :1141-1165)
+    Sources/NeonFieldOps/bls12_377_ops.c   (bls12_377_g1_pippenger_msm, :1476-1550,
+                                            bls12_377_g1_scalar_mul, :1301)
 
 from where they lie in the read-only reference checkout into
 ``oracle/_ref/libzkref.so`` (git-ignored; it travels to the GPU host with the
 rest of the working tree so the CPU baseline and the parity tests can use it
 there without the reference checkout).  Intermediate files stay in a
-temporary directory; only the library is written to ``oracle/_ref``.
+temporary directory under ``oracle/_ref`` that is removed after the link;
+only the library remains.
 
 The only change made on the way is mechanical and concerns threading, not
 arithmetic: the reference uses Apple GCD blocks
@@ -35,7 +38,8 @@ import tempfile
 HERE = os.path.dirname(os.path.abspath(__file__))
 OUT = os.path.join(HERE, "_ref")
 LIB = os.path.join(OUT, "libzkref.so")
-SOURCES = ["Sources/NeonFieldOps/bn254_msm.c", "Sources/NeonFieldOps/bls12_381_ops.c"]
+SOURCES = ["Sources/NeonFieldOps/bn254_msm.c", "Sources/NeonFieldOps/bls12_381_ops.c",
+           "Sources/NeonFieldOps/bls12_377_ops.c"]
 HEADER_DIR = "Sources/NeonFieldOps/include"
 
 
@@ -119,7 +123,7 @@ def build(ref_root, force=False, cc="gcc"):
     os.makedirs(OUT, exist_ok=True)
     # the rewritten translation units and objects are build intermediates:
     # they live in a temporary directory and only the library is kept
-    with tempfile.TemporaryDirectory(prefix="zkref_") as tmpd:
+    with tempfile.TemporaryDirectory(prefix="build_", dir=OUT) as tmpd:
         inc = os.path.join(tmpd, "include")
         os.makedirs(os.path.join(inc, "dispatch"))
         with open(os.path.join(inc, "dispatch", "dispatch.h"), "w") as f:

@@ -2,7 +2,8 @@
 
 ``RefOracle`` binds the reference's own C Pippenger built by
 ``oracle/build_ref.py`` (bn254_pippenger_msm, bn254_msm.c:1145-1187;
-bls12_381_g1_pippenger_msm, bls12_381_ops.c:1141-1165).  ``COracle`` binds the
+bls12_381_g1_pippenger_msm, bls12_381_ops.c:1141-1165;
+bls12_377_g1_pippenger_msm, bls12_377_ops.c:1476).  ``COracle`` binds the
 C restatement ``oracle/cmsm.c``.  Both take and return the reference byte
 layouts (affine points Montgomery LE, integer scalars 8x u32 LE) and results
 are compared after normalising to affine, which is unique per group element.
@@ -18,8 +19,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 REF_LIB = os.path.join(HERE, "_ref", "libzkref.so")
 CMSM_LIB = os.path.join(HERE, "_build", "libcmsm.so")
 
-CURVE_ID = {"bn254": 0, "bls12_381": 1}
-FP_BYTES = {"bn254": 32, "bls12_381": 48}
+CURVE_ID = {"bn254": 0, "bls12_381": 1, "bls12_377": 2}
+FP_BYTES = {"bn254": 32, "bls12_381": 48, "bls12_377": 48}
 
 _u64p = ctypes.POINTER(ctypes.c_uint64)
 _u32p = ctypes.POINTER(ctypes.c_uint32)
@@ -98,8 +99,10 @@ class RefOracle:
             raise FileNotFoundError(path + " (run: python oracle/build_ref.py)")
         self.lib = ctypes.CDLL(path)
         L = self.lib
-        for f in ("bn254_pippenger_msm", "bls12_381_g1_pippenger_msm"):
+        for f in ("bn254_pippenger_msm", "bls12_381_g1_pippenger_msm", "bls12_377_g1_pippenger_msm"):
             getattr(L, f).argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]
+        L.bls12_377_g1_to_affine.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+        L.bls12_377_fr_mul.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
         L.bn254_projective_to_affine.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
         L.bn254_fr_batch_to_limbs.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int]
         L.bls12_381_fr_mul.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
@@ -116,7 +119,8 @@ class RefOracle:
         pts = np.frombuffer(points, dtype=np.uint8)
         sc = np.frombuffer(scalars_int, dtype=np.uint8)
         out = np.zeros(3 * FP_BYTES[curve], dtype=np.uint8)
-        f = self.lib.bn254_pippenger_msm if curve == "bn254" else self.lib.bls12_381_g1_pippenger_msm
+        f = {"bn254": self.lib.bn254_pippenger_msm, "bls12_381": self.lib.bls12_381_g1_pippenger_msm,
+             "bls12_377": self.lib.bls12_377_g1_pippenger_msm}[curve]
         f(pts.ctypes.data, sc.ctypes.data, int(n), out.ctypes.data)
         return out.tobytes()
 
@@ -126,6 +130,11 @@ class RefOracle:
             j = np.frombuffer(jac, dtype=np.uint8)
             out = np.zeros(64, dtype=np.uint8)
             self.lib.bn254_projective_to_affine(j.ctypes.data, out.ctypes.data)
+            return out.tobytes()
+        if curve == "bls12_377":
+            j = np.frombuffer(jac, dtype=np.uint8)
+            out = np.zeros(96, dtype=np.uint8)
+            self.lib.bls12_377_g1_to_affine(j.ctypes.data, out.ctypes.data)
             return out.tobytes()
         # the reference exports no BLS12-381 Jacobian->affine; normalise with the restatement
         return self._conv().jacobian_to_affine(curve, jac)
@@ -139,8 +148,9 @@ class RefOracle:
             one = np.array([1, 0, 0, 0], dtype=np.uint64)
             mv = m.view(np.uint64).reshape(-1, 4)
             ov = out.view(np.uint64).reshape(-1, 4)
+            mul = self.lib.bls12_381_fr_mul if curve == "bls12_381" else self.lib.bls12_377_fr_mul
             for i in range(n):
-                self.lib.bls12_381_fr_mul(mv[i].ctypes.data, one.ctypes.data, ov[i].ctypes.data)
+                mul(mv[i].ctypes.data, one.ctypes.data, ov[i].ctypes.data)
         return out.tobytes()
 
 

@@ -10,7 +10,8 @@ restatement (``oracle/cmsm.c``) and the reference's own C Pippenger
 What it restates, with the reference location each part follows:
 
 * Field / point formats: affine points are (x, y) in Montgomery form, little
-  endian, 8x u32 (BN254, R = 2^256) or 12x u32 (BLS12-381, R = 2^384); the
+  endian, 8x u32 (BN254, R = 2^256) or 12x u32 (BLS12-381 and BLS12-377,
+  R = 2^384); the
   affine identity is (0, 0); Jacobian identity has Z = 0
   (zkMetal-ffi/include/zkmetal.h:4-6, NeonFieldOps/bn254_msm.c:1502-1514,
   MSM/PointOperations.swift:6-42, Curve/BLS12381Curve.swift:11-31).
@@ -481,4 +482,13 @@ BLS12_381 = Curve(
     gy=0x08b3f481e3aaa0f1a09e30ed741d8ae4fcf5e095d5d00af600db18cb2c04b3edd03cc744a2888ae40caa232946c5e7e1,
     limbs32=12)
 
-CURVES = {"bn254": BN254, "bls12_381": BLS12_381}
+BLS12_377 = Curve(
+    "bls12_377",
+    p=0x01ae3a4617c510eac63b05c06ca1493b1a22d9f300f5138f1ef3622fba094800170b5d44300000008508c00000000001,
+    r=0x12ab655e9a2ca55660b44d1e5c37b00159aa76fed00000010a11800000000001,
+    b=1,
+    gx=81937999373150964239938255573465948239988671502647976594219695644855304257327692006745978603320413799295628339695,
+    gy=241266749859715473739788878240585681733927191168601896383759122102112907357779751001206799952863815012735208165030,
+    limbs32=12)
+
+CURVES = {"bn254": BN254, "bls12_381": BLS12_381, "bls12_377": BLS12_377}

@@ -11,6 +11,9 @@ if ROOT not in sys.path:
 def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a B200 (sm_100a) CUDA device")
     config.addinivalue_line("markers", "slow: long-running parity case")
+    # temporary files of the tests stay inside the repository (git-ignored)
+    if not config.option.basetemp:
+        config.option.basetemp = os.path.join(ROOT, "tests", "_tmp")
 
 
 @pytest.fixture(scope="session")

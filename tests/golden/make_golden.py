@@ -12,7 +12,8 @@ change to the generator is caught instead of silently changing the inputs.
 Also stored: the known-answer shapes of the reference tests
 (Tests/zkMetalTests/MSMTests.swift:7-62, DASTests.swift:8-150): 5*G,
 MSM([G, 42G], [7, 11]) = 469*G on BLS12-381, 16-point zero-padded version,
-scalar 0 -> identity, scalar 1 -> point.
+scalar 0 -> identity, scalar 1 -> point; BLS12-377 cases from the reference's
+bls12_377_g1_pippenger_msm (NeonFieldOps/bls12_377_ops.c:1476).
 
 Run (needs the reference checkout to build the C oracle):
     python tests/golden/make_golden.py
@@ -42,6 +43,10 @@ CASES = [
     ("bls12_381", 22, 40, "uniform", True),
     ("bls12_381", 23, 40, "witness", True),
     ("bls12_381", 24, 200, "uniform", False),
+    ("bls12_377", 31, 1, "uniform", True),
+    ("bls12_377", 32, 40, "uniform", True),
+    ("bls12_377", 33, 40, "witness", True),
+    ("bls12_377", 34, 200, "uniform", False),
 ]
 
 
@@ -71,7 +76,7 @@ def main():
                                  result_affine=res.hex(), checked_naive=naive))
         print(curve, seed, n, dist, res.hex()[:16])
     # known answers
-    for C in (R.BN254, R.BLS12_381):
+    for C in (R.BN254, R.BLS12_381, R.BLS12_377):
         G = (C.gx, C.gy)
         five = R.scalar_mul(C, G, 5)
         out["kat"].append(dict(curve=C.name, name="5G", points=[C.enc_affine(G).hex()], scalars=[5],
@@ -89,7 +94,7 @@ def main():
     assert got16 == want
     out["kat"].append(dict(curve=C.name, name="SRS42[:16]*[7,11,0..]=469G", points=[C.enc_affine(P).hex() for P in srs],
                            scalars=sc16, result_affine=want.hex()))
-    for C in (R.BN254, R.BLS12_381):
+    for C in (R.BN254, R.BLS12_381, R.BLS12_377):
         G = (C.gx, C.gy)
         out["kat"].append(dict(curve=C.name, name="0*G=identity", points=[C.enc_affine(G).hex()], scalars=[0],
                                result_affine=C.enc_affine(None).hex()))

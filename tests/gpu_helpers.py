@@ -8,7 +8,7 @@ import torch
 from oracle import pyref as R
 from zkmetal_b200 import lib as zl
 
-CURVE_ID = {"bn254": zl.BN254, "bls12_381": zl.BLS12_381}
+CURVE_ID = {"bn254": zl.BN254, "bls12_381": zl.BLS12_381, "bls12_377": zl.BLS12_377}
 
 
 def dev(nbytes):

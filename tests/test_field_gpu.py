@@ -16,7 +16,8 @@ import torch
 from oracle import pyref as R
 from zkmetal_b200 import lib as zl
 
-CASES = [("bn254", R.BN254, 8, zl.BN254), ("bls12_381", R.BLS12_381, 12, zl.BLS12_381)]
+CASES = [("bn254", R.BN254, 8, zl.BN254), ("bls12_381", R.BLS12_381, 12, zl.BLS12_381),
+         ("bls12_377", R.BLS12_377, 12, zl.BLS12_377)]
 
 
 def _limbs(vals, n):

@@ -20,20 +20,26 @@ import torch
 from oracle import pyref as R
 from tests.gpu_helpers import (CURVE_ID, check, gen_inputs, jac_to_affine_bytes, msm_device, np_bytes, oracle_msm,
                                to_host)
-from zkmetal_b200 import BLS12381MSM, CommitmentTable, MetalMSM, MSMError, multiMSM
+from zkmetal_b200 import BLS12377MSM, BLS12381MSM, CommitmentTable, MetalMSM, MSMError, multiMSM
 from zkmetal_b200 import lib as zl
 
 pytestmark = pytest.mark.gpu
 
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "msm_golden.json")
-ENGINES = {"bn254": MetalMSM, "bls12_381": BLS12381MSM}
+ENGINES = {"bn254": MetalMSM, "bls12_381": BLS12381MSM, "bls12_377": BLS12377MSM}
+CURVES3 = ["bn254", "bls12_381", "bls12_377"]
+# drop-in host entry points per curve: integer scalars, Montgomery scalars, batch
+FR_FN = {"bn254": "zkmetal_bn254_msm_fr", "bls12_381": "zkmetal_bls12_381_g1_msm_fr",
+         "bls12_377": "zkmetal_bls12_377_g1_msm_fr"}
+BATCH_FN = {"bn254": "zkmetal_bn254_msm_batch", "bls12_381": "zkmetal_bls12_381_g1_msm_batch",
+            "bls12_377": "zkmetal_bls12_377_g1_msm_batch"}
 
 
 @pytest.fixture(scope="module")
 def eng():
     if not torch.cuda.is_available():
         pytest.skip("no CUDA device")
-    return {"bn254": MetalMSM(), "bls12_381": BLS12381MSM()}
+    return {"bn254": MetalMSM(), "bls12_381": BLS12381MSM(), "bls12_377": BLS12377MSM()}
 
 
 def aff(C, res):
@@ -44,7 +50,7 @@ def test_gpu_available(eng):
     assert zl.lib().zkmetal_gpu_available() == 1
 
 
-@pytest.mark.parametrize("curve", ["bn254", "bls12_381"])
+@pytest.mark.parametrize("curve", CURVES3)
 def test_5G(eng, curve):
     C = R.CURVES[curve]
     G = (C.gx, C.gy)
@@ -75,7 +81,7 @@ def test_golden_kats(eng, kat):
     assert aff(C, r) == bytes.fromhex(kat["result_affine"])
 
 
-@pytest.mark.parametrize("curve", ["bn254", "bls12_381"])
+@pytest.mark.parametrize("curve", CURVES3)
 def test_prefixes_vs_naive(eng, curve):
     """MSMTests.swift:56-62 shape: n in {1, 2, 4, ..., 64} against naive sums."""
     C = R.CURVES[curve]
@@ -86,7 +92,7 @@ def test_prefixes_vs_naive(eng, curve):
         assert aff(C, eng[curve].msm(R.pack_points(C, pts[:n]), R.pack_scalars_int(sc[:n]))) == want, n
 
 
-@pytest.mark.parametrize("curve", ["bn254", "bls12_381"])
+@pytest.mark.parametrize("curve", CURVES3)
 def test_edge_cases(eng, curve):
     C = R.CURVES[curve]
     G = (C.gx, C.gy)
@@ -128,7 +134,7 @@ def test_invalid_inputs(eng):
     assert zl.lib().zkmetal_bn254_msm_batch(e.handle, buf, buf, buf, 0, buf) == zl.ERR_INVALID_INPUT
 
 
-@pytest.mark.parametrize("curve", ["bn254", "bls12_381"])
+@pytest.mark.parametrize("curve", CURVES3)
 def test_generator_matches_restatement(eng, curve):
     C = R.CURVES[curve]
     n = 12
@@ -144,7 +150,8 @@ def test_generator_matches_restatement(eng, curve):
 @pytest.mark.parametrize("curve,n,dist", [("bn254", 4096, "uniform"), ("bn254", 4096, "witness"),
                                           ("bn254", 1 << 16, "uniform"), ("bn254", 1 << 16, "witness"),
                                           ("bls12_381", 4096, "uniform"), ("bls12_381", 1 << 16, "witness"),
-                                          ("bls12_381", 1 << 16, "uniform")])
+                                          ("bls12_381", 1 << 16, "uniform"), ("bls12_377", 4096, "uniform"),
+                                          ("bls12_377", 4096, "witness"), ("bls12_377", 1 << 16, "uniform")])
 def test_vs_reference_c(eng, oracles, curve, n, dist):
     ref, cm = oracles
     orc = ref if ref is not None else cm
@@ -155,7 +162,7 @@ def test_vs_reference_c(eng, oracles, curve, n, dist):
     assert got == want
 
 
-@pytest.mark.parametrize("curve", ["bn254", "bls12_381"])
+@pytest.mark.parametrize("curve", CURVES3)
 def test_tuning_invariance(eng, oracles, curve):
     """Window width, chunk length and GLV on/off change the schedule, never the result."""
     ref, cm = oracles
@@ -179,7 +186,7 @@ def test_tuning_invariance(eng, oracles, curve):
     assert jac_to_affine_bytes(C, results.pop()) == oracle_msm(orc, curve, to_host(p), to_host(s), n, zl.SCALAR_INT)
 
 
-@pytest.mark.parametrize("curve", ["bn254", "bls12_381"])
+@pytest.mark.parametrize("curve", CURVES3)
 def test_determinism_across_runs_and_engines(eng, curve):
     C = R.CURVES[curve]
     n = 32768
@@ -209,7 +216,7 @@ def test_small_scalar_variants(eng):
         assert jac_to_affine_bytes(C, rx.raw + ry.raw + rz.raw) == C.enc_affine(R.naive_msm(C, pts, sc))
 
 
-@pytest.mark.parametrize("curve", ["bn254", "bls12_381"])
+@pytest.mark.parametrize("curve", CURVES3)
 @pytest.mark.parametrize("dist", ["uniform", "witness"])
 def test_striped_host_msm_matches_unstriped(eng, oracles, curve, dist):
     """Host-buffer MSMs streamed in stripes (consecutive point ranges, the
@@ -224,7 +231,7 @@ def test_striped_host_msm_matches_unstriped(eng, oracles, curve, dist):
     p, s = gen_inputs(E, curve, 901, n, dist, zl.SCALAR_MONT)
     pb = np.frombuffer(to_host(p), dtype=np.uint8).copy()
     sb = np.frombuffer(to_host(s), dtype=np.uint8).copy()
-    fn = L.zkmetal_bn254_msm_fr if curve == "bn254" else L.zkmetal_bls12_381_g1_msm_fr
+    fn = getattr(L, FR_FN[curve])
     outs = []
     for stripe_log2 in (0, 12, 11, 13):
         check(L.zkmsm_engine_set_stripe(E.handle, stripe_log2))
@@ -241,7 +248,7 @@ def test_striped_host_msm_matches_unstriped(eng, oracles, curve, dist):
     E.close()
 
 
-@pytest.mark.parametrize("curve", ["bn254", "bls12_381"])
+@pytest.mark.parametrize("curve", CURVES3)
 def test_batch_entry_point_matches_plain(eng, curve):
     """zkmetal_*_msm_batch: concatenated inputs, count 0 -> 96/144 zero bytes
     (zkMetal_ffi.swift:1260-1264); each result equals its own plain call."""
@@ -254,7 +261,7 @@ def test_batch_entry_point_matches_plain(eng, curve):
     pb, sb = np_bytes(R.pack_points(C, pts)), np_bytes(R.pack_scalars_int(sc))
     cnt = np.array(counts, dtype=np.uint32)
     out = ctypes.create_string_buffer(len(counts) * 3 * C.fp_bytes)
-    fn = zl.lib().zkmetal_bn254_msm_batch if curve == "bn254" else zl.lib().zkmetal_bls12_381_g1_msm_batch
+    fn = getattr(zl.lib(), BATCH_FN[curve])
     check(fn(e.handle, pb.ctypes.data, sb.ctypes.data, cnt.ctypes.data, len(counts), out))
     f3 = 3 * C.fp_bytes
     off = 0
@@ -269,7 +276,7 @@ def test_batch_entry_point_matches_plain(eng, curve):
         off += c
 
 
-@pytest.mark.parametrize("curve", ["bn254", "bls12_381"])
+@pytest.mark.parametrize("curve", CURVES3)
 def test_resident_table_batch_commit(eng, curve):
     """Many uneven MSMs over prefixes of one resident table, bit-exact against
     separate plain calls (the batched-commitments pattern)."""
@@ -311,7 +318,8 @@ def test_multi_msm_matches_single(eng):
 
 
 @pytest.mark.slow
-@pytest.mark.parametrize("curve,dist", [("bn254", "uniform"), ("bn254", "witness"), ("bls12_381", "uniform")])
+@pytest.mark.parametrize("curve,dist", [("bn254", "uniform"), ("bn254", "witness"), ("bls12_381", "uniform"),
+                                        ("bls12_377", "uniform")])
 def test_2_20_vs_reference_c(eng, oracles, curve, dist):
     ref, cm = oracles
     orc = ref if ref is not None else cm

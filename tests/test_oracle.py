@@ -45,7 +45,7 @@ def test_golden_kats(kat, oracles):
     assert cm.msm(C.name, pb, sb, len(kat["scalars"])) == bytes.fromhex(kat["result_affine"])
 
 
-@pytest.mark.parametrize("curve", ["bn254", "bls12_381"])
+@pytest.mark.parametrize("curve", ["bn254", "bls12_381", "bls12_377"])
 def test_edge_cases_restatements_agree(curve, oracles):
     """Duplicate bases, P + (-P), identity bases, zero / one / r-1 / 2^256-1
     scalars: cases the reference tests do not cover."""
@@ -68,7 +68,7 @@ def test_edge_cases_restatements_agree(curve, oracles):
     assert cm.msm(curve, R.pack_points(C, pts2), R.pack_scalars_int(sc2), 2) == bytes(2 * C.fp_bytes)
 
 
-@pytest.mark.parametrize("curve", ["bn254", "bls12_381"])
+@pytest.mark.parametrize("curve", ["bn254", "bls12_381", "bls12_377"])
 def test_glv_split_bound(curve):
     """k = k1 + k2*lambda (mod r) and |k_i| < 2^HALF_BITS over random and
     edge scalars (the bound fixes the signed window count)."""
@@ -87,7 +87,7 @@ def test_glv_split_bound(curve):
 
 
 def test_endomorphism_constants():
-    for C in (R.BN254, R.BLS12_381):
+    for C in (R.BN254, R.BLS12_381, R.BLS12_377):
         assert pow(C.beta, 3, C.p) == 1 and C.beta != 1
         assert (C.lam * C.lam + C.lam + 1) % C.r == 0
         G = (C.gx, C.gy)
@@ -107,7 +107,7 @@ def test_signed_digits_roundtrip(c):
         assert all(-(1 << (c - 1)) <= d <= (1 << (c - 1)) for d in ds)
 
 
-@pytest.mark.parametrize("curve", ["bn254", "bls12_381"])
+@pytest.mark.parametrize("curve", ["bn254", "bls12_381", "bls12_377"])
 def test_montgomery_fr_conversion(curve, oracles):
     ref, cm = oracles
     C = R.CURVES[curve]

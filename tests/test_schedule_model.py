@@ -223,13 +223,15 @@ CASES = [
     ("bls12_381", [600], "uniform", 16, 16, -1, 0),     # 9 windows for 128-bit halves
     ("bls12_381", [250, 0, 40], "witness", 0, 0, -1, 0),
     ("bls12_381", [300], "uniform", 13, 64, 0, 0),
+    ("bls12_377", [500], "uniform", 0, 0, -1, 0),       # 126-bit GLV halves
+    ("bls12_377", [200, 0, 33], "witness", 9, 16, 0, 0),
 ]
 
 
 @pytest.mark.parametrize("curve,counts,dist,window,chunk,glv,bits", CASES)
 def test_schedule_model(curve, counts, dist, window, chunk, glv, bits):
     C = R.CURVES[curve]
-    cid = zl.BN254 if curve == "bn254" else zl.BLS12_381
+    cid = {"bn254": zl.BN254, "bls12_381": zl.BLS12_381, "bls12_377": zl.BLS12_377}[curve]
     pl = plan(cid, counts, 0, window, chunk, glv, bits)
     rng = random.Random(sum(counts) + window)
     total = sum(counts)

@@ -12,7 +12,7 @@ import torch
 
 from oracle import pyref as R
 from tests.gpu_helpers import check, gen_inputs, jac_to_affine_bytes, msm_device, oracle_msm, to_host
-from zkmetal_b200 import BLS12381MSM, CommitmentServer, CommitmentTable, MetalMSM, MSMError
+from zkmetal_b200 import BLS12377MSM, BLS12381MSM, CommitmentServer, CommitmentTable, MetalMSM, MSMError
 from zkmetal_b200 import lib as zl
 
 pytestmark = pytest.mark.gpu
@@ -22,7 +22,7 @@ pytestmark = pytest.mark.gpu
 def eng():
     if not torch.cuda.is_available():
         pytest.skip("no CUDA device")
-    return {"bn254": MetalMSM(), "bls12_381": BLS12381MSM()}
+    return {"bn254": MetalMSM(), "bls12_381": BLS12381MSM(), "bls12_377": BLS12377MSM()}
 
 
 def table_bytes(table, nbytes):
@@ -72,7 +72,7 @@ def test_shift_copies_are_window_shifts(eng, oracles, curve, spacing):
 
 
 @pytest.mark.parametrize("curve,spacing,T", [("bn254", 4, 1 << 13), ("bn254", 6, 1 << 12),
-                                             ("bls12_381", 4, 1 << 12)])
+                                             ("bls12_381", 4, 1 << 12), ("bls12_377", 5, 1 << 12)])
 @pytest.mark.parametrize("dist,fmt", [("uniform", zl.SCALAR_MONT), ("witness", zl.SCALAR_INT)])
 def test_shift_batch_matches_plain(eng, curve, spacing, T, dist, fmt):
     e = eng[curve]
@@ -97,7 +97,7 @@ def test_shift_batch_matches_plain(eng, curve, spacing, T, dist, fmt):
         t.close()
 
 
-@pytest.mark.parametrize("curve", ["bn254", "bls12_381"])
+@pytest.mark.parametrize("curve", ["bn254", "bls12_381", "bls12_377"])
 def test_shift_batch_matches_oracle(eng, oracles, curve):
     ref, cm = oracles
     orc = ref if ref is not None else cm

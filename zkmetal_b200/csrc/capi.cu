@@ -19,7 +19,23 @@ namespace zkmsm {
 static thread_local std::string g_last_error;
 void set_error(const std::string& s) { g_last_error = s; }
 
-static int fp_bytes(int curve) { return curve == ZKMSM_BLS12_381 ? 48 : 32; }
+static int fp_bytes(int curve) { return curve == ZKMSM_BN254 ? 32 : 48; }
+
+static bool curve_ok(int curve) {
+    return curve == ZKMSM_BN254 || curve == ZKMSM_BLS12_381 || curve == ZKMSM_BLS12_377;
+}
+
+// Calls f(C{}) with the curve configuration of a curve id (checked by
+// curve_ok before).
+template <class F>
+static void with_curve(int curve, F&& f) {
+    switch (curve) {
+        case ZKMSM_BN254: f(Bn254{}); break;
+        case ZKMSM_BLS12_381: f(Bls381{}); break;
+        case ZKMSM_BLS12_377: f(Bls377{}); break;
+        default: throw std::invalid_argument("unknown curve id");
+    }
+}
 
 // A window setting: 0 (automatic), a width 2..24, or a two-width layout
 // c | nlo << 16 (nlo >= 1 windows of c = 2..22 bits, then c + 1-bit windows).
@@ -442,6 +458,29 @@ ZkMetalStatus zkmetal_bls12_381_g1_msm_batch(ZkMetalMSMEngine engine, const uint
     });
 }
 
+ZkMetalStatus zkmetal_bls12_377_g1_msm(ZkMetalMSMEngine engine, const uint8_t* points, const uint8_t* scalars,
+                                       uint32_t n, uint8_t* rx, uint8_t* ry, uint8_t* rz) {
+    if (!engine) return ZKMETAL_ERR_INVALID_INPUT;
+    return guarded([&] { return msm_host<Bls377>(ENG(engine), points, scalars, n, ZKMSM_SCALAR_INT, 0, rx, ry, rz); });
+}
+
+ZkMetalStatus zkmetal_bls12_377_g1_msm_fr(ZkMetalMSMEngine engine, const uint8_t* points, const uint8_t* scalars,
+                                          uint32_t n, uint8_t* rx, uint8_t* ry, uint8_t* rz) {
+    if (!engine) return ZKMETAL_ERR_INVALID_INPUT;
+    return guarded(
+        [&] { return msm_host<Bls377>(ENG(engine), points, scalars, n, ZKMSM_SCALAR_MONT, 0, rx, ry, rz); });
+}
+
+ZkMetalStatus zkmetal_bls12_377_g1_msm_batch(ZkMetalMSMEngine engine, const uint8_t* all_points,
+                                             const uint8_t* all_scalars, const uint32_t* counts, uint32_t n_msms,
+                                             uint8_t* results) {
+    if (!engine) return ZKMETAL_ERR_INVALID_INPUT;
+    return guarded([&] {
+        return msm_batch_host<Bls377>(ENG(engine), all_points, all_scalars, counts, n_msms, ZKMSM_SCALAR_INT,
+                                      results);
+    });
+}
+
 void zkmetal_set_shader_dir(const char*) {}
 
 int32_t zkmetal_gpu_available(void) { return have_gpu() ? 1 : 0; }
@@ -453,7 +492,7 @@ const char* zkmsm_last_error(void) { return g_last_error.c_str(); }
 ZkMetalStatus zkmsm_msm_device(ZkMetalMSMEngine engine, int curve, const void* d_points, const void* d_scalars,
                                int fmt, uint32_t n, uint8_t* result, void* stream) {
     if (!engine || !d_points || !d_scalars || !result || n == 0) return ZKMETAL_ERR_INVALID_INPUT;
-    if (curve != ZKMSM_BN254 && curve != ZKMSM_BLS12_381) return ZKMETAL_ERR_INVALID_INPUT;
+    if (!curve_ok(curve)) return ZKMETAL_ERR_INVALID_INPUT;
     if (fmt != ZKMSM_SCALAR_INT && fmt != ZKMSM_SCALAR_MONT) return ZKMETAL_ERR_INVALID_INPUT;
     return guarded([&] {
         Engine& e = ENG(engine);
@@ -466,17 +505,13 @@ ZkMetalStatus zkmsm_msm_device(ZkMetalMSMEngine engine, int curve, const void* d
         } restore{e, saved};
         const uint32_t* pts = static_cast<const uint32_t*>(d_points);
         const uint32_t* sc = static_cast<const uint32_t*>(d_scalars);
-        if (curve == ZKMSM_BN254) {
-            Plan& pl = e.get_plan<Bn254>({n}, {0}, fmt);
-            e.w_phi.ensure((size_t)n * 64 + 16);
-            e.make_phi<Bn254>(pts, n, e.w_phi.as<uint32_t>());
-            e.run_device<Bn254>(pl, pts, e.w_phi.as<uint32_t>(), sc, result);
-        } else {
-            Plan& pl = e.get_plan<Bls381>({n}, {0}, fmt);
-            e.w_phi.ensure((size_t)n * 96 + 16);
-            e.make_phi<Bls381>(pts, n, e.w_phi.as<uint32_t>());
-            e.run_device<Bls381>(pl, pts, e.w_phi.as<uint32_t>(), sc, result);
-        }
+        with_curve(curve, [&](auto cv) {
+            using C = decltype(cv);
+            Plan& pl = e.get_plan<C>({n}, {0}, fmt);
+            e.w_phi.ensure((size_t)n * 2 * fp_bytes(curve) + 16);
+            e.make_phi<C>(pts, n, e.w_phi.as<uint32_t>());
+            e.run_device<C>(pl, pts, e.w_phi.as<uint32_t>(), sc, result);
+        });
         return ZKMETAL_SUCCESS;
     });
 }
@@ -484,7 +519,7 @@ ZkMetalStatus zkmsm_msm_device(ZkMetalMSMEngine engine, int curve, const void* d
 ZkMetalStatus zkmsm_msm_device_async(ZkMetalMSMEngine engine, int curve, const void* d_points, const void* d_phi,
                                      const void* d_scalars, int fmt, uint32_t n, void* d_result, void* stream) {
     if (!engine || !d_points || !d_scalars || !d_result || n == 0 || n >= (1u << 30)) return ZKMETAL_ERR_INVALID_INPUT;
-    if (curve != ZKMSM_BN254 && curve != ZKMSM_BLS12_381) return ZKMETAL_ERR_INVALID_INPUT;
+    if (!curve_ok(curve)) return ZKMETAL_ERR_INVALID_INPUT;
     if (fmt != ZKMSM_SCALAR_INT && fmt != ZKMSM_SCALAR_MONT) return ZKMETAL_ERR_INVALID_INPUT;
     return guarded([&] {
         Engine& e = ENG(engine);
@@ -499,25 +534,17 @@ ZkMetalStatus zkmsm_msm_device_async(ZkMetalMSMEngine engine, int curve, const v
         const uint32_t* phi = static_cast<const uint32_t*>(d_phi);
         const uint32_t* sc = static_cast<const uint32_t*>(d_scalars);
         uint32_t* res = static_cast<uint32_t*>(d_result);
-        if (curve == ZKMSM_BN254) {
-            Plan& pl = e.get_plan<Bn254>({n}, {0}, fmt);
-            e.ensure_workspace<Bn254>(pl);
+        with_curve(curve, [&](auto cv) {
+            using C = decltype(cv);
+            Plan& pl = e.get_plan<C>({n}, {0}, fmt);
+            e.ensure_workspace<C>(pl);
             if (!phi) {
-                e.w_phi.ensure((size_t)n * 64 + 16);
-                e.make_phi<Bn254>(pts, n, e.w_phi.as<uint32_t>());
+                e.w_phi.ensure((size_t)n * 2 * fp_bytes(curve) + 16);
+                e.make_phi<C>(pts, n, e.w_phi.as<uint32_t>());
                 phi = e.w_phi.as<uint32_t>();
             }
-            e.enqueue<Bn254>(pl, pts, phi, sc, res);
-        } else {
-            Plan& pl = e.get_plan<Bls381>({n}, {0}, fmt);
-            e.ensure_workspace<Bls381>(pl);
-            if (!phi) {
-                e.w_phi.ensure((size_t)n * 96 + 16);
-                e.make_phi<Bls381>(pts, n, e.w_phi.as<uint32_t>());
-                phi = e.w_phi.as<uint32_t>();
-            }
-            e.enqueue<Bls381>(pl, pts, phi, sc, res);
-        }
+            e.enqueue<C>(pl, pts, phi, sc, res);
+        });
         return ZKMETAL_SUCCESS;
     });
 }
@@ -525,7 +552,7 @@ ZkMetalStatus zkmsm_msm_device_async(ZkMetalMSMEngine engine, int curve, const v
 ZkMetalStatus zkmsm_table_create(ZkMetalMSMEngine engine, int curve, const void* points, uint64_t n,
                                  int on_device, ZkMsmTable* out) {
     if (!engine || !points || !out || n == 0 || n >= (1ull << 30)) return ZKMETAL_ERR_INVALID_INPUT;
-    if (curve != ZKMSM_BN254 && curve != ZKMSM_BLS12_381) return ZKMETAL_ERR_INVALID_INPUT;
+    if (!curve_ok(curve)) return ZKMETAL_ERR_INVALID_INPUT;
     return guarded([&] {
         Engine& e = ENG(engine);
         std::unique_ptr<Table> t(new Table{&e, curve, n, {}, {}});
@@ -534,8 +561,9 @@ ZkMetalStatus zkmsm_table_create(ZkMetalMSMEngine engine, int curve, const void*
         t->phi.ensure(bytes);
         ZK_CUDA(cudaMemcpyAsync(t->points.p, points, bytes, on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
                                 e.stream));
-        if (curve == ZKMSM_BN254) e.make_phi<Bn254>(t->points.as<uint32_t>(), n, t->phi.as<uint32_t>());
-        else e.make_phi<Bls381>(t->points.as<uint32_t>(), n, t->phi.as<uint32_t>());
+        with_curve(curve, [&](auto cv) {
+            e.make_phi<decltype(cv)>(t->points.as<uint32_t>(), n, t->phi.as<uint32_t>());
+        });
         ZK_CUDA(cudaStreamSynchronize(e.stream));
         *out = t.release();
         return ZKMETAL_SUCCESS;
@@ -546,7 +574,8 @@ ZkMetalStatus zkmsm_table_precompute(ZkMsmTable table, int spacing_bits) {
     if (!table || spacing_bits < 0 || spacing_bits == 1 || spacing_bits > 24) return ZKMETAL_ERR_INVALID_INPUT;
     Table& t = *static_cast<Table*>(table);
     const uint32_t s = (uint32_t)spacing_bits;
-    const uint32_t fr_bits = t.curve == ZKMSM_BN254 ? CurveTraits<Bn254>::fr_bits : CurveTraits<Bls381>::fr_bits;
+    uint32_t fr_bits = 0;
+    with_curve(t.curve, [&](auto cv) { fr_bits = CurveTraits<decltype(cv)>::fr_bits; });
     // a window's top digit may carry into bit fr_bits, so copies cover fr_bits + 1 bits
     const uint32_t copies = s ? (fr_bits + 1 + s - 1) / s : 1;
     if ((uint64_t)copies * t.n > VAL_IDX_MASK) {
@@ -560,8 +589,7 @@ ZkMetalStatus zkmsm_table_precompute(ZkMsmTable table, int spacing_bits) {
         DevBuf nb;
         nb.ensure((size_t)copies * t.n * ab);
         ZK_CUDA(cudaMemcpyAsync(nb.p, t.points.p, (size_t)t.n * ab, cudaMemcpyDeviceToDevice, e.stream));
-        if (t.curve == ZKMSM_BN254) e.make_shifts<Bn254>(nb.as<uint32_t>(), t.n, s, copies);
-        else e.make_shifts<Bls381>(nb.as<uint32_t>(), t.n, s, copies);
+        with_curve(t.curve, [&](auto cv) { e.make_shifts<decltype(cv)>(nb.as<uint32_t>(), t.n, s, copies); });
         ZK_CUDA(cudaStreamSynchronize(e.stream));
         e.drop_graphs();  // graphs captured over the old table address
         std::swap(t.points.p, nb.p);
@@ -600,13 +628,11 @@ ZkMetalStatus zkmsm_batch_commit(ZkMetalMSMEngine engine, ZkMsmTable table, cons
         }
         int fb = fp_bytes(t.curve);
         std::vector<uint8_t> out((size_t)n_msms * 3 * fb);
-        if (t.curve == ZKMSM_BN254) {
-            Plan& pl = e.get_plan<Bn254>(cnt, boff, fmt, 0, 0, t.shifts());
-            e.run_device_graph<Bn254>(pl, t.points.as<uint32_t>(), t.phi.as<uint32_t>(), sc, out.data());
-        } else {
-            Plan& pl = e.get_plan<Bls381>(cnt, boff, fmt, 0, 0, t.shifts());
-            e.run_device_graph<Bls381>(pl, t.points.as<uint32_t>(), t.phi.as<uint32_t>(), sc, out.data());
-        }
+        with_curve(t.curve, [&](auto cv) {
+            using C = decltype(cv);
+            Plan& pl = e.get_plan<C>(cnt, boff, fmt, 0, 0, t.shifts());
+            e.run_device_graph<C>(pl, t.points.as<uint32_t>(), t.phi.as<uint32_t>(), sc, out.data());
+        });
         for (uint32_t m = 0; m < n_msms; m++) {
             uint8_t* dst = results + (size_t)m * 3 * fb;
             if (counts[m] == 0) memset(dst, 0, 3 * fb);
@@ -619,10 +645,10 @@ ZkMetalStatus zkmsm_batch_commit(ZkMetalMSMEngine engine, ZkMsmTable table, cons
 ZkMetalStatus zkmsm_autotune(ZkMetalMSMEngine engine, int curve, int min_log2n, int max_log2n, char* report,
                              uint64_t report_len) {
     if (!engine || min_log2n < 4 || max_log2n > 26 || min_log2n > max_log2n) return ZKMETAL_ERR_INVALID_INPUT;
-    if (curve != ZKMSM_BN254 && curve != ZKMSM_BLS12_381) return ZKMETAL_ERR_INVALID_INPUT;
+    if (!curve_ok(curve)) return ZKMETAL_ERR_INVALID_INPUT;
     return guarded([&] {
-        std::string r = curve == ZKMSM_BN254 ? autotune<Bn254>(ENG(engine), min_log2n, max_log2n)
-                                             : autotune<Bls381>(ENG(engine), min_log2n, max_log2n);
+        std::string r;
+        with_curve(curve, [&](auto cv) { r = autotune<decltype(cv)>(ENG(engine), min_log2n, max_log2n); });
         if (report && report_len) {
             size_t k = std::min<size_t>(r.size(), report_len - 1);
             memcpy(report, r.data(), k);
@@ -663,7 +689,7 @@ ZkMetalStatus zkmsm_tuning_load(ZkMetalMSMEngine engine, const char* path) {
     Engine& e = ENG(engine);
     int k, l2, c;
     while (fscanf(f, "%d %d %d", &k, &l2, &c) == 3)
-        if (k >= 0 && k < 4 && l2 >= 0 && l2 < 40 && (c == 0 || (c >= 2 && c <= 24)))
+        if (k >= 0 && k < 6 && l2 >= 0 && l2 < 40 && (c == 0 || (c >= 2 && c <= 24)))
             e.tuning.window_table[{k, l2}] = c;  // 0: the planner's own layout
     fclose(f);
     e.tuning.version++;
@@ -688,24 +714,23 @@ ZkMetalStatus zkmsm_engine_set_stripe(ZkMetalMSMEngine engine, int stripe_log2) 
 
 ZkMetalStatus zkmsm_gen_bases(ZkMetalMSMEngine engine, int curve, uint64_t seed, uint64_t index0, uint64_t n,
                               void* d_out) {
-    if (!engine || !d_out) return ZKMETAL_ERR_INVALID_INPUT;
+    if (!engine || !d_out || !curve_ok(curve)) return ZKMETAL_ERR_INVALID_INPUT;
     return guarded([&] {
-        if (curve == ZKMSM_BN254) ENG(engine).gen_bases<Bn254>(seed, index0, n, static_cast<uint32_t*>(d_out));
-        else if (curve == ZKMSM_BLS12_381) ENG(engine).gen_bases<Bls381>(seed, index0, n, static_cast<uint32_t*>(d_out));
-        else return ZKMETAL_ERR_INVALID_INPUT;
+        with_curve(curve, [&](auto cv) {
+            ENG(engine).gen_bases<decltype(cv)>(seed, index0, n, static_cast<uint32_t*>(d_out));
+        });
         return ZKMETAL_SUCCESS;
     });
 }
 
 ZkMetalStatus zkmsm_gen_scalars(ZkMetalMSMEngine engine, int curve, uint64_t seed, uint64_t index0, uint64_t n,
                                 int dist, int fmt, void* d_out) {
-    if (!engine || !d_out || (dist != 0 && dist != 1) || (fmt != 0 && fmt != 1)) return ZKMETAL_ERR_INVALID_INPUT;
+    if (!engine || !d_out || !curve_ok(curve) || (dist != 0 && dist != 1) || (fmt != 0 && fmt != 1))
+        return ZKMETAL_ERR_INVALID_INPUT;
     return guarded([&] {
-        if (curve == ZKMSM_BN254)
-            ENG(engine).gen_scalars<Bn254>(seed, index0, n, dist, fmt, static_cast<uint32_t*>(d_out));
-        else if (curve == ZKMSM_BLS12_381)
-            ENG(engine).gen_scalars<Bls381>(seed, index0, n, dist, fmt, static_cast<uint32_t*>(d_out));
-        else return ZKMETAL_ERR_INVALID_INPUT;
+        with_curve(curve, [&](auto cv) {
+            ENG(engine).gen_scalars<decltype(cv)>(seed, index0, n, dist, fmt, static_cast<uint32_t*>(d_out));
+        });
         return ZKMETAL_SUCCESS;
     });
 }
@@ -741,8 +766,9 @@ static ZkMetalStatus plan_json(int curve, const uint32_t* counts, uint32_t n_msm
         t.glv = glv;
         std::vector<uint32_t> cnt(counts, counts + n_msms), boff(n_msms, 0);
         Plan pl;
-        if (curve == ZKMSM_BN254) Engine::plan_shape<Bn254>(pl, t, cnt, boff, fmt, scalar_bits, 0, sh);
-        else Engine::plan_shape<Bls381>(pl, t, cnt, boff, fmt, scalar_bits, 0, sh);
+        with_curve(curve, [&](auto cv) {
+            Engine::plan_shape<decltype(cv)>(pl, t, cnt, boff, fmt, scalar_bits, 0, sh);
+        });
         std::string s = "{\"descs\":[";
         for (size_t i = 0; i < pl.descs.size(); i++) {
             auto& d = pl.descs[i];

@@ -81,6 +81,10 @@ struct DevBuf {
     ~DevBuf() { release(); }
 };
 
+// Curves with an engine instantiation (CurveTraits<C>::id = 0 .. NCURVES - 1);
+// every per-curve array of the engine has this many entries.
+constexpr int NCURVES = 3;
+
 struct Tuning {
     // 0: autotuned table if present, else cost model; 2..24: equal windows of
     // that width; c | nlo << 16: nlo windows of c bits, the rest c + 1 bits
@@ -93,7 +97,7 @@ struct Tuning {
     uint64_t version = 0;  // bumped whenever the table changes
     // threads of the level-1 accumulation kernel resident at once on the
     // device, per curve (0: unknown; then chunks are not wave-aligned)
-    uint32_t acc_wave[2] = {0, 0};
+    uint32_t acc_wave[NCURVES] = {};
 };
 
 // Host description of one batch run.
@@ -253,6 +257,12 @@ struct CurveTraits<Bls381> {
     static constexpr uint32_t half_bits = Bls381Glv::HALF_BITS;
     static constexpr uint32_t fr_bits = Bls381Fr::BITS;
 };
+template <>
+struct CurveTraits<Bls377> {
+    static constexpr int id = 2;
+    static constexpr uint32_t half_bits = Bls377Glv::HALF_BITS;
+    static constexpr uint32_t fr_bits = Bls377Fr::BITS;
+};
 
 class Engine {
    public:
@@ -303,7 +313,7 @@ class Engine {
     DevBuf w_ents2, w_thist, w_stripe_buckets;
     DevBuf w_cnt, w_pos, w_tiles, w_totals, w_pkeys[2], w_pvals[2], w_redS[2], w_redW[2];
     DevBuf w_results, w_comb;
-    bool comb_ready[2] = {false, false};
+    bool comb_ready[NCURVES] = {};
     uint32_t* h_results = nullptr;  // pinned
     size_t h_results_cap = 0;
 
@@ -331,6 +341,7 @@ class Engine {
         bind_workspace_stream();
         tuning.acc_wave[0] = acc_resident_threads<Bn254>();
         tuning.acc_wave[1] = acc_resident_threads<Bls381>();
+        tuning.acc_wave[2] = acc_resident_threads<Bls377>();
     }
     // Second stream and events for host-to-device copies that overlap the
     // compute stream (striped MSMs from host buffers).
@@ -666,7 +677,7 @@ class Engine {
     }
 
     // Curve-specific device work: defined in engine_impl.cuh and instantiated
-    // once per curve (inst_bn254.cu, inst_bls381.cu).
+    // once per curve (inst_bn254.cu, inst_bls381.cu, inst_bls377.cu).
     // flags: ENQ_ACC_ONLY stops after the bucket sums (no window sums, no
     // result).  bucket_base (default: the engine's bucket array) receives the
     // bucket sums.
@@ -756,7 +767,7 @@ class Engine {
 };
 
 // Curve-specific device code is instantiated in its own translation unit
-// (inst_bn254.cu, inst_bls381.cu) so the two curves compile in parallel.
+// (inst_bn254.cu, inst_bls381.cu, inst_bls377.cu) so the curves compile in parallel.
 #define ZKMSM_ENGINE_TEMPLATES(EXT, C)                                                                  \
     EXT template void Engine::enqueue<C>(const Plan&, const uint32_t*, const uint32_t*, const uint32_t*, \
                                          uint32_t*, int, void*);                                        \

@@ -207,9 +207,11 @@ uint32_t Engine::acc_resident_threads() {
 template <class C>
 void Engine::gen_bases(uint64_t seed, uint64_t index0, uint64_t n, uint32_t* d_out) {
     using P = typename C::Fp;
-    int ci = CurveTraits<C>::id;
+    const int ci = CurveTraits<C>::id;
+    static_assert(CurveTraits<C>::id < NCURVES, "per-curve arrays hold NCURVES entries");
     if (!comb_ready[ci]) {
-        w_comb.ensure(2 * 32 * 256 * 2 * 12 * 4);
+        // one 32 x 256-entry table of 12-limb affine points per curve
+        w_comb.ensure((size_t)NCURVES * 32 * 256 * 2 * 12 * 4);
         uint32_t* tab = w_comb.as<uint32_t>() + ci * 32 * 256 * 2 * 12;
         k_comb_table<C><<<(32 * 256 + 127) / 128, 128, 0, stream>>>(tab);
         launches++;

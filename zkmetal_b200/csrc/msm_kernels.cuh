@@ -56,12 +56,13 @@ ZK_DEV void prepare_scalar(Halves& h, const uint32_t* __restrict__ s8, uint32_t 
         fe_from_mont(s, s);  // s * R^-1 mod r  (bn254_msm.c:1537-1552)
     } else {
         // integer form may exceed r: subtract r until below (MSMEngine.swift:182-200);
-        // 2^256 < 6r for both curves, so five passes always suffice
+        // REDUCE_PASSES = floor((2^256 - 1) / r) passes always suffice (5 for
+        // BN254, 2 for BLS12-381, 13 for BLS12-377)
         Fe<Fr> r;
 #pragma unroll
         for (int i = 0; i < 8; i++) r.v[i] = Fr::P(i);
 #pragma unroll 1
-        for (int it = 0; it < 6 && fe_geq_int(s, r); it++) fe_sub_int(s, s, r);
+        for (int it = 0; it < Fr::REDUCE_PASSES && fe_geq_int(s, r); it++) fe_sub_int(s, s, r);
     }
     if (!glv) {
 #pragma unroll
@@ -721,6 +722,10 @@ struct AccLaunch {
 };
 template <>
 struct AccLaunch<Bls381> {
+    static constexpr int THREADS = 256, MIN_BLOCKS = 2;
+};
+template <>
+struct AccLaunch<Bls377> {  // the same 12-limb arithmetic as BLS12-381
     static constexpr int THREADS = 256, MIN_BLOCKS = 2;
 };
 template <class C>

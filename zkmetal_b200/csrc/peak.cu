@@ -219,6 +219,7 @@ extern "C" ZkMetalStatus zkmsm_sum_results_device(int curve, const void* d_resul
     uint32_t* out = static_cast<uint32_t*>(d_out);
     if (curve == ZKMSM_BN254) k_sum_results<Bn254><<<1, 32, 0, s>>>(in, count, out);
     else if (curve == ZKMSM_BLS12_381) k_sum_results<Bls381><<<1, 32, 0, s>>>(in, count, out);
+    else if (curve == ZKMSM_BLS12_377) k_sum_results<Bls377><<<1, 32, 0, s>>>(in, count, out);
     else return ZKMETAL_ERR_INVALID_INPUT;
     return cudaGetLastError() == cudaSuccess ? ZKMETAL_SUCCESS : ZKMETAL_ERR_GPU_ERROR;
 }
@@ -233,6 +234,7 @@ extern "C" ZkMetalStatus zkmsm_field_op(int curve, int op, const void* d_a, cons
     const unsigned g = (n + 127) / 128;
     if (curve == ZKMSM_BN254) k_field_op<Bn254Fp><<<g, 128>>>(op, a, b, o, n);
     else if (curve == ZKMSM_BLS12_381) k_field_op<Bls381Fp><<<g, 128>>>(op, a, b, o, n);
+    else if (curve == ZKMSM_BLS12_377) k_field_op<Bls377Fp><<<g, 128>>>(op, a, b, o, n);
     else return ZKMETAL_ERR_INVALID_INPUT;
     if (cudaGetLastError() != cudaSuccess || cudaDeviceSynchronize() != cudaSuccess) return ZKMETAL_ERR_GPU_ERROR;
     return ZKMETAL_SUCCESS;
@@ -240,7 +242,7 @@ extern "C" ZkMetalStatus zkmsm_field_op(int curve, int op, const void* d_a, cons
 
 extern "C" ZkMetalStatus zkmsm_sum_results(int curve, const uint8_t* results, uint32_t count, uint8_t* out) {
     if (!results || !out || count == 0) return ZKMETAL_ERR_INVALID_INPUT;
-    if (curve != ZKMSM_BN254 && curve != ZKMSM_BLS12_381) return ZKMETAL_ERR_INVALID_INPUT;
+    if (curve != ZKMSM_BN254 && curve != ZKMSM_BLS12_381 && curve != ZKMSM_BLS12_377) return ZKMETAL_ERR_INVALID_INPUT;
     size_t fb = curve == ZKMSM_BN254 ? 32 : 48;
     size_t in_bytes = (size_t)count * 3 * fb;
     uint32_t *d_in = nullptr, *d_out = nullptr;
@@ -251,7 +253,8 @@ extern "C" ZkMetalStatus zkmsm_sum_results(int curve, const uint8_t* results, ui
     }
     cudaMemcpy(d_in, results, in_bytes, cudaMemcpyHostToDevice);
     if (curve == ZKMSM_BN254) k_sum_results<Bn254><<<1, 32>>>(d_in, count, d_out);
-    else k_sum_results<Bls381><<<1, 32>>>(d_in, count, d_out);
+    else if (curve == ZKMSM_BLS12_381) k_sum_results<Bls381><<<1, 32>>>(d_in, count, d_out);
+    else k_sum_results<Bls377><<<1, 32>>>(d_in, count, d_out);
     cudaError_t e = cudaMemcpy(out, d_out, 3 * fb, cudaMemcpyDeviceToHost);
     cudaFree(d_in);
     cudaFree(d_out);

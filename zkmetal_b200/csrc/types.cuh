@@ -13,6 +13,7 @@ struct CurveCfg {
 };
 using Bn254 = CurveCfg<Bn254Fp, Bn254Fr, Bn254Glv, Bn254Gen>;
 using Bls381 = CurveCfg<Bls381Fp, Bls381Fr, Bls381Glv, Bls381Gen>;
+using Bls377 = CurveCfg<Bls377Fp, Bls377Fr, Bls377Glv, Bls377Gen>;
 
 // One MSM of a batch, as the kernels see it.
 struct MsmDesc {

@@ -31,10 +31,17 @@ G_BL = (int("17f1d3a73197d7942695638c4fa9ac0fc3688c4f9774b905a14e3a3f171bac58"
         int("08b3f481e3aaa0f1a09e30ed741d8ae4fcf5e095d5d00af600db18cb2c04b3ed"
             "d03cc744a2888ae40caa232946c5e7e1", 16))
 
+P_377 = int("01ae3a4617c510eac63b05c06ca1493b1a22d9f300f5138f1ef3622fba094800"
+            "170b5d44300000008508c00000000001", 16)
+R_377 = 0x12ab655e9a2ca55660b44d1e5c37b00159aa76fed00000010a11800000000001
+G_377 = (81937999373150964239938255573465948239988671502647976594219695644855304257327692006745978603320413799295628339695,
+         241266749859715473739788878240585681733927191168601896383759122102112907357779751001206799952863815012735208165030)
+
 CURVES = [
     # name, p, r, b, generator, Fp limbs (32-bit)
     ("Bn254", P_BN, R_BN, 3, (1, 2), 8),
     ("Bls381", P_BL, R_BL, 4, G_BL, 12),
+    ("Bls377", P_377, R_377, 1, G_377, 12),
 ]
 
 
@@ -151,6 +158,8 @@ def emit():
                    % ((-pow(r, -1, 1 << 32)) % (1 << 32)))
         out.append(fn_table("P", limbs(r, 8)))
         out.append(fn_table("R2", limbs(Rr * Rr % r, 8)))
+        out.append("    // subtractions of r that bring any 256-bit integer below r\n")
+        out.append("    static constexpr int REDUCE_PASSES = %d;\n" % (((1 << 256) - 1) // r))
         out.append("};\n\n")
         out.append("struct %sGlv {\n" % name)
         out.append("    // phi(x, y) = (BETA * x, y) = LAMBDA * (x, y) on G1\n")

@@ -24,10 +24,11 @@ ERR_BUSY = -5
 
 BN254 = 0
 BLS12_381 = 1
+BLS12_377 = 2
 SCALAR_INT = 0
 SCALAR_MONT = 1
 
-FP_BYTES = {BN254: 32, BLS12_381: 48}
+FP_BYTES = {BN254: 32, BLS12_381: 48, BLS12_377: 48}
 
 c_u8p = ctypes.c_void_p
 c_vp = ctypes.c_void_p
@@ -61,6 +62,9 @@ _SIGS = {
     "zkmetal_bls12_381_g1_msm": (c_i32, [c_vp, c_u8p, c_u8p, c_u32, c_u8p, c_u8p, c_u8p]),
     "zkmetal_bls12_381_g1_msm_fr": (c_i32, [c_vp, c_u8p, c_u8p, c_u32, c_u8p, c_u8p, c_u8p]),
     "zkmetal_bls12_381_g1_msm_batch": (c_i32, [c_vp, c_u8p, c_u8p, c_vp, c_u32, c_u8p]),
+    "zkmetal_bls12_377_g1_msm": (c_i32, [c_vp, c_u8p, c_u8p, c_u32, c_u8p, c_u8p, c_u8p]),
+    "zkmetal_bls12_377_g1_msm_fr": (c_i32, [c_vp, c_u8p, c_u8p, c_u32, c_u8p, c_u8p, c_u8p]),
+    "zkmetal_bls12_377_g1_msm_batch": (c_i32, [c_vp, c_u8p, c_u8p, c_vp, c_u32, c_u8p]),
     "zkmetal_set_shader_dir": (None, [ctypes.c_char_p]),
     "zkmetal_gpu_available": (c_i32, []),
     "zkmetal_version": (ctypes.c_char_p, []),

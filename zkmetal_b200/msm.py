@@ -163,6 +163,20 @@ class BLS12381MSM(_Engine):
         return self._call(_l.lib().zkmetal_bls12_381_g1_msm_fr, p, s, n)
 
 
+class BLS12377MSM(_Engine):
+    """BLS12-377 G1 MSM engine (BLS12377MSMEngine.swift:7; msm at :266)."""
+
+    curve = _l.BLS12_377
+
+    def msm(self, points, scalars):
+        p, s, n = self._prep(points, scalars)
+        return self._call(_l.lib().zkmetal_bls12_377_g1_msm, p, s, n)
+
+    def msmFr(self, points, scalars_mont):
+        p, s, n = self._prep(points, scalars_mont)
+        return self._call(_l.lib().zkmetal_bls12_377_g1_msm_fr, p, s, n)
+
+
 def multiMSM(engine, points, scalar_sets):
     """k MSMs over the same bases (MultiMSM.swift:21-72), run as one batch.
 
