@@ -541,6 +541,44 @@ def run_bls_config(seed=0x5EED0003, log2n=22, n_batch=8, lo=14, hi=22):
             "bit_exact_vs_plain": r_bat == r_bat0 == r_dev}
 
 
+def run_bls377_config(seed=0x5EED0005, log2n=22, steps=5):
+    """BLS12-377 G1 (the adjacent curve of the same 12-limb kernels): plain
+    MSMs with device-resident bases and uniform Montgomery scalars at 2^20
+    and 2^22, device ms per MSM (CUDA events on the library's stream)."""
+    import torch
+    from zkmetal_b200 import BLS12377MSM
+    from zkmetal_b200 import lib as zl
+    L = zl.lib()
+    T = 1 << log2n
+    e = BLS12377MSM()
+    pts = _dev(torch, T * 96)
+    sc = _dev(torch, T * 32)
+    torch.cuda.synchronize()
+    assert L.zkmsm_gen_bases(e.handle, zl.BLS12_377, seed, 0, T, pts.data_ptr()) == 0
+    assert L.zkmsm_gen_scalars(e.handle, zl.BLS12_377, seed + 1, 0, T, 0, 1, sc.data_ptr()) == 0
+    stream = torch.cuda.Stream()
+    res = _dev(torch, 144)
+    out = {}
+    for lg in (20, log2n):
+        n = 1 << lg
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(stream):
+            for _ in range(3):
+                assert L.zkmsm_msm_device_async(e.handle, zl.BLS12_377, pts.data_ptr(), None, sc.data_ptr(), 1, n,
+                                                res.data_ptr(), stream.cuda_stream) == 0
+            ev0.record(stream)
+            for _ in range(steps):
+                assert L.zkmsm_msm_device_async(e.handle, zl.BLS12_377, pts.data_ptr(), None, sc.data_ptr(), 1, n,
+                                                res.data_ptr(), stream.cuda_stream) == 0
+            ev1.record(stream)
+        torch.cuda.synchronize()
+        ms = ev0.elapsed_time(ev1) / steps
+        out["plain_2p%d_ms" % lg] = round(ms, 3)
+        out["plain_2p%d_points_per_s" % lg] = round(n / (ms * 1e-3))
+    e.close()
+    return out
+
+
 # --------------------------------------------------------------- GPU arm
 def run_ours(args):
     import torch
@@ -742,6 +780,11 @@ def run_ours(args):
             line["bls12_381"] = run_bls_config()
         except Exception as exc:
             line["bls12_381"] = {"error": repr(exc)}
+        release()
+        try:
+            line["bls12_377"] = run_bls377_config()
+        except Exception as exc:
+            line["bls12_377"] = {"error": repr(exc)}
         release()
         try:
             line["serve"] = run_serve_config(duration_s=args.serve_seconds, plain_sample=40)

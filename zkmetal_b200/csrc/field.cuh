@@ -143,7 +143,7 @@ ZK_DEV void fe_mul_body(Fe<P>& r, const Fe<P>& a, const Fe<P>& b) {
                 asm volatile("madc.hi.cc.u32 %0, %1, %2, %0;" : "+r"(t[j + 1]) : "r"(a.v[j]), "r"(bi));
             asm volatile("madc.hi.u32 %0, %1, %2, %0;" : "+r"(t[N]) : "r"(a.v[N - 1]), "r"(bi));
         }
-        const uint32_t m = t[0] * P::N0;
+        const uint32_t m = t[0] * P::N0R();
         asm volatile("mad.lo.cc.u32 %0, %1, %2, %0;" : "+r"(t[0]) : "r"(m), "r"(P::P(0)));
 #pragma unroll
         for (int j = 1; j < N; j++)
@@ -220,7 +220,7 @@ ZK_DEV void fe_mul_body_eo(Fe<P>& r, const Fe<P>& a, const Fe<P>& b) {
                 o[j] = y[j];
             }
         }
-        const uint32_t m = e[0] * P::N0;
+        const uint32_t m = e[0] * P::N0R();
         asm volatile("mad.lo.cc.u32 %0, %1, %2, %0;" : "+r"(e[0]) : "r"(m), "r"(P::P(0)));
         asm volatile("madc.hi.cc.u32 %0, %1, %2, %0;" : "+r"(e[1]) : "r"(m), "r"(P::P(0)));
 #pragma unroll

@@ -141,10 +141,25 @@ def emit():
         n0 = (-pow(p, -1, 1 << 32)) % (1 << 32)
         g = glv(p, r, G)
         Rr = 1 << 256
+        # n0 = -p^-1 mod 2^32 of 0xffffffff (BLS12-377) lets the compiler turn
+        # m = t0 * n0 into a negation and rework the reduction around it:
+        # 25.1 against 29.9 G products/s for the same 12-limb product.  Such an
+        # n0 is read from constant memory (mutable, so never folded).
+        opaque = n0 == 0xFFFFFFFF
+        if opaque:
+            out.append("#ifdef __CUDACC__\n")
+            out.append("static __constant__ uint32_t %sFp_N0_MEM = 0x%08xu;\n" % (name, n0))
+            out.append("#endif\n")
         out.append("struct %sFp {\n" % name)
         out.append("    static constexpr int N = %d;\n" % N)
         out.append("    static constexpr int BITS = %d;\n" % p.bit_length())
         out.append("    static constexpr uint32_t N0 = 0x%08xu;\n" % n0)
+        if opaque:
+            out.append("#ifdef __CUDACC__\n")
+            out.append("    __device__ static uint32_t N0R() { return %sFp_N0_MEM; }\n" % name)
+            out.append("#endif\n")
+        else:
+            out.append("    __host__ __device__ static constexpr uint32_t N0R() { return N0; }\n")
         out.append(fn_table("P", limbs(p, N)))
         out.append(fn_table("ONE", limbs(R % p, N)))
         out.append(fn_table("R2", limbs(R * R % p, N)))
@@ -156,6 +171,7 @@ def emit():
         out.append("    static constexpr int BITS = %d;\n" % r.bit_length())
         out.append("    static constexpr uint32_t N0 = 0x%08xu;\n"
                    % ((-pow(r, -1, 1 << 32)) % (1 << 32)))
+        out.append("    __host__ __device__ static constexpr uint32_t N0R() { return N0; }\n")
         out.append(fn_table("P", limbs(r, 8)))
         out.append(fn_table("R2", limbs(Rr * Rr % r, 8)))
         out.append("    // subtractions of r that bring any 256-bit integer below r\n")
