@@ -579,6 +579,44 @@ def run_bls377_config(seed=0x5EED0005, log2n=22, steps=5):
     return out
 
 
+def run_g2_config(seed=0x5EED0006, log2n=20, steps=3):
+    """BN254 G2 (Fp2 coordinates, no endomorphism split): plain MSMs with
+    device-resident bases and uniform Montgomery scalars at 2^16 and 2^20,
+    device ms per MSM (CUDA events on the library's stream)."""
+    import torch
+    from zkmetal_b200 import BN254G2MSM
+    from zkmetal_b200 import lib as zl
+    L = zl.lib()
+    T = 1 << log2n
+    e = BN254G2MSM()
+    pts = _dev(torch, T * 128)
+    sc = _dev(torch, T * 32)
+    torch.cuda.synchronize()
+    assert L.zkmsm_gen_bases(e.handle, zl.BN254_G2, seed, 0, T, pts.data_ptr()) == 0
+    assert L.zkmsm_gen_scalars(e.handle, zl.BN254_G2, seed + 1, 0, T, 0, 1, sc.data_ptr()) == 0
+    stream = torch.cuda.Stream()
+    res = _dev(torch, 192)
+    out = {}
+    for lg in (16, log2n):
+        n = 1 << lg
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(stream):
+            for _ in range(2):
+                assert L.zkmsm_msm_device_async(e.handle, zl.BN254_G2, pts.data_ptr(), None, sc.data_ptr(), 1, n,
+                                                res.data_ptr(), stream.cuda_stream) == 0
+            ev0.record(stream)
+            for _ in range(steps):
+                assert L.zkmsm_msm_device_async(e.handle, zl.BN254_G2, pts.data_ptr(), None, sc.data_ptr(), 1, n,
+                                                res.data_ptr(), stream.cuda_stream) == 0
+            ev1.record(stream)
+        torch.cuda.synchronize()
+        ms = ev0.elapsed_time(ev1) / steps
+        out["plain_2p%d_ms" % lg] = round(ms, 3)
+        out["plain_2p%d_points_per_s" % lg] = round(n / (ms * 1e-3))
+    e.close()
+    return out
+
+
 # --------------------------------------------------------------- GPU arm
 def run_ours(args):
     import torch
@@ -785,6 +823,11 @@ def run_ours(args):
             line["bls12_377"] = run_bls377_config()
         except Exception as exc:
             line["bls12_377"] = {"error": repr(exc)}
+        release()
+        try:
+            line["bn254_g2"] = run_g2_config()
+        except Exception as exc:
+            line["bn254_g2"] = {"error": repr(exc)}
         release()
         try:
             line["serve"] = run_serve_config(duration_s=args.serve_seconds, plain_sample=40)

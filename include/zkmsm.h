@@ -125,6 +125,18 @@ ZkMetalStatus zkmetal_bls12_377_g1_msm_batch(ZkMetalMSMEngine engine, const uint
                                              const uint8_t* all_scalars, const uint32_t* counts,
                                              uint32_t n_msms, uint8_t* results);
 
+/* ---- BN254 G2 MSM -------------------------------------------------------
+ * NEW symbols.  They replace the Swift API BN254G2MSM.msm
+ * (MSM/BN254G2MSMEngine.swift:51, msm at :289).  Points 128 B (x.c0, x.c1,
+ * y.c0, y.c1, each 32 B Montgomery: G2AffinePoint of
+ * Curve/BN254Pairing.swift:301-305); results x, y, z as 64 B Fp2 elements
+ * (Z = 1 = (1, 0), or the identity (1, 1, 0) with z = 0).  Scalars as in the
+ * BN254 G1 calls; no endomorphism split. */
+ZkMetalStatus zkmetal_bn254_g2_msm(ZkMetalMSMEngine engine, const uint8_t* points, const uint8_t* scalars,
+                                   uint32_t n_points, uint8_t* result_x, uint8_t* result_y, uint8_t* result_z);
+ZkMetalStatus zkmetal_bn254_g2_msm_fr(ZkMetalMSMEngine engine, const uint8_t* points, const uint8_t* scalars_mont,
+                                      uint32_t n_points, uint8_t* result_x, uint8_t* result_y, uint8_t* result_z);
+
 /* ---- misc: zkmetal.h:520-530 --------------------------------------------- */
 /* replaces zkmetal_set_shader_dir (zkmetal.h:524): accepted and ignored (no shaders) */
 void zkmetal_set_shader_dir(const char* path);
@@ -139,6 +151,7 @@ const char* zkmetal_version(void);
 #define ZKMSM_BN254 0
 #define ZKMSM_BLS12_381 1
 #define ZKMSM_BLS12_377 2
+#define ZKMSM_BN254_G2 3
 /* Scalar encoding */
 #define ZKMSM_SCALAR_INT 0
 #define ZKMSM_SCALAR_MONT 1

@@ -492,3 +492,111 @@ BLS12_377 = Curve(
     limbs32=12)
 
 CURVES = {"bn254": BN254, "bls12_381": BLS12_381, "bls12_377": BLS12_377}
+
+
+# ---------------------------------------------------------------------------
+# BN254 G2 (test restatement of BN254G2MSM.msm, MSM/BN254G2MSMEngine.swift:289,
+# and its CPU path g2ScalarMul + g2Add, :543-560): the twist
+# y^2 = x^3 + 3/(9 + u) over Fp2 = Fp[u]/(u^2 + 1).  An Fp2 element is a
+# pair (c0, c1) = c0 + c1*u; an affine point ((x0, x1), (y0, y1)), None for
+# the identity.  Affine arithmetic with Python integers: small n only.
+# Byte layout (Curve/BN254Pairing.swift:13-16, 301-305): x.c0, x.c1, y.c0,
+# y.c1, each 32 B little endian Montgomery (R = 2^256); identity = zeros.
+# ---------------------------------------------------------------------------
+
+
+class G2Curve:
+    name = "bn254_g2"
+
+    def __init__(self):
+        self.p = BN254.p
+        self.r = BN254.r
+        self.fp_bytes = 64          # one Fp2 coordinate
+        self.R = 1 << 256
+        self.b = self.mul((3, 0), self.inv((9, 1)))
+        self.gx = (0x1800deef121f1e76426a00665e5c4479674322d4f75edadd46debd5cd992f6ed,
+                   0x198e9393920d483a7260bfb731fb5d25f1aa493335a9e71297e485b7aef312c2)
+        self.gy = (0x12c85ea5db8c6deb4aab71808dcb408fe3d1e7690c43d37b4ce6cc0166fa7daa,
+                   0x090689d0585ff075ec9e99ad690c3395bc4b313370b38ef355acdadcd122975b)
+        assert self.on_curve((self.gx, self.gy))
+
+    # -- Fp2 ---------------------------------------------------------------
+    def add2(self, a, b):
+        return ((a[0] + b[0]) % self.p, (a[1] + b[1]) % self.p)
+
+    def sub2(self, a, b):
+        return ((a[0] - b[0]) % self.p, (a[1] - b[1]) % self.p)
+
+    def mul(self, a, b):
+        p = self.p
+        return ((a[0] * b[0] - a[1] * b[1]) % p, (a[0] * b[1] + a[1] * b[0]) % p)
+
+    def inv(self, a):
+        t = pow(a[0] * a[0] + a[1] * a[1], -1, self.p)
+        return (a[0] * t % self.p, -a[1] * t % self.p)
+
+    # -- points ------------------------------------------------------------
+    def on_curve(self, P):
+        if P is None:
+            return True
+        x, y = P
+        return self.mul(y, y) == self.add2(self.mul(self.mul(x, x), x), self.b)
+
+    def neg(self, P):
+        return None if P is None else (P[0], ((-P[1][0]) % self.p, (-P[1][1]) % self.p))
+
+    def add(self, A, B):
+        if A is None:
+            return B
+        if B is None:
+            return A
+        if A[0] == B[0]:
+            if self.add2(A[1], B[1]) == (0, 0):
+                return None
+            lam = self.mul(self.mul((3, 0), self.mul(A[0], A[0])), self.inv(self.add2(A[1], A[1])))
+        else:
+            lam = self.mul(self.sub2(B[1], A[1]), self.inv(self.sub2(B[0], A[0])))
+        x3 = self.sub2(self.sub2(self.mul(lam, lam), A[0]), B[0])
+        return (x3, self.sub2(self.mul(lam, self.sub2(A[0], x3)), A[1]))
+
+    def scalar_mul(self, P, k):
+        acc = None
+        for bit in bin(k % self.r)[2:] if k % self.r else "":
+            acc = self.add(acc, acc)
+            if bit == "1":
+                acc = self.add(acc, P)
+        return acc
+
+    def naive_msm(self, points, scalars):
+        acc = None
+        for P, k in zip(points, scalars):
+            acc = self.add(acc, self.scalar_mul(P, k))
+        return acc
+
+    def make_bases(self, seed, n):
+        G = (self.gx, self.gy)
+        return [self.scalar_mul(G, base_scalar(self, seed, i)) for i in range(n)]
+
+    # -- bytes -------------------------------------------------------------
+    def enc_fp2(self, a):
+        return b"".join((c * self.R % self.p).to_bytes(32, "little") for c in a)
+
+    def dec_fp2(self, b):
+        inv_r = pow(self.R, -1, self.p)
+        return tuple(int.from_bytes(b[32 * i:32 * i + 32], "little") * inv_r % self.p for i in range(2))
+
+    def enc_affine(self, P):
+        if P is None:
+            return bytes(128)
+        return self.enc_fp2(P[0]) + self.enc_fp2(P[1])
+
+    def dec_affine(self, b):
+        if not any(b[:128]):
+            return None
+        return (self.dec_fp2(b[:64]), self.dec_fp2(b[64:128]))
+
+    def pack_points(self, pts):
+        return b"".join(self.enc_affine(P) for P in pts)
+
+
+BN254_G2 = G2Curve()

@@ -145,3 +145,17 @@ def test_c_restatement_matches_reference_medium(oracles):
     sc = [rng.randrange(1 << 256) for _ in range(n)]
     pb, sb = R.pack_points(C, pts), R.pack_scalars_int(sc)
     assert cm.msm("bn254", pb, sb, n) == ref.msm("bn254", pb, sb, n)
+
+
+def test_g2_restatement_group_laws():
+    """BN254 G2 restatement: generator on the twist, order r, additivity,
+    encoding round trip."""
+    G2 = R.BN254_G2
+    G = (G2.gx, G2.gy)
+    assert G2.on_curve(G)
+    assert G2.scalar_mul(G, G2.r) is None
+    P = G2.scalar_mul(G, 1234567)
+    assert G2.add(P, G2.neg(P)) is None
+    assert G2.add(G2.scalar_mul(G, 5), G2.scalar_mul(G, 7)) == G2.scalar_mul(G, 12)
+    assert G2.dec_affine(G2.enc_affine(P)) == P
+    assert G2.enc_affine(None) == bytes(128)

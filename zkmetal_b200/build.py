@@ -17,7 +17,7 @@ ROOT = os.path.dirname(HERE)
 LIB = os.path.join(HERE, "libzkmsm.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
-SOURCES = ["capi.cu", "inst_bn254.cu", "inst_bls381.cu", "inst_bls377.cu", "peak.cu", "noalloc.cu", "server.cu"]
+SOURCES = ["capi.cu", "inst_bn254.cu", "inst_bls381.cu", "inst_bls377.cu", "inst_bn254g2.cu", "peak.cu", "noalloc.cu", "server.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

@@ -19,10 +19,11 @@ namespace zkmsm {
 static thread_local std::string g_last_error;
 void set_error(const std::string& s) { g_last_error = s; }
 
-static int fp_bytes(int curve) { return curve == ZKMSM_BN254 ? 32 : 48; }
+// bytes of one coordinate (a BN254 G2 coordinate is an Fp2 element: 64 B)
+static int fp_bytes(int curve) { return curve == ZKMSM_BN254 ? 32 : curve == ZKMSM_BN254_G2 ? 64 : 48; }
 
 static bool curve_ok(int curve) {
-    return curve == ZKMSM_BN254 || curve == ZKMSM_BLS12_381 || curve == ZKMSM_BLS12_377;
+    return curve == ZKMSM_BN254 || curve == ZKMSM_BLS12_381 || curve == ZKMSM_BLS12_377 || curve == ZKMSM_BN254_G2;
 }
 
 // Calls f(C{}) with the curve configuration of a curve id (checked by
@@ -33,6 +34,7 @@ static void with_curve(int curve, F&& f) {
         case ZKMSM_BN254: f(Bn254{}); break;
         case ZKMSM_BLS12_381: f(Bls381{}); break;
         case ZKMSM_BLS12_377: f(Bls377{}); break;
+        case ZKMSM_BN254_G2: f(Bn254G2{}); break;
         default: throw std::invalid_argument("unknown curve id");
     }
 }
@@ -188,7 +190,7 @@ static ZkMetalStatus msm_host(Engine& e, const uint8_t* points, const uint8_t* s
     if (n == 0 || !points || !scalars || !rx || !ry || !rz) return ZKMETAL_ERR_INVALID_INPUT;
     const auto rg = stripe_ranges(e, n);
     if (rg.size() > 1) {
-        uint8_t out[3 * 48];
+        uint8_t out[3 * 4 * MAX_COORD_WORDS];
         msm_host_striped<C>(e, points, scalars, n, fmt, scalar_bits, rg, out);
         memcpy(rx, out, fb);
         memcpy(ry, out + fb, fb);
@@ -203,7 +205,7 @@ static ZkMetalStatus msm_host(Engine& e, const uint8_t* points, const uint8_t* s
         e.w_phi.ensure((size_t)n * 2 * fb + 16);
         e.make_phi<C>(e.w_points.as<uint32_t>(), n, e.w_phi.as<uint32_t>());
     }
-    uint8_t out[3 * 48];
+    uint8_t out[3 * 4 * MAX_COORD_WORDS];
     e.run_device<C>(pl, e.w_points.as<uint32_t>(), glv ? e.w_phi.as<uint32_t>() : e.w_points.as<uint32_t>(),
                     e.w_scalars.as<uint32_t>(), out);
     memcpy(rx, out, fb);
@@ -479,6 +481,19 @@ ZkMetalStatus zkmetal_bls12_377_g1_msm_batch(ZkMetalMSMEngine engine, const uint
         return msm_batch_host<Bls377>(ENG(engine), all_points, all_scalars, counts, n_msms, ZKMSM_SCALAR_INT,
                                       results);
     });
+}
+
+ZkMetalStatus zkmetal_bn254_g2_msm(ZkMetalMSMEngine engine, const uint8_t* points, const uint8_t* scalars,
+                                   uint32_t n, uint8_t* rx, uint8_t* ry, uint8_t* rz) {
+    if (!engine) return ZKMETAL_ERR_INVALID_INPUT;
+    return guarded([&] { return msm_host<Bn254G2>(ENG(engine), points, scalars, n, ZKMSM_SCALAR_INT, 0, rx, ry, rz); });
+}
+
+ZkMetalStatus zkmetal_bn254_g2_msm_fr(ZkMetalMSMEngine engine, const uint8_t* points, const uint8_t* scalars,
+                                      uint32_t n, uint8_t* rx, uint8_t* ry, uint8_t* rz) {
+    if (!engine) return ZKMETAL_ERR_INVALID_INPUT;
+    return guarded(
+        [&] { return msm_host<Bn254G2>(ENG(engine), points, scalars, n, ZKMSM_SCALAR_MONT, 0, rx, ry, rz); });
 }
 
 void zkmetal_set_shader_dir(const char*) {}

@@ -12,6 +12,7 @@
 // no doubling-based special form.
 #pragma once
 #include "field.cuh"
+#include "field2.cuh"
 
 namespace zkmsm {
 

@@ -83,7 +83,9 @@ struct DevBuf {
 
 // Curves with an engine instantiation (CurveTraits<C>::id = 0 .. NCURVES - 1);
 // every per-curve array of the engine has this many entries.
-constexpr int NCURVES = 3;
+constexpr int NCURVES = 4;
+// widest coordinate of any curve, in 32-bit words (BN254 G2: two 8-word Fp)
+constexpr int MAX_COORD_WORDS = 16;
 
 struct Tuning {
     // 0: autotuned table if present, else cost model; 2..24: equal windows of
@@ -247,21 +249,31 @@ template <class C>
 struct CurveTraits;
 template <>
 struct CurveTraits<Bn254> {
+    static constexpr bool glv = true;  // endomorphism split available
     static constexpr int id = 0;
     static constexpr uint32_t half_bits = Bn254Glv::HALF_BITS;
     static constexpr uint32_t fr_bits = Bn254Fr::BITS;
 };
 template <>
 struct CurveTraits<Bls381> {
+    static constexpr bool glv = true;
     static constexpr int id = 1;
     static constexpr uint32_t half_bits = Bls381Glv::HALF_BITS;
     static constexpr uint32_t fr_bits = Bls381Fr::BITS;
 };
 template <>
 struct CurveTraits<Bls377> {
+    static constexpr bool glv = true;
     static constexpr int id = 2;
     static constexpr uint32_t half_bits = Bls377Glv::HALF_BITS;
     static constexpr uint32_t fr_bits = Bls377Fr::BITS;
+};
+template <>
+struct CurveTraits<Bn254G2> {
+    static constexpr bool glv = false;  // plain 254-bit windows
+    static constexpr int id = 3;
+    static constexpr uint32_t half_bits = Bn254Fr::BITS;
+    static constexpr uint32_t fr_bits = Bn254Fr::BITS;
 };
 
 class Engine {
@@ -342,6 +354,7 @@ class Engine {
         tuning.acc_wave[0] = acc_resident_threads<Bn254>();
         tuning.acc_wave[1] = acc_resident_threads<Bls381>();
         tuning.acc_wave[2] = acc_resident_threads<Bls377>();
+        tuning.acc_wave[3] = acc_resident_threads<Bn254G2>();
     }
     // Second stream and events for host-to-device copies that overlap the
     // compute stream (striped MSMs from host buffers).
@@ -414,7 +427,7 @@ class Engine {
                 pl.descs.push_back(d);
                 continue;
             }
-            d.glv = small ? 0 : (tuning.glv == 0 ? 0 : 1);
+            d.glv = (small || !CurveTraits<C>::glv) ? 0 : (tuning.glv == 0 ? 0 : 1);
             uint32_t bits = small ? scalar_bits : (d.glv ? CurveTraits<C>::half_bits : CurveTraits<C>::fr_bits);
             uint64_t epw = (uint64_t)d.n * (d.glv ? 2 : 1);
             // a window setting of 2^16 or more is a layout: c | nlo << 16
@@ -677,7 +690,7 @@ class Engine {
     }
 
     // Curve-specific device work: defined in engine_impl.cuh and instantiated
-    // once per curve (inst_bn254.cu, inst_bls381.cu, inst_bls377.cu).
+    // once per curve (inst_bn254.cu, inst_bls381.cu, inst_bls377.cu, inst_bn254g2.cu).
     // flags: ENQ_ACC_ONLY stops after the bucket sums (no window sums, no
     // result).  bucket_base (default: the engine's bucket array) receives the
     // bucket sums.
@@ -767,7 +780,7 @@ class Engine {
 };
 
 // Curve-specific device code is instantiated in its own translation unit
-// (inst_bn254.cu, inst_bls381.cu, inst_bls377.cu) so the curves compile in parallel.
+// (inst_bn254.cu, inst_bls381.cu, inst_bls377.cu, inst_bn254g2.cu) so the curves compile in parallel.
 #define ZKMSM_ENGINE_TEMPLATES(EXT, C)                                                                  \
     EXT template void Engine::enqueue<C>(const Plan&, const uint32_t*, const uint32_t*, const uint32_t*, \
                                          uint32_t*, int, void*);                                        \

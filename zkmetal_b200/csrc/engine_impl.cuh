@@ -161,7 +161,7 @@ void Engine::fold_buckets(void* base, uint32_t nb, uint32_t S) {
 // endomorphism table for a base array
 template <class C>
 void Engine::make_phi(const uint32_t* d_bases, uint64_t n, uint32_t* d_phi) {
-    if (!n) return;
+    if (!n || !CurveTraits<C>::glv) return;  // no endomorphism image without a GLV split
     k_endo<C><<<(unsigned)((n + 255) / 256), 256, 0, stream>>>(d_bases, (uint32_t)n, d_phi);
     launches++;
     ZK_CUDA(cudaGetLastError());
@@ -210,15 +210,17 @@ void Engine::gen_bases(uint64_t seed, uint64_t index0, uint64_t n, uint32_t* d_o
     const int ci = CurveTraits<C>::id;
     static_assert(CurveTraits<C>::id < NCURVES, "per-curve arrays hold NCURVES entries");
     if (!comb_ready[ci]) {
-        // one 32 x 256-entry table of 12-limb affine points per curve
-        w_comb.ensure((size_t)NCURVES * 32 * 256 * 2 * 12 * 4);
-        uint32_t* tab = w_comb.as<uint32_t>() + ci * 32 * 256 * 2 * 12;
+        // one 32 x 256-entry table of affine points per curve, each slot
+        // sized for the widest coordinate
+        static_assert(P::N <= MAX_COORD_WORDS, "coordinate wider than the comb table slot");
+        w_comb.ensure((size_t)NCURVES * 32 * 256 * 2 * MAX_COORD_WORDS * 4);
+        uint32_t* tab = w_comb.as<uint32_t>() + (size_t)ci * 32 * 256 * 2 * MAX_COORD_WORDS;
         k_comb_table<C><<<(32 * 256 + 127) / 128, 128, 0, stream>>>(tab);
         launches++;
         ZK_CUDA(cudaGetLastError());
         comb_ready[ci] = true;
     }
-    uint32_t* tab = w_comb.as<uint32_t>() + ci * 32 * 256 * 2 * 12;
+    uint32_t* tab = w_comb.as<uint32_t>() + (size_t)ci * 32 * 256 * 2 * MAX_COORD_WORDS;
     (void)sizeof(P);
     if (n) k_gen_bases<C><<<(unsigned)((n + 127) / 128), 128, 0, stream>>>(tab, d_out, n, seed, index0);
     launches += (n) ? 1 : 0;

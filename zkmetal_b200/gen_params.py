@@ -45,6 +45,58 @@ CURVES = [
 ]
 
 
+# BN254 G2: the twist y^2 = x^3 + 3/(9 + u) over Fp2 = Fp[u]/(u^2 + 1), with
+# the generator of EIP-197 (coordinates c0 + c1*u)
+G2_BN = ((0x1800deef121f1e76426a00665e5c4479674322d4f75edadd46debd5cd992f6ed,
+          0x198e9393920d483a7260bfb731fb5d25f1aa493335a9e71297e485b7aef312c2),
+         (0x12c85ea5db8c6deb4aab71808dcb408fe3d1e7690c43d37b4ce6cc0166fa7daa,
+          0x090689d0585ff075ec9e99ad690c3395bc4b313370b38ef355acdadcd122975b))
+
+
+def f2_mul(a, b, p):
+    return ((a[0] * b[0] - a[1] * b[1]) % p, (a[0] * b[1] + a[1] * b[0]) % p)
+
+
+def f2_add(a, b, p):
+    return ((a[0] + b[0]) % p, (a[1] + b[1]) % p)
+
+
+def f2_inv(a, p):
+    t = pow(a[0] * a[0] + a[1] * a[1], -1, p)
+    return (a[0] * t % p, -a[1] * t % p)
+
+
+def g2_check(p, r, G):
+    """G on the twist and of order r (double-and-add in affine Fp2)."""
+    b2 = f2_mul((3, 0), f2_inv((9, 1), p), p)
+    x, y = G
+    assert f2_mul(y, y, p) == f2_add(f2_mul(f2_mul(x, x, p), x, p), b2, p), "G2 generator not on the twist"
+
+    def add(A, B):
+        if A is None:
+            return B
+        if B is None:
+            return A
+        if A[0] == B[0]:
+            if f2_add(A[1], B[1], p) == (0, 0):
+                return None
+            num = f2_mul((3, 0), f2_mul(A[0], A[0], p), p)
+            lam = f2_mul(num, f2_inv(f2_add(A[1], A[1], p), p), p)
+        else:
+            lam = f2_mul(((B[1][0] - A[1][0]) % p, (B[1][1] - A[1][1]) % p),
+                         f2_inv(((B[0][0] - A[0][0]) % p, (B[0][1] - A[0][1]) % p), p), p)
+        l2 = f2_mul(lam, lam, p)
+        x3 = ((l2[0] - A[0][0] - B[0][0]) % p, (l2[1] - A[0][1] - B[0][1]) % p)
+        t = f2_mul(lam, ((A[0][0] - x3[0]) % p, (A[0][1] - x3[1]) % p), p)
+        return (x3, ((t[0] - A[1][0]) % p, (t[1] - A[1][1]) % p))
+    acc = None
+    for bit in bin(r)[2:]:
+        acc = add(acc, acc)
+        if bit == "1":
+            acc = add(acc, G)
+    assert acc is None, "G2 generator order is not r"
+
+
 def limbs(x, n):
     return [(x >> (32 * i)) & 0xFFFFFFFF for i in range(n)]
 
@@ -196,6 +248,15 @@ def emit():
         out.append(fn_table("Y_MONT", limbs(G[1] * R % p, N)))
         out.append("    static constexpr uint32_t B = %du;\n" % b)
         out.append("};\n\n")
+    # BN254 G2 generator (Fp2 coordinates c0 limbs then c1 limbs, Montgomery)
+    g2_check(P_BN, R_BN, G2_BN)
+    R = 1 << 256
+    (x0, x1), (y0, y1) = G2_BN
+    out.append("// BN254 G2 generator on the twist y^2 = x^3 + 3/(9 + u): c0 limbs, then c1 limbs\n")
+    out.append("struct Bn254G2Gen {\n")
+    out.append(fn_table("X_MONT", limbs(x0 * R % P_BN, 8) + limbs(x1 * R % P_BN, 8)))
+    out.append(fn_table("Y_MONT", limbs(y0 * R % P_BN, 8) + limbs(y1 * R % P_BN, 8)))
+    out.append("};\n\n")
     out.append("}  // namespace zkmsm\n")
     return "".join(out)
 

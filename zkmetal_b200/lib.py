@@ -25,10 +25,11 @@ ERR_BUSY = -5
 BN254 = 0
 BLS12_381 = 1
 BLS12_377 = 2
+BN254_G2 = 3
 SCALAR_INT = 0
 SCALAR_MONT = 1
 
-FP_BYTES = {BN254: 32, BLS12_381: 48, BLS12_377: 48}
+FP_BYTES = {BN254: 32, BLS12_381: 48, BLS12_377: 48, BN254_G2: 64}  # bytes per coordinate
 
 c_u8p = ctypes.c_void_p
 c_vp = ctypes.c_void_p
@@ -65,6 +66,8 @@ _SIGS = {
     "zkmetal_bls12_377_g1_msm": (c_i32, [c_vp, c_u8p, c_u8p, c_u32, c_u8p, c_u8p, c_u8p]),
     "zkmetal_bls12_377_g1_msm_fr": (c_i32, [c_vp, c_u8p, c_u8p, c_u32, c_u8p, c_u8p, c_u8p]),
     "zkmetal_bls12_377_g1_msm_batch": (c_i32, [c_vp, c_u8p, c_u8p, c_vp, c_u32, c_u8p]),
+    "zkmetal_bn254_g2_msm": (c_i32, [c_vp, c_u8p, c_u8p, c_u32, c_u8p, c_u8p, c_u8p]),
+    "zkmetal_bn254_g2_msm_fr": (c_i32, [c_vp, c_u8p, c_u8p, c_u32, c_u8p, c_u8p, c_u8p]),
     "zkmetal_set_shader_dir": (None, [ctypes.c_char_p]),
     "zkmetal_gpu_available": (c_i32, []),
     "zkmetal_version": (ctypes.c_char_p, []),

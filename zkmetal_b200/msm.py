@@ -177,6 +177,22 @@ class BLS12377MSM(_Engine):
         return self._call(_l.lib().zkmetal_bls12_377_g1_msm_fr, p, s, n)
 
 
+class BN254G2MSM(_Engine):
+    """BN254 G2 MSM engine (BN254G2MSMEngine.swift:51; msm at :289): points
+    are G2AffinePoint (x.c0, x.c1, y.c0, y.c1, 32 B each, Montgomery), the
+    result a G2ProjectivePoint with 64 B Fp2 coordinates."""
+
+    curve = _l.BN254_G2
+
+    def msm(self, points, scalars):
+        p, s, n = self._prep(points, scalars)
+        return self._call(_l.lib().zkmetal_bn254_g2_msm, p, s, n)
+
+    def msmFr(self, points, scalars_mont):
+        p, s, n = self._prep(points, scalars_mont)
+        return self._call(_l.lib().zkmetal_bn254_g2_msm_fr, p, s, n)
+
+
 def multiMSM(engine, points, scalar_sets):
     """k MSMs over the same bases (MultiMSM.swift:21-72), run as one batch.
 
