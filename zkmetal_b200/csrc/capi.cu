@@ -572,8 +572,10 @@ ZkMetalStatus zkmsm_table_create(ZkMetalMSMEngine engine, int curve, const void*
         Engine& e = ENG(engine);
         std::unique_ptr<Table> t(new Table{&e, curve, n, {}, {}});
         size_t bytes = (size_t)n * 2 * fp_bytes(curve);
-        t->points.ensure(bytes);
-        t->phi.ensure(bytes);
+        t->points.alloc_exact(bytes);
+        with_curve(curve, [&](auto cv) {
+            if (CurveTraits<decltype(cv)>::glv) t->phi.alloc_exact(bytes);
+        });
         ZK_CUDA(cudaMemcpyAsync(t->points.p, points, bytes, on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
                                 e.stream));
         with_curve(curve, [&](auto cv) {
@@ -602,7 +604,7 @@ ZkMetalStatus zkmsm_table_precompute(ZkMsmTable table, int spacing_bits) {
         Engine& e = *t.engine;
         const size_t ab = (size_t)2 * fp_bytes(t.curve);
         DevBuf nb;
-        nb.ensure((size_t)copies * t.n * ab);
+        nb.alloc_exact((size_t)copies * t.n * ab);
         ZK_CUDA(cudaMemcpyAsync(nb.p, t.points.p, (size_t)t.n * ab, cudaMemcpyDeviceToDevice, e.stream));
         with_curve(t.curve, [&](auto cv) { e.make_shifts<decltype(cv)>(nb.as<uint32_t>(), t.n, s, copies); });
         ZK_CUDA(cudaStreamSynchronize(e.stream));

@@ -68,6 +68,14 @@ struct DevBuf {
         cap = want;
         return true;
     }
+    // exactly `bytes` (synchronous allocation, contents dropped): for
+    // long-lived buffers such as resident tables, where growth slack would
+    // waste gigabytes
+    void alloc_exact(size_t bytes) {
+        release();
+        ZK_CUDA(cudaMalloc(&p, bytes));
+        cap = bytes;
+    }
     template <class T>
     T* as() const { return static_cast<T*>(p); }
     void release() {

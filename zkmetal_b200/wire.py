@@ -27,8 +27,18 @@ R_BN254 = 1 << 256
 
 
 def _hex_int(s):
-    s = s[2:] if s.startswith("0x") else s
-    return int(s, 16) if s else 0
+    """Coordinate string -> integer as fpFromHex reads it: left-padded to 64
+    hex digits, four 16-digit limbs, a limb that does not parse is 0."""
+    clean = s[2:] if s.startswith("0x") else s
+    padded = "0" * max(0, 64 - len(clean)) + clean
+    v = 0
+    for i in range(4):
+        try:
+            limb = int(padded[i * 16:(i + 1) * 16], 16)
+        except ValueError:
+            limb = 0
+        v = (v << 64) | limb
+    return v
 
 
 def _scalar_limbs(s):
