@@ -96,8 +96,12 @@ void Engine::enqueue(const Plan& pl, const uint32_t* d_bases, const uint32_t* d_
             launches++;
         } else {
             const Xyzz<P>* ivals = w_pvals[cur ^ 1].as<Xyzz<P>>();
-            k_acc_lj<C><<<(T + 255) / 256, 256, 0, stream>>>(keys, ivals, d_len, K, w_cnt.as<uint32_t>(),
-                                                             buckets, okeys, ovals);
+            if (T <= RED_INLINE_MAX_NODES)  // few threads: latency-bound
+                k_acc_lj<C, true><<<(T + 255) / 256, 256, 0, stream>>>(keys, ivals, d_len, K, w_cnt.as<uint32_t>(),
+                                                                       buckets, okeys, ovals);
+            else
+                k_acc_lj<C, false><<<(T + 255) / 256, 256, 0, stream>>>(keys, ivals, d_len, K,
+                                                                        w_cnt.as<uint32_t>(), buckets, okeys, ovals);
             launches++;
         }
         ZK_CUDA(cudaGetLastError());
@@ -141,8 +145,7 @@ void Engine::enqueue_reduce(const Plan& pl, const void* bucket_base, uint32_t* d
         rc ^= 1;
     }
     if (ev) prof_mark(*ev, 4);
-    k_combine<C><<<(nd + COMBINE_WARPS - 1) / COMBINE_WARPS, 32 * COMBINE_WARPS, 0, stream>>>(inS, inW, dd, nd,
-                                                                                              d_results);
+    k_combine<C><<<nd, 32 * COMBINE_WARPS, 0, stream>>>(inS, inW, dd, nd, d_results);
     launches++;
     ZK_CUDA(cudaGetLastError());
     if (ev) prof_mark(*ev, 5);

@@ -802,8 +802,10 @@ __global__ void __launch_bounds__(128) k_bucket_fold(Xyzz<typename C::Fp>* __res
     store_xyzz(b + i, acc);
 }
 
-// Level >= 2: the same over partial sums (XYZZ + XYZZ additions).
-template <class C>
+// Level >= 2: the same over partial sums (XYZZ + XYZZ additions).  INL:
+// inline products, for levels of few threads (latency-bound: an inline
+// addition has ~40% less latency than one with out-of-line products).
+template <class C, bool INL>
 __global__ void __launch_bounds__(256) k_acc_lj(const uint32_t* __restrict__ keys,
                                                 const Xyzz<typename C::Fp>* __restrict__ vals,
                                                 const uint32_t* __restrict__ d_len, uint32_t K,
@@ -841,7 +843,7 @@ __global__ void __launch_bounds__(256) k_acc_lj(const uint32_t* __restrict__ key
         }
         Xyzz<P> q;
         load_xyzz(q, vals + i);
-        xyzz_add(acc, q);
+        xyzz_add<P, INL>(acc, q);
     }
     bool cont_after = end < M && keys[end] == cur;
     if ((first_run && cont_before) || cont_after) {
@@ -910,16 +912,23 @@ __global__ void __launch_bounds__(128) k_reduce_level(const Xyzz<typename C::Fp>
     store_xyzz(outW + g, x);
 }
 
-// Window combine, one warp per MSM: R = sum_w 2^bit(w) * (S_w + W_w).  Lane
-// l forms the sums of windows 2l and 2l + 1, folds them into
-// G_l = T_2l + 2^width(2l) T_2l+1 and shifts G_l to its own bit offset,
-// 2^bit(2l) G_l: all lanes double in one converged loop, so the warp spends
-// the largest offset once (the doublings of Horner's rule, no more).  A tree
-// of warp shuffles then adds the G_l: log2(windows) + 3 additions on the
-// critical path instead of two per window.  Lane 0 normalises to affine and
-// writes the reference-layout Jacobian (X, Y, Z) Montgomery with Z = 1 (or
-// the identity (1, 1, 0)).  Up to 64 windows; a shift-table MSM has one
-// window sum and no doublings.
+// Window combine, one block of four warps per MSM:
+// R = sum_w 2^bit(w) * (S_w + W_w).  Lane l owns windows 2l and 2l + 1; it
+// forms G_l = T_2l + 2^width(2l) T_2l+1 (T_w = S_w + W_w) and shifts G_l to
+// its bit offset, 2^bit(2l) G_l; a tree of warp shuffles then adds the G_l,
+// and lane 0 normalises to affine and writes the reference-layout Jacobian
+// (X, Y, Z) Montgomery with Z = 1 (or the identity (1, 1, 0)).  The critical
+// path holds the doublings of Horner's rule (for the top window) but only
+// log2(windows) + 3 additions.
+//
+// Doublings are the bulk of that path, and one warp does a doubling's nine
+// products one after another (a product occupies the warp's scheduler for
+// ~830 cycles).  So the four warps share every doubling: its products form
+// three layers of at most four independent ones (dbl-2008-s-1 in XYZZ),
+// each warp takes one product of a layer for all 32 lanes' points, on its
+// own scheduler, and the values pass through shared memory between layers.
+// Additions and the normalisation run on warp 0.  Up to 64 windows; a
+// shift-table MSM has one window sum and no doublings.
 constexpr uint32_t COMBINE_WARPS = 4;
 
 template <class P>
@@ -933,52 +942,196 @@ ZK_DEV void shfl_down_xyzz(Xyzz<P>& r, const Xyzz<P>& a, uint32_t delta) {
     }
 }
 
+// one field element per lane, word-major (conflict-free for 32 lanes)
+template <class P>
+struct SmFe {
+    uint32_t w[P::N][32];
+    ZK_DEV void get(Fe<P>& a, uint32_t lane) const {
+#pragma unroll
+        for (int i = 0; i < P::N; i++) a.v[i] = w[i][lane];
+    }
+    ZK_DEV void put(uint32_t lane, const Fe<P>& a) {
+#pragma unroll
+        for (int i = 0; i < P::N; i++) w[i][lane] = a.v[i];
+    }
+};
+
+template <class P>
+struct CombineShared {
+    SmFe<P> x, y, zz, zzz;                        // the lanes' points
+    SmFe<P> v, x2, w, s, m, m2, zz3, zzz3, wy, x3, y3a;  // products of one doubling
+};
+
+// All four warps double lane l's point cnt(l) times (cnt from `cnt_of`, the
+// same in every warp), in lockstep: three product layers and a write-back
+// per doubling, separated by block barriers.
+template <class P, class F>
+ZK_DEV void coop_doublings(CombineShared<P>& sh, uint32_t lane, uint32_t warp, F cnt_of) {
+    const uint32_t cnt = cnt_of(lane);
+    const uint32_t most = __reduce_max_sync(0xffffffffu, cnt);
+#pragma unroll 1
+    for (uint32_t b = 0; b < most; b++) {
+        const bool act = b < cnt;
+        Fe<P> a, c, t;
+        // layer 1: V = (2Y)^2 | X2 = X^2
+        if (act && warp == 0) {
+            sh.y.get(a, lane);
+            fe_dbl(a, a);
+            fe_mul_x<true>(t, a, a);
+            sh.v.put(lane, t);
+        } else if (act && warp == 1) {
+            sh.x.get(a, lane);
+            fe_mul_x<true>(t, a, a);
+            sh.x2.put(lane, t);
+        }
+        __syncthreads();
+        // layer 2: W = U*V | S = X*V | M = 3*X2, M2 = M^2 | ZZ3 = V*ZZ
+        if (act) {
+            if (warp == 0) {
+                sh.y.get(a, lane);
+                fe_dbl(a, a);
+                sh.v.get(c, lane);
+                fe_mul_x<true>(t, a, c);
+                sh.w.put(lane, t);
+            } else if (warp == 1) {
+                sh.x.get(a, lane);
+                sh.v.get(c, lane);
+                fe_mul_x<true>(t, a, c);
+                sh.s.put(lane, t);
+            } else if (warp == 2) {
+                sh.x2.get(a, lane);
+                fe_dbl(c, a);
+                fe_add(a, a, c);
+                sh.m.put(lane, a);
+                fe_mul_x<true>(t, a, a);
+                sh.m2.put(lane, t);
+            } else {
+                sh.v.get(a, lane);
+                sh.zz.get(c, lane);
+                fe_mul_x<true>(t, a, c);
+                sh.zz3.put(lane, t);
+            }
+        }
+        __syncthreads();
+        // layer 3: ZZZ3 = W*ZZZ | W*Y | X3 = M2 - 2S, M*(S - X3)
+        if (act) {
+            if (warp == 0) {
+                sh.w.get(a, lane);
+                sh.zzz.get(c, lane);
+                fe_mul_x<true>(t, a, c);
+                sh.zzz3.put(lane, t);
+            } else if (warp == 1) {
+                sh.w.get(a, lane);
+                sh.y.get(c, lane);
+                fe_mul_x<true>(t, a, c);
+                sh.wy.put(lane, t);
+            } else if (warp == 2) {
+                Fe<P> sv, x3;
+                sh.m2.get(a, lane);
+                sh.s.get(sv, lane);
+                fe_sub(a, a, sv);
+                fe_sub(x3, a, sv);
+                sh.x3.put(lane, x3);
+                fe_sub(a, sv, x3);
+                sh.m.get(c, lane);
+                fe_mul_x<true>(t, c, a);
+                sh.y3a.put(lane, t);
+            }
+        }
+        __syncthreads();
+        // write-back; the identity and 2-torsion stay / become the identity
+        if (act && warp == 0) {
+            Xyzz<P> pt;
+            sh.zz.get(pt.zz, lane);
+            sh.y.get(pt.y, lane);
+            if (xyzz_is_id(pt) || fe_is_zero(pt.y)) {
+                xyzz_set_id(pt);
+            } else {
+                sh.x3.get(pt.x, lane);
+                sh.y3a.get(a, lane);
+                sh.wy.get(c, lane);
+                fe_sub(pt.y, a, c);
+                sh.zz3.get(pt.zz, lane);
+                sh.zzz3.get(pt.zzz, lane);
+            }
+            sh.x.put(lane, pt.x);
+            sh.y.put(lane, pt.y);
+            sh.zz.put(lane, pt.zz);
+            sh.zzz.put(lane, pt.zzz);
+        }
+        __syncthreads();
+    }
+}
+
 template <class C>
 __global__ void __launch_bounds__(32 * COMBINE_WARPS) k_combine(const Xyzz<typename C::Fp>* __restrict__ rootS,
                                                                const Xyzz<typename C::Fp>* __restrict__ rootW,
                                                                const MsmDesc* __restrict__ descs, int nd,
                                                                uint32_t* __restrict__ out) {
     using P = typename C::Fp;
-    const uint32_t lane = threadIdx.x & 31;
-    const int m = (int)(blockIdx.x * COMBINE_WARPS + (threadIdx.x >> 5));
-    if (m >= nd) return;  // warp-uniform
+    __shared__ CombineShared<P> sh;
+    const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int m = (int)blockIdx.x;
+    if (m >= nd) return;  // block-uniform
     const MsmDesc d = descs[m];
     uint32_t* o = out + (size_t)m * 3 * P::N;
     Fe<P> one;
     fe_set_one(one);
     if (d.n == 0) {
-        if (lane == 0)
+        if (threadIdx.x == 0)
             for (int l = 0; l < P::N; l++) { o[l] = one.v[l]; o[P::N + l] = one.v[l]; o[2 * P::N + l] = 0; }
         return;
     }
     const uint32_t nw = d.nred;
     const uint32_t w0 = 2 * lane;
     Xyzz<P> g, q;
-    xyzz_set_id(g);
-    if (w0 + 1 < nw) {
-        load_xyzz(g, rootS + d.win_off + w0 + 1);
-        load_xyzz(q, rootW + d.win_off + w0 + 1);
-        xyzz_add<P, true>(g, q);
-#pragma unroll 1
-        for (uint32_t b = 0; b < win_width(d, w0); b++) xyzz_dbl<P, true>(g, g);
+    // T_2l+1, to be shifted by the width of window 2l
+    if (warp == 0) {
+        xyzz_set_id(g);
+        if (w0 + 1 < nw) {
+            load_xyzz(g, rootS + d.win_off + w0 + 1);
+            load_xyzz(q, rootW + d.win_off + w0 + 1);
+            xyzz_add<P, true>(g, q);
+        }
+        sh.x.put(lane, g.x);
+        sh.y.put(lane, g.y);
+        sh.zz.put(lane, g.zz);
+        sh.zzz.put(lane, g.zzz);
     }
-    if (w0 < nw) {
-        load_xyzz(q, rootS + d.win_off + w0);
-        xyzz_add<P, true>(g, q);
-        load_xyzz(q, rootW + d.win_off + w0);
-        xyzz_add<P, true>(g, q);
+    __syncthreads();
+    coop_doublings<P>(sh, lane, warp, [&](uint32_t l) { return 2 * l + 1 < nw ? win_width(d, 2 * l) : 0u; });
+    // G_l = T_2l + 2^width(2l) T_2l+1, then shifted to bit(2l)
+    if (warp == 0) {
+        sh.x.get(g.x, lane);
+        sh.y.get(g.y, lane);
+        sh.zz.get(g.zz, lane);
+        sh.zzz.get(g.zzz, lane);
+        if (w0 < nw) {
+            load_xyzz(q, rootS + d.win_off + w0);
+            xyzz_add<P, true>(g, q);
+            load_xyzz(q, rootW + d.win_off + w0);
+            xyzz_add<P, true>(g, q);
+        }
+        sh.x.put(lane, g.x);
+        sh.y.put(lane, g.y);
+        sh.zz.put(lane, g.zz);
+        sh.zzz.put(lane, g.zzz);
     }
-    const uint32_t shift = w0 < nw ? win_bit(d, w0) : 0u;
-#pragma unroll 1
-    for (uint32_t b = 0; b < shift; b++) xyzz_dbl<P, true>(g, g);
+    __syncthreads();
+    coop_doublings<P>(sh, lane, warp, [&](uint32_t l) { return 2 * l < nw ? win_bit(d, 2 * l) : 0u; });
+    if (warp != 0) return;
+    sh.x.get(g.x, lane);
+    sh.y.get(g.y, lane);
+    sh.zz.get(g.zz, lane);
+    sh.zzz.get(g.zzz, lane);
 #pragma unroll 1
     for (uint32_t st = 1; st < 32; st <<= 1) {
-        shfl_down_xyzz(q, g, st);  // every lane takes part in the shuffle
+        shfl_down_xyzz(q, g, st);  // every lane of warp 0 takes part in the shuffle
         if ((lane & (2 * st - 1)) == 0 && 2 * (lane + st) < nw) xyzz_add<P, true>(g, q);
     }
     if (lane == 0) {
         // normalise a copy: passing g itself to the out-of-line call would
-        // take its address and keep it in local memory through the loops
+        // take its address and keep it in local memory
         Xyzz<P> t = g;
         Affine<P> a;
         xyzz_to_affine_ni(a, t);

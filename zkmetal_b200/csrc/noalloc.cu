@@ -205,7 +205,8 @@ extern "C" ZkMetalStatus zkmsm_bn254_msm_noalloc(const void* d_points, const voi
             k_acc_l1<C><<<(Tl + AccLaunch<C>::THREADS - 1) / AccLaunch<C>::THREADS, AccLaunch<C>::THREADS, 0, s>>>(ents, tot + l, Kl, pts, phi, cnt, buckets, pk[cur],
                                                           pv[cur]);
         else
-            k_acc_lj<C><<<(Tl + 255) / 256, 256, 0, s>>>(lk, pv[cur ^ 1], tot + l, Kl, cnt, buckets, pk[cur], pv[cur]);
+            k_acc_lj<C, false><<<(Tl + 255) / 256, 256, 0, s>>>(lk, pv[cur ^ 1], tot + l, Kl, cnt, buckets, pk[cur],
+                                                               pv[cur]);
         lk = pk[cur];
         ks = 1;
         cur ^= 1;
