@@ -173,3 +173,30 @@ def test_server_large_batch_matches_plain(eng):
     finally:
         srv.close()
         table.close()
+
+
+@pytest.mark.parametrize("shift", [0, 4])
+def test_grouped_batch_from_host_scalars(eng, shift):
+    """A batch of host scalars large enough to run as groups (copy of group g
+    + 1 overlapping group g) equals the plain MSMs, with and without window
+    shifts, zero counts included."""
+    e = eng["bn254"]
+    T = 1 << 22
+    p, _ = gen_inputs(e, "bn254", 141, T, "uniform", zl.SCALAR_MONT)
+    counts = [T, 1 << 19, 3, 0, T, 777, 0]   # over 2^23 points: two groups
+    sc = scalars_host(e, "bn254", 142, sum(counts), "witness")
+    table = CommitmentTable(e, p.data_ptr(), on_device=True, n=T)
+    try:
+        if shift:
+            table.precompute(shift)
+        res = table.batch_commit(sc, counts, fmt=zl.SCALAR_MONT)
+    finally:
+        table.close()
+    off = 0
+    for i, c in enumerate(counts):
+        got = res[i].x + res[i].y + res[i].z
+        if c == 0:
+            assert got == bytes(96)
+        else:
+            assert got == plain(e, "bn254", p, sc[off * 32:], c), (i, c)
+        off += c
