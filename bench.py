@@ -106,7 +106,7 @@ def executed_products(n, curve_id=0, window=0):
     return json.loads(buf.value.decode())["entry_bound"] * 10 * (2 * limbs * limbs + limbs)
 
 
-def reference_cpu_msm_ms(n_sample, points_b, scalars_mont_b, repeats=1):
+def reference_cpu_msm_ms(n_sample, points_b, scalars_mont_b, repeats=1, scalars_are_int=False):
     """Time the reference C Pippenger on host cores; returns (ms per run, threads, kind)."""
     from oracle import lib as olib
     from oracle import build as obuild
@@ -118,7 +118,8 @@ def reference_cpu_msm_ms(n_sample, points_b, scalars_mont_b, repeats=1):
             pass
     kind = "reference" if os.path.exists(olib.REF_LIB) else "port"
     orc = olib.RefOracle() if kind == "reference" else olib.COracle()
-    sc_int = orc.fr_from_mont("bn254", scalars_mont_b, n_sample)  # conversion timed separately (not here)
+    sc_int = scalars_mont_b if scalars_are_int else \
+        orc.fr_from_mont("bn254", scalars_mont_b, n_sample)  # conversion timed separately (not here)
     times = []
     for _ in range(repeats):
         t0 = time.perf_counter()
@@ -150,17 +151,55 @@ def host_inputs(n, seed, index0=0):
     return pb, sb
 
 
+def host_inputs_cpu(n, seed, distinct_log2=16):
+    """Inputs for the reference arm made on the host alone (no GPU, none of
+    this library): 2^distinct_log2 distinct bases k_i*G from the C
+    restatement, repeated to n points (the Pippenger's cost does not depend on
+    bases repeating), and n integer scalars uniform in [0, r)."""
+    import numpy as np
+    from oracle import build as obuild
+    from oracle import lib as olib
+    from oracle import pyref as R
+    obuild.build_cmsm()
+    C = R.BN254
+    rng = np.random.default_rng(seed)
+
+    def uniform_fr(m):
+        out = np.empty((m, 8), dtype=np.uint32)
+        filled = 0
+        while filled < m:
+            w = rng.integers(0, 1 << 32, size=(m - filled, 8), dtype=np.uint64).astype(np.uint32)
+            w[:, 7] &= (1 << (C.r.bit_length() - 224)) - 1
+            r_top = C.r >> 224
+            keep = w[:, 7] < r_top  # rows with the top limb of r need the full comparison
+            for i in np.nonzero(w[:, 7] == r_top)[0]:
+                keep[i] = int.from_bytes(w[i].tobytes(), "little") < C.r
+            k = int(keep.sum())
+            out[filled:filled + k] = w[keep]
+            filled += k
+        return out
+
+    d = min(n, 1 << distinct_log2)
+    ks = uniform_fr(d)
+    ks[ks.sum(axis=1) == 0, 0] = 1  # k_i >= 1
+    bases = np.frombuffer(olib.COracle().fixed_base_mul("bn254", C.enc_affine((C.gx, C.gy)), ks.tobytes(), d),
+                          dtype=np.uint8).reshape(d, 64)
+    pb = np.tile(bases, (-(-n // d), 1))[:n].tobytes()
+    sb = uniform_fr(n).tobytes()
+    return pb, sb
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
     n_full = 1 << args.log2n
     n_sample = min(n_full, 1 << args.cpu_log2n)
-    pb, sb = host_inputs(n_sample, args.seed)
+    pb, sb = host_inputs_cpu(n_sample, args.seed)
     scale = n_full / n_sample
     ms_all = []
     for i in range(args.warmup + args.steps):
-        ms, threads, kind = reference_cpu_msm_ms(n_sample, pb, sb)
+        ms, threads, kind = reference_cpu_msm_ms(n_sample, pb, sb, scalars_are_int=True)
         if i >= args.warmup:
             ms_all.append(ms * scale)
     v = statistics.mean(ms_all)
@@ -169,8 +208,8 @@ def run_reference(args):
     line = {"metric": METRIC, "value": round(v, 3), "unit": "ms", "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(v, 3), "higher_is_better": False, "scaling": "weak",
             "vs_baseline": None, "dtype": "u64", "data": "synthetic", "impl": "reference",
-            "config": {"workload": "bn254_g1_msm", "n": n_full, "scalars": "uniform Fr (Montgomery form)",
-                       "bases": "k_i*G, k_i uniform in [1,r)"},
+            "config": {"workload": "bn254_g1_msm", "n": n_full, "scalars": "uniform Fr (integer form)",
+                       "bases": "k_i*G, k_i uniform in [1,r): 2^16 distinct bases repeated (made on the host)"},
             "cpu_baseline": {"value": round(v, 3), "unit": "ms", "cores": threads, "kind": kind, "sample": sample},
             "e2e": {"value": round(v, 3), "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
