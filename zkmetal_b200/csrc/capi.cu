@@ -182,6 +182,9 @@ static void msm_host_striped(Engine& e, const uint8_t* points, const uint8_t* sc
     ZK_CUDA(cudaStreamSynchronize(e.stream));
 }
 
+// host-buffer MSMs up to this many points run as a replayed CUDA graph
+constexpr uint32_t SMALL_GRAPH_POINTS = 1u << 16;
+
 template <class C>
 static ZkMetalStatus msm_host(Engine& e, const uint8_t* points, const uint8_t* scalars, uint32_t n, int fmt,
                               uint32_t scalar_bits, uint8_t* rx, uint8_t* ry, uint8_t* rz) {
@@ -206,8 +209,14 @@ static ZkMetalStatus msm_host(Engine& e, const uint8_t* points, const uint8_t* s
         e.make_phi<C>(e.w_points.as<uint32_t>(), n, e.w_phi.as<uint32_t>());
     }
     uint8_t out[3 * 4 * MAX_COORD_WORDS];
-    e.run_device<C>(pl, e.w_points.as<uint32_t>(), glv ? e.w_phi.as<uint32_t>() : e.w_points.as<uint32_t>(),
-                    e.w_scalars.as<uint32_t>(), out);
+    const uint32_t* phi = glv ? e.w_phi.as<uint32_t>() : e.w_points.as<uint32_t>();
+    // small MSMs are a chain of ~30 short launches: replay them as one CUDA
+    // graph (captured on the first call of a shape; the buffers are the
+    // engine's own, so later calls of the same size replay it)
+    if (n <= SMALL_GRAPH_POINTS)
+        e.run_device_graph<C>(pl, e.w_points.as<uint32_t>(), phi, e.w_scalars.as<uint32_t>(), out);
+    else
+        e.run_device<C>(pl, e.w_points.as<uint32_t>(), phi, e.w_scalars.as<uint32_t>(), out);
     memcpy(rx, out, fb);
     memcpy(ry, out + fb, fb);
     memcpy(rz, out + 2 * fb, fb);

@@ -12,7 +12,12 @@ namespace zkmsm {
 // Exclusive scan of n u32 in place; total to d_total; optional copy.
 static void scan_u32(Engine& e, uint32_t* d_in_out, uint32_t n, uint32_t* d_total, uint32_t* d_copy) {
     uint32_t tiles = (n + SCAN_TILE - 1) / SCAN_TILE;
-    if (tiles == 0) tiles = 1;  // w_tiles is sized by ensure_workspace (no allocation here: graph capture)
+    if (tiles <= 1) {
+        k_scan_single<<<1, SCAN_THREADS, 0, e.stream>>>(d_in_out, n, d_total, d_copy);
+        e.launches++;
+        ZK_CUDA(cudaGetLastError());
+        return;
+    }
     k_scan_tiles<<<tiles, SCAN_THREADS, 0, e.stream>>>(d_in_out, n, d_in_out, e.w_tiles.as<uint32_t>());
     e.launches++;
     k_scan_sums<<<1, SCAN_THREADS, 0, e.stream>>>(e.w_tiles.as<uint32_t>(), tiles, d_total);

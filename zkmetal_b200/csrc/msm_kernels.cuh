@@ -1198,6 +1198,32 @@ static __global__ void __launch_bounds__(SCAN_THREADS) k_scan_tiles(const uint32
     if (threadIdx.x == 0) tile_sums[blockIdx.x] = total;
 }
 
+// the whole scan in one launch when the array fits one tile (small MSMs run a
+// dozen such scans, each otherwise three dependent launches)
+static __global__ void __launch_bounds__(SCAN_THREADS) k_scan_single(uint32_t* __restrict__ data, uint32_t n,
+                                                              uint32_t* __restrict__ d_total,
+                                                              uint32_t* __restrict__ copy) {
+    __shared__ uint32_t sh[SCAN_THREADS / 32];
+    const uint32_t base = threadIdx.x * SCAN_ITEMS;
+    uint32_t v[SCAN_ITEMS], s = 0;
+#pragma unroll
+    for (int i = 0; i < SCAN_ITEMS; i++) {
+        v[i] = base + i < n ? data[base + i] : 0;
+        s += v[i];
+    }
+    uint32_t total;
+    uint32_t pre = block_excl_scan(s, sh, total);
+#pragma unroll
+    for (int i = 0; i < SCAN_ITEMS; i++) {
+        if (base + i < n) {
+            data[base + i] = pre;
+            if (copy) copy[base + i] = pre;
+        }
+        pre += v[i];
+    }
+    if (threadIdx.x == 0) *d_total = total;
+}
+
 // phase 2: one block scans the tile totals in place; writes the grand total
 static __global__ void __launch_bounds__(SCAN_THREADS) k_scan_sums(uint32_t* __restrict__ tile_sums, uint32_t ntiles,
                                                             uint32_t* __restrict__ d_total) {
