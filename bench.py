@@ -619,7 +619,7 @@ def run_bls377_config(seed=0x5EED0005, log2n=22, steps=5):
 
 
 def run_g2_config(seed=0x5EED0006, log2n=20, steps=3):
-    """BN254 G2 (Fp2 coordinates, no endomorphism split): plain MSMs with
+    """BN254 G2 (Fp2 coordinates, GLV with the twist's Frobenius endomorphism): plain MSMs with
     device-resident bases and uniform Montgomery scalars at 2^16 and 2^20,
     device ms per MSM (CUDA events on the library's stream)."""
     import torch

@@ -131,7 +131,7 @@ ZkMetalStatus zkmetal_bls12_377_g1_msm_batch(ZkMetalMSMEngine engine, const uint
  * y.c0, y.c1, each 32 B Montgomery: G2AffinePoint of
  * Curve/BN254Pairing.swift:301-305); results x, y, z as 64 B Fp2 elements
  * (Z = 1 = (1, 0), or the identity (1, 1, 0) with z = 0).  Scalars as in the
- * BN254 G1 calls; no endomorphism split. */
+ * BN254 G1 calls; the GLV split uses the twist's Frobenius endomorphism. */
 ZkMetalStatus zkmetal_bn254_g2_msm(ZkMetalMSMEngine engine, const uint8_t* points, const uint8_t* scalars,
                                    uint32_t n_points, uint8_t* result_x, uint8_t* result_y, uint8_t* result_z);
 ZkMetalStatus zkmetal_bn254_g2_msm_fr(ZkMetalMSMEngine engine, const uint8_t* points, const uint8_t* scalars_mont,

@@ -278,9 +278,9 @@ struct CurveTraits<Bls377> {
 };
 template <>
 struct CurveTraits<Bn254G2> {
-    static constexpr bool glv = false;  // plain 254-bit windows
+    static constexpr bool glv = true;  // split with psi
     static constexpr int id = 3;
-    static constexpr uint32_t half_bits = Bn254Fr::BITS;
+    static constexpr uint32_t half_bits = Bn254G2Glv::HALF_BITS;
     static constexpr uint32_t fr_bits = Bn254Fr::BITS;
 };
 

@@ -40,6 +40,14 @@ ZK_DEV void fp2_join(Fe<Fp2Of<B>>& r, const Fe<B>& c0, const Fe<B>& c1) {
     }
 }
 
+// conj(c0 + c1 u) = c0 - c1 u (the Frobenius map of Fp2), in place
+template <class B>
+ZK_DEV void conj_fp2(Fe<Fp2Of<B>>& a) {
+    Fe<B> c0, c1;
+    fp2_split(a, c0, c1);
+    fe_neg(c1, c1);
+    fp2_join(a, c0, c1);
+}
 template <class B>
 ZK_DEV void fe_set_one(Fe<Fp2Of<B>>& r) {
 #pragma unroll

@@ -582,7 +582,9 @@ ZK_DEV void store_xyzz(Xyzz<P>* dst, const Xyzz<P>& a) {
 
 // ------------------------------------------------------------ endomorphism
 
-// phi[i] = (beta * x_i, y_i)   [glv_kernels.metal:260-297]
+// phi[i] = (beta * x_i, y_i)   [glv_kernels.metal:260-297]; on BN254 G2
+// (Glv::PSI) the image is psi(P) = (conj(x) * GAMMA1, conj(y) * GAMMA2), the
+// Frobenius endomorphism of the twist, = (p mod r) * P on G2
 template <class C>
 __global__ void __launch_bounds__(256) k_endo(const uint32_t* __restrict__ bases, uint32_t n,
                                               uint32_t* __restrict__ phi) {
@@ -591,10 +593,23 @@ __global__ void __launch_bounds__(256) k_endo(const uint32_t* __restrict__ bases
     if (i >= n) return;
     Affine<P> a;
     load_affine(a, bases, i);
-    Fe<P> beta;
+    if constexpr (C::Glv::PSI) {
+        Fe<P> g1, g2;
 #pragma unroll
-    for (int l = 0; l < P::N; l++) beta.v[l] = C::Glv::BETA_MONT(l);
-    fe_mul(a.x, a.x, beta);
+        for (int l = 0; l < P::N; l++) {
+            g1.v[l] = C::Glv::GAMMA1_MONT(l);
+            g2.v[l] = C::Glv::GAMMA2_MONT(l);
+        }
+        conj_fp2(a.x);
+        conj_fp2(a.y);
+        fe_mul(a.x, a.x, g1);
+        fe_mul(a.y, a.y, g2);
+    } else {
+        Fe<P> beta;
+#pragma unroll
+        for (int l = 0; l < P::N; l++) beta.v[l] = C::Glv::BETA_MONT(l);
+        fe_mul(a.x, a.x, beta);
+    }
     uint4* d = reinterpret_cast<uint4*>(phi + (size_t)i * 2 * P::N);
     store_fe(d, a.x);
     store_fe(d + P::N / 4, a.y);

@@ -14,9 +14,9 @@ struct CurveCfg {
 using Bn254 = CurveCfg<Bn254Fp, Bn254Fr, Bn254Glv, Bn254Gen>;
 using Bls381 = CurveCfg<Bls381Fp, Bls381Fr, Bls381Glv, Bls381Gen>;
 using Bls377 = CurveCfg<Bls377Fp, Bls377Fr, Bls377Glv, Bls377Gen>;
-// BN254 G2: Fp2 coordinates, the same scalar field; no endomorphism split
-// (Bn254Glv only fills the template: G2 plans never use GLV)
-using Bn254G2 = CurveCfg<Fp2Of<Bn254Fp>, Bn254Fr, Bn254Glv, Bn254G2Gen>;
+// BN254 G2: Fp2 coordinates, the same scalar field; GLV with the
+// endomorphism psi (eigenvalue p mod r) instead of phi
+using Bn254G2 = CurveCfg<Fp2Of<Bn254Fp>, Bn254Fr, Bn254G2Glv, Bn254G2Gen>;
 
 // One MSM of a batch, as the kernels see it.
 struct MsmDesc {

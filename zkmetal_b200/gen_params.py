@@ -97,6 +97,42 @@ def g2_check(p, r, G):
     assert acc is None, "G2 generator order is not r"
 
 
+def g2_psi_check(p, r, G, gam1, gam2, lam):
+    """psi(P) == lam * P for P = 1234567 * G on the twist."""
+    b2 = f2_mul((3, 0), f2_inv((9, 1), p), p)
+
+    def add(A, B):
+        if A is None:
+            return B
+        if B is None:
+            return A
+        if A[0] == B[0]:
+            if f2_add(A[1], B[1], p) == (0, 0):
+                return None
+            lam_ = f2_mul(f2_mul((3, 0), f2_mul(A[0], A[0], p), p), f2_inv(f2_add(A[1], A[1], p), p), p)
+        else:
+            lam_ = f2_mul(((B[1][0] - A[1][0]) % p, (B[1][1] - A[1][1]) % p),
+                          f2_inv(((B[0][0] - A[0][0]) % p, (B[0][1] - A[0][1]) % p), p), p)
+        l2 = f2_mul(lam_, lam_, p)
+        x3 = ((l2[0] - A[0][0] - B[0][0]) % p, (l2[1] - A[0][1] - B[0][1]) % p)
+        t = f2_mul(lam_, ((A[0][0] - x3[0]) % p, (A[0][1] - x3[1]) % p), p)
+        return (x3, ((t[0] - A[1][0]) % p, (t[1] - A[1][1]) % p))
+
+    def mul(P, k):
+        acc = None
+        for bit in bin(k)[2:]:
+            acc = add(acc, acc)
+            if bit == "1":
+                acc = add(acc, P)
+        return acc
+    P = mul(G, 1234567)
+    conj = lambda a: (a[0], (-a[1]) % p)
+    psi = (f2_mul(conj(P[0]), gam1, p), f2_mul(conj(P[1]), gam2, p))
+    y2 = f2_mul(psi[1], psi[1], p)
+    on = y2 == f2_add(f2_mul(f2_mul(psi[0], psi[0], p), psi[0], p), b2, p)
+    return on and psi == mul(P, lam)
+
+
 def limbs(x, n):
     return [(x >> (32 * i)) & 0xFFFFFFFF for i in range(n)]
 
@@ -140,6 +176,14 @@ def glv(p, r, G):
         else:
             continue
         break
+    out = glv_lattice(r, lam)
+    out["beta"] = beta
+    return out
+
+
+def glv_lattice(r, lam):
+    """Short basis of {(a, b): a + b*lam = 0 mod r}, Babai multipliers and the
+    bit bound of the halves, for any endomorphism eigenvalue lam."""
     seq = [(r, 0), (lam, 1)]
     r0, r1, t0, t1 = r, lam, 0, 1
     while r1:
@@ -167,7 +211,7 @@ def glv(p, r, G):
     # |k1| < 3/4 (|a1| + |a2|), |k2| < 3/4 (|b1| + |b2|).
     bound = (3 * max(abs(a1) + abs(a2), abs(b1) + abs(b2)) + 3) // 4 + 1
     bits = bound.bit_length()
-    return dict(lam=lam, beta=beta, a1=a1, b1=b1, a2=a2, b2=b2, g1=g1, g2=g2, bits=bits)
+    return dict(lam=lam, a1=a1, b1=b1, a2=a2, b2=b2, g1=g1, g2=g2, bits=bits)
 
 
 def arr(name, vals, ctype="uint32_t"):
@@ -230,6 +274,7 @@ def emit():
         out.append("    static constexpr int REDUCE_PASSES = %d;\n" % (((1 << 256) - 1) // r))
         out.append("};\n\n")
         out.append("struct %sGlv {\n" % name)
+        out.append("    static constexpr bool PSI = false;  // the endomorphism is phi below\n")
         out.append("    // phi(x, y) = (BETA * x, y) = LAMBDA * (x, y) on G1\n")
         out.append(fn_table("BETA_MONT", limbs(g["beta"] * R % p, N)))
         out.append(fn_table("LAMBDA", limbs(g["lam"], 8)))
@@ -252,6 +297,39 @@ def emit():
     g2_check(P_BN, R_BN, G2_BN)
     R = 1 << 256
     (x0, x1), (y0, y1) = G2_BN
+    # BN254 G2 endomorphism psi(x, y) = (conj(x) * g1, conj(y) * g2) with
+    # g1 = xi^((p-1)/3), g2 = xi^((p-1)/2), xi = 9 + u: on G2 it is
+    # multiplication by lam = p mod r (checked on the generator below)
+    p = P_BN
+
+    def f2pow(a, e):
+        res, base = (1, 0), a
+        while e:
+            if e & 1:
+                res = f2_mul(res, base, p)
+            base = f2_mul(base, base, p)
+            e >>= 1
+        return res
+    gam1, gam2 = f2pow((9, 1), (p - 1) // 3), f2pow((9, 1), (p - 1) // 2)
+    lam2 = p % R_BN
+    assert g2_psi_check(p, R_BN, G2_BN, gam1, gam2, lam2), "psi is not lam * P on G2"
+    g = glv_lattice(R_BN, lam2)
+    R = 1 << 256
+    out.append("// BN254 G2: GLV with psi(x, y) = (conj(x) * GAMMA1, conj(y) * GAMMA2) = LAMBDA * (x, y)\n")
+    out.append("struct Bn254G2Glv {\n")
+    out.append("    static constexpr bool PSI = true;\n")
+    out.append(fn_table("GAMMA1_MONT", limbs(gam1[0] * R % p, 8) + limbs(gam1[1] * R % p, 8)))
+    out.append(fn_table("GAMMA2_MONT", limbs(gam2[0] * R % p, 8) + limbs(gam2[1] * R % p, 8)))
+    out.append("    __host__ __device__ static constexpr uint32_t BETA_MONT(int) { return 0u; }  // unused (PSI)\n")
+    out.append(fn_table("LAMBDA", limbs(g["lam"], 8)))
+    for key in ("a1", "b1", "a2", "b2"):
+        v = g[key]
+        out.append("    static constexpr int %s_NEG = %d;\n" % (key.upper(), 1 if v < 0 else 0))
+        out.append(fn_table(key.upper(), limbs(abs(v), 5)))
+    out.append(fn_table("G1", limbs(g["g1"], 5)))
+    out.append(fn_table("G2", limbs(g["g2"], 5)))
+    out.append("    static constexpr int HALF_BITS = %d;  // |k1|, |k2| < 2^HALF_BITS\n" % g["bits"])
+    out.append("};\n\n")
     out.append("// BN254 G2 generator on the twist y^2 = x^3 + 3/(9 + u): c0 limbs, then c1 limbs\n")
     out.append("struct Bn254G2Gen {\n")
     out.append(fn_table("X_MONT", limbs(x0 * R % P_BN, 8) + limbs(x1 * R % P_BN, 8)))
