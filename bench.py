@@ -422,24 +422,34 @@ def run_serve_config(duration_s=60.0, rate=200.0, seed=0x5EED0004, table_log2=22
             assert L.zkmsm_gen_scalars(engines[c].handle, c, seed + 10 + 2 * c + dist, 0, 2 * T, dist, 1,
                                        s.data_ptr()) == 0
             pools[(c, dist)] = _pinned(torch, s).numpy()
-    rng = np.random.default_rng(seed)
-    reqs, t = [], 0.0
-    while True:
-        t += rng.exponential(1.0 / rate)
-        if t > duration_s:
-            break
-        c = 0 if rng.random() < 0.7 else 1
-        n = int(round(2 ** rng.uniform(10, 22)))
-        dist = int(rng.random() < 0.5)
-        off = int(rng.integers(0, T))
-        reqs.append((t, c, n, dist, off))
+    def poisson(rng, horizon_s):
+        out, t = [], 0.0
+        while True:
+            t += rng.exponential(1.0 / rate)
+            if t > horizon_s:
+                return out
+            c = 0 if rng.random() < 0.7 else 1
+            n = int(round(2 ** rng.uniform(10, 22)))
+            dist = int(rng.random() < 0.5)
+            off = int(rng.integers(0, T))
+            out.append((t, c, n, dist, off))
+
+    reqs = poisson(np.random.default_rng(seed), duration_s)
     srv = CommitmentServer(tables[0], tables[1], workers=3)
-    # warm-up (untimed): a burst of the largest requests of each curve brings
-    # every worker's buffers to their working size
+    # warm-up (untimed): a burst of the largest requests of each curve, then
+    # 2 s of an independently seeded stream of the same distribution
+    # submitted at once, bring every worker's workspace to the size that
+    # full batches of many requests need (a growth that maps new device
+    # memory stalls all workers for up to a few hundred ms)
     warm = [srv.submit(c, pools[(c, 0)][:T * 32], zl.SCALAR_MONT) for c in (0, 1) for _ in range(4)]
     warm += [srv.submit(c, pools[(c, 1)][:(T >> k) * 32], zl.SCALAR_MONT) for c in (0, 1) for k in range(1, 12)]
     for i in warm:
         srv.wait(i)
+    for _ in range(2):
+        warm = [srv.submit(c, pools[(c, dist)][off * 32:(off + n) * 32], zl.SCALAR_MONT)
+                for (ta, c, n, dist, off) in poisson(np.random.default_rng(seed + 99), 2.0)]
+        for i in warm:
+            srv.wait(i)
     ids = [None] * len(reqs)
     start = time.perf_counter()
 
@@ -505,6 +515,7 @@ def run_serve_config(duration_s=60.0, rate=200.0, seed=0x5EED0004, table_log2=22
             "plain_dropin_commits_per_s": round(k / t_plain, 1),
             "speedup_vs_plain_dropin": round((len(reqs) / wall) / (k / t_plain), 2),
             "capacity_vs_plain_dropin": round((k_sat / t_sat) / (k / t_plain), 2),
+            "hbm_budget_gb": round(st["budget_bytes"] / 1e9, 1),
             "bit_exact_vs_plain": served[:k] == plain}
 
 

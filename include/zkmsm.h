@@ -202,8 +202,9 @@ const void* zkmsm_table_device_points(ZkMsmTable table);
 /* Batched commitments over a resident table: MSM i = sum_j s_ij * T[j] for
  * j < counts[i] (a prefix of the table).  scalars: concatenated 32 B scalars
  * (HOST unless scalars_on_device), results: n_msms x 3 field elements (HOST).
- * All MSMs run as one batch captured in a CUDA graph (replayed when the same
- * shape repeats); window width and chunking come from the autotuner. */
+ * All MSMs run as one batch; a shape that repeats is captured in a CUDA graph
+ * on its second call and replayed after that.  Window width and chunking
+ * come from the autotuner. */
 ZkMetalStatus zkmsm_batch_commit(ZkMetalMSMEngine engine, ZkMsmTable table, const void* scalars,
                                  int scalars_on_device, int scalar_fmt, const uint32_t* counts, uint32_t n_msms,
                                  uint8_t* results);

@@ -211,7 +211,7 @@ static ZkMetalStatus msm_host(Engine& e, const uint8_t* points, const uint8_t* s
     uint8_t out[3 * 4 * MAX_COORD_WORDS];
     const uint32_t* phi = glv ? e.w_phi.as<uint32_t>() : e.w_points.as<uint32_t>();
     // small MSMs are a chain of ~30 short launches: replay them as one CUDA
-    // graph (captured on the first call of a shape; the buffers are the
+    // graph (captured on the second call of a shape; the buffers are the
     // engine's own, so later calls of the same size replay it)
     if (n <= SMALL_GRAPH_POINTS)
         e.run_device_graph<C>(pl, e.w_points.as<uint32_t>(), phi, e.w_scalars.as<uint32_t>(), out);

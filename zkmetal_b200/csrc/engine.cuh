@@ -132,6 +132,8 @@ struct Plan {
     // device copies of descs and reduction tasks (uploaded once per plan)
     DevBuf d_descs, d_tasks;
     std::vector<size_t> task_level_off;
+    // calls of this plan through run_device_graph that found no captured graph
+    mutable uint32_t graph_misses = 0;
     // forget the host-side shape (device tables are kept for reuse)
     void clear_host() {
         descs.clear();
@@ -144,6 +146,7 @@ struct Plan {
         red_tasks.clear();
         red_nout.clear();
         task_level_off.clear();
+        graph_misses = 0;
     }
 };
 
@@ -741,6 +744,13 @@ class Engine {
         put(stream);
         auto it = graphs.find(key);
         if (it == graphs.end()) {
+            // the first call of a plan runs its launches directly: capturing
+            // and instantiating costs about as much as the launches it saves
+            // (~1 ms for a small MSM), which only a repeated shape pays back
+            if (pl.graph_misses++ == 0) {
+                run_device<C>(pl, d_bases, d_phi, d_scalars, out);
+                return;
+            }
             if (graphs.size() >= 64) drop_graphs();
             bool prof = profile;
             profile = false;

@@ -194,13 +194,26 @@ struct Server {
                     double oldest = 0;
                     for (auto& r : batch)
                         oldest = std::max(oldest, std::chrono::duration<double, std::milli>(t_b0 - r->t_submit).count());
+                    const DevBuf* ws[] = {&eng->w_counts, &eng->w_cursor, &eng->w_ents, &eng->w_ents2,
+                                          &eng->w_thist, &eng->w_buckets, &eng->w_cnt, &eng->w_pkeys[0],
+                                          &eng->w_pkeys[1], &eng->w_pvals[0], &eng->w_pvals[1], &eng->w_redS[0],
+                                          &eng->w_redS[1], &eng->w_redW[0], &eng->w_redW[1], &eng->w_tiles};
+                    uint64_t wsb = d_cap;
+                    for (const DevBuf* b : ws) wsb += b->cap;
+                    uint64_t pool_res = 0, pool_used = 0;
+                    cudaMemPool_t pool;
+                    if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+                        cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &pool_res);
+                        cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemCurrent, &pool_used);
+                    }
                     fprintf(stderr,
-                            "trace t %.3f worker %p curve %d reqs %zu points %llu run %.2f ms oldest wait %.2f ms "
-                            "growths %llu\n",
-                            std::chrono::duration<double>(t_b0 - t_created).count(), (void*)eng.get(), curve,
+                            "trace t %.3f worker %d curve %d reqs %zu points %llu run %.2f ms oldest wait %.2f ms "
+                            "growths %llu ws_mb %llu pool_res_mb %llu pool_used_mb %llu\n",
+                            std::chrono::duration<double>(t_b0 - t_created).count(), w, curve,
                             batch.size(), (unsigned long long)total,
                             std::chrono::duration<double, std::milli>(t_b1 - t_b0).count(), oldest,
-                            (unsigned long long)eng->workspace_growths);
+                            (unsigned long long)eng->workspace_growths, (unsigned long long)(wsb >> 20),
+                            (unsigned long long)(pool_res >> 20), (unsigned long long)(pool_used >> 20));
                 }
 #endif
             } catch (const CudaError& e) {
@@ -266,13 +279,15 @@ ZkMetalStatus zkmsm_server_create(ZkMsmTable bn254_table, ZkMsmTable bls12_381_t
     // has to map new physical memory (gigabytes for a large batch of many
     // medium MSMs) held up the other workers' batches for a few hundred
     // milliseconds.  Memory reserved once and kept by the pool is handed out
-    // without mapping.
+    // without mapping.  A worker's workspace for a full batch of small and
+    // medium MSMs over window-shift tables (one sorted entry per window per
+    // point, two entry arrays, scalars) reaches about 480 B per batch point.
     {
         size_t fr = 0, tot = 0;
         cudaMemPool_t pool;
         if (cudaMemGetInfo(&fr, &tot) == cudaSuccess && cudaDeviceGetDefaultMemPool(&pool, s->device) == cudaSuccess) {
             const uint64_t want =
-                    std::min<uint64_t>((uint64_t)workers * s->max_batch_points * 384 + (1ull << 30), fr / 4);
+                    std::min<uint64_t>((uint64_t)workers * s->max_batch_points * 512 + (1ull << 30), fr / 4);
             uint64_t thr = 0;
             cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
             if (thr < want) {
