@@ -55,14 +55,17 @@ def test_batch_graph_replay_and_launch_count(eng, tables):
     counts = [4096, 100, 1 << 15, 1, 777]
     sc = scalars_host(e, "bn254", 310, sum(counts), "witness")
     L = zl.lib()
-    r1 = table.batch_commit(sc, counts, fmt=zl.SCALAR_MONT)
+    r1 = table.batch_commit(sc, counts, fmt=zl.SCALAR_MONT)  # launches issued directly
     l0 = L.zkmsm_engine_launch_count(e.handle)
-    r2 = table.batch_commit(sc, counts, fmt=zl.SCALAR_MONT)  # replayed graph
-    assert L.zkmsm_engine_launch_count(e.handle) > l0
+    r2 = table.batch_commit(sc, counts, fmt=zl.SCALAR_MONT)  # captured into a graph
+    l1 = L.zkmsm_engine_launch_count(e.handle)
+    r3 = table.batch_commit(sc, counts, fmt=zl.SCALAR_MONT)  # replayed graph
+    l2 = L.zkmsm_engine_launch_count(e.handle)
+    assert l1 > l0 and l2 - l1 == l1 - l0
     off = 0
     for i, c in enumerate(counts):
         a = r1[i].x + r1[i].y + r1[i].z
-        assert a == r2[i].x + r2[i].y + r2[i].z
+        assert a == r2[i].x + r2[i].y + r2[i].z == r3[i].x + r3[i].y + r3[i].z
         assert a == plain(e, "bn254", pts, sc[off * 32:], c)
         off += c
 

@@ -347,3 +347,28 @@ def test_2_24_split_linearity(eng, oracles, dist):
     b = jac_to_affine_bytes(C, msm_device(e, "bn254", p[h * 64:], s[h * 32:], zl.SCALAR_MONT, h))
     assert full == cm.affine_add("bn254", a, b)
     assert C.on_curve(C.dec_affine(full))
+
+
+def test_small_dropin_graph_sequence():
+    """Drop-in calls of up to 2^16 points run their launches directly on the
+    first call of a size, capture a CUDA graph on the second and replay it
+    after that.  Every call must equal the device-pointer MSM of the same
+    inputs: with new scalars between replays, other sizes interleaved, and a
+    larger call that regrows the workspace and drops the captured graphs."""
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    e = MetalMSM()  # fresh engine: no plans or graphs yet
+    try:
+        N = 1 << 13
+        p, s1 = gen_inputs(e, "bn254", 501, N, "uniform", zl.SCALAR_MONT)
+        _, s2 = gen_inputs(e, "bn254", 502, N, "witness", zl.SCALAR_MONT)
+        ph = to_host(p)
+        sh = {1: to_host(s1), 2: to_host(s2)}
+        sd = {1: s1, 2: s2}
+        seq = [(1000, 1), (1000, 1), (1000, 2), (1000, 1), (777, 2), (1000, 2), (N, 1), (1000, 1), (1000, 2),
+               (1000, 1), (777, 1), (777, 2)]
+        for n, k in seq:
+            r = e.msmFr(ph[:n * 64], sh[k][:n * 32])
+            assert r.x + r.y + r.z == msm_device(e, "bn254", p, sd[k], zl.SCALAR_MONT, n), (n, k)
+    finally:
+        e.close()
