@@ -259,8 +259,10 @@ ZkMetalStatus zkmsm_engine_set_tuning(ZkMetalMSMEngine engine, int window_bits, 
  * 1.6x per stripe up to 2^stripe_log2): each stripe's host-to-device copy
  * overlaps the previous stripe's sort and accumulation, every stripe fills
  * its own bucket array in the window layout of the largest stripe, and the
- * arrays are added and reduced once (the same point).  -1 (default): automatic, largest stripe half of n's next power of
- * two, only for n >= 2^22; 0: off; 2..30: fixed. */
+ * arrays are added and reduced once (the same point).  -1 (default):
+ * automatic: largest stripe half of n's next power of two from 2^22 points,
+ * and 2^20 points for BN254 G1 calls of 2^21 <= n < 2^22; none below; 0:
+ * off; 2..30: fixed. */
 ZkMetalStatus zkmsm_engine_set_stripe(ZkMetalMSMEngine engine, int stripe_log2);
 
 /* Synthetic inputs on the device (seeded, counter based):
