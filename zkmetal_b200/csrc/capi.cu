@@ -212,23 +212,49 @@ static ZkMetalStatus msm_host(Engine& e, const uint8_t* points, const uint8_t* s
         memcpy(rz, out + 2 * fb, fb);
         return ZKMETAL_SUCCESS;
     }
-    h2d(e, e.w_points, points, (size_t)n * 2 * fb);
-    h2d(e, e.w_scalars, scalars, (size_t)n * 32);
-    Plan& pl = e.get_plan<C>({n}, {0}, fmt, scalar_bits);
-    bool glv = pl.descs[0].glv;
-    if (glv) {
-        e.w_phi.ensure((size_t)n * 2 * fb + 16);
-        e.make_phi<C>(e.w_points.as<uint32_t>(), n, e.w_phi.as<uint32_t>());
-    }
     uint8_t out[3 * 4 * MAX_COORD_WORDS];
-    const uint32_t* phi = glv ? e.w_phi.as<uint32_t>() : e.w_points.as<uint32_t>();
-    // small MSMs are a chain of ~30 short launches: replay them as one CUDA
-    // graph (captured on the second call of a shape; the buffers are the
-    // engine's own, so later calls of the same size replay it)
-    if (n <= SMALL_GRAPH_POINTS)
+    if (n <= SMALL_GRAPH_POINTS) {
+        // small MSMs are a chain of ~30 short launches: replay them as one
+        // CUDA graph (captured on the second call of a shape; the buffers
+        // are the engine's own, so later calls of the same size replay it)
+        h2d(e, e.w_points, points, (size_t)n * 2 * fb);
+        h2d(e, e.w_scalars, scalars, (size_t)n * 32);
+        Plan& pl = e.get_plan<C>({n}, {0}, fmt, scalar_bits);
+        const bool glv = pl.descs[0].glv;
+        if (glv) {
+            e.w_phi.ensure((size_t)n * 2 * fb + 16);
+            e.make_phi<C>(e.w_points.as<uint32_t>(), n, e.w_phi.as<uint32_t>());
+        }
+        const uint32_t* phi = glv ? e.w_phi.as<uint32_t>() : e.w_points.as<uint32_t>();
         e.run_device_graph<C>(pl, e.w_points.as<uint32_t>(), phi, e.w_scalars.as<uint32_t>(), out);
-    else
-        e.run_device<C>(pl, e.w_points.as<uint32_t>(), phi, e.w_scalars.as<uint32_t>(), out);
+    } else {
+        // the scalars go first on the engine stream and the bases on the
+        // copy stream: the scalar preparation and sort, which read only the
+        // scalars, run while the bases arrive
+        Plan& pl = e.get_plan<C>({n}, {0}, fmt, scalar_bits);
+        const bool glv = pl.descs[0].glv;
+        bool grew = e.w_points.ensure((size_t)n * 2 * fb + 16);
+        grew |= e.w_scalars.ensure((size_t)n * 32 + 16);
+        if (glv) grew |= e.w_phi.ensure((size_t)n * 2 * fb + 16);
+        if (grew) e.drop_graphs();
+        e.ensure_workspace<C>(pl);
+        e.ensure_copy_resources(2);
+        // buffers (re)allocated in the engine stream's order: the copy waits for that
+        ZK_CUDA(cudaEventRecord(e.copy_events[0], e.stream));
+        ZK_CUDA(cudaStreamWaitEvent(e.copy_stream, e.copy_events[0], 0));
+        ZK_CUDA(cudaMemcpyAsync(e.w_scalars.p, scalars, (size_t)n * 32, cudaMemcpyHostToDevice, e.stream));
+        ZK_CUDA(cudaMemcpyAsync(e.w_points.p, points, (size_t)n * 2 * fb, cudaMemcpyHostToDevice, e.copy_stream));
+        ZK_CUDA(cudaEventRecord(e.copy_events[1], e.copy_stream));
+        Engine::BasesWait bw;
+        bw.ready = e.copy_events[1];
+        bw.phi_n = glv ? n : 0;
+        bw.phi_out = glv ? e.w_phi.as<uint32_t>() : nullptr;
+        const uint32_t* phi = glv ? e.w_phi.as<uint32_t>() : e.w_points.as<uint32_t>();
+        e.enqueue<C>(pl, e.w_points.as<uint32_t>(), phi, e.w_scalars.as<uint32_t>(), e.w_results.as<uint32_t>(), 0,
+                     nullptr, &bw);
+        ZK_CUDA(cudaMemcpyAsync(out, e.w_results.p, 3 * P::N * 4, cudaMemcpyDeviceToHost, e.stream));
+        ZK_CUDA(cudaStreamSynchronize(e.stream));
+    }
     memcpy(rx, out, fb);
     memcpy(ry, out + fb, fb);
     memcpy(rz, out + 2 * fb, fb);

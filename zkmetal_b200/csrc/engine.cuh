@@ -706,9 +706,18 @@ class Engine {
     // result).  bucket_base (default: the engine's bucket array) receives the
     // bucket sums.
     static constexpr int ENQ_ACC_ONLY = 1;
+    // Bases still being copied on another stream when the pipeline is
+    // enqueued: the scalar preparation and sort (which read only scalars)
+    // run first, then the engine stream waits for `ready` and, when phi_out
+    // is set, writes the endomorphism image of the phi_n bases there.
+    struct BasesWait {
+        cudaEvent_t ready = nullptr;
+        uint64_t phi_n = 0;
+        uint32_t* phi_out = nullptr;
+    };
     template <class C>
     void enqueue(const Plan& pl, const uint32_t* d_bases, const uint32_t* d_phi, const uint32_t* d_scalars,
-                 uint32_t* d_results, int flags = 0, void* bucket_base = nullptr);
+                 uint32_t* d_results, int flags = 0, void* bucket_base = nullptr, const BasesWait* bw = nullptr);
     template <class C>
     void enqueue_reduce(const Plan& pl, const void* bucket_base, uint32_t* d_results,
                         std::vector<cudaEvent_t>* ev = nullptr);
@@ -801,7 +810,7 @@ class Engine {
 // (inst_bn254.cu, inst_bls381.cu, inst_bls377.cu, inst_bn254g2.cu) so the curves compile in parallel.
 #define ZKMSM_ENGINE_TEMPLATES(EXT, C)                                                                  \
     EXT template void Engine::enqueue<C>(const Plan&, const uint32_t*, const uint32_t*, const uint32_t*, \
-                                         uint32_t*, int, void*);                                        \
+                                         uint32_t*, int, void*, const BasesWait*);                      \
     EXT template void Engine::enqueue_reduce<C>(const Plan&, const void*, uint32_t*,                     \
                                                 std::vector<cudaEvent_t>*);                             \
     EXT template void Engine::fold_buckets<C>(void*, uint32_t, uint32_t);                               \

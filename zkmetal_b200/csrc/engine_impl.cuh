@@ -33,7 +33,7 @@ static void scan_u32(Engine& e, uint32_t* d_in_out, uint32_t n, uint32_t* d_tota
 // d_results.  No host synchronisation inside (graph capturable).
 template <class C>
 void Engine::enqueue(const Plan& pl, const uint32_t* d_bases, const uint32_t* d_phi, const uint32_t* d_scalars,
-             uint32_t* d_results, int flags, void* bucket_base) {
+             uint32_t* d_results, int flags, void* bucket_base, const BasesWait* bw) {
     using P = typename C::Fp;
     const int nd = (int)pl.descs.size();
     const MsmDesc* dd = pl.d_descs.as<MsmDesc>();
@@ -76,6 +76,10 @@ void Engine::enqueue(const Plan& pl, const uint32_t* d_bases, const uint32_t* d_
         launches++;
         ZK_CUDA(cudaGetLastError());
         std::swap(bufA, bufB);
+    }
+    if (bw) {  // nothing above reads the bases
+        ZK_CUDA(cudaStreamWaitEvent(stream, bw->ready, 0));
+        if (bw->phi_out) make_phi<C>(d_bases, bw->phi_n, bw->phi_out);
     }
     prof_mark(ev, 1);
     // segmented sums
