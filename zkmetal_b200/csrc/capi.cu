@@ -165,7 +165,9 @@ static void msm_host_striped(Engine& e, const uint8_t* points, const uint8_t* sc
     if (grew) e.drop_graphs();
     for (auto& kv : plans) e.ensure_workspace<C>(*kv.second);
     e.w_stripe_buckets.ensure(S * nb * xs + 16);
-    e.ensure_copy_resources(S + 1);
+    // events: [s] stripe s's scalars copied, [S] buffers allocated,
+    // [S + 1 + s] stripe s's bases copied
+    e.ensure_copy_resources(2 * S + 1);
     // buffers (re)allocated in the compute stream's order: the copies wait for that
     ZK_CUDA(cudaEventRecord(e.copy_events[S], e.stream));
     ZK_CUDA(cudaStreamWaitEvent(e.copy_stream, e.copy_events[S], 0));
@@ -178,15 +180,21 @@ static void msm_host_striped(Engine& e, const uint8_t* points, const uint8_t* sc
         const uint32_t cnt = rg[s].second;
         ZK_CUDA(cudaMemcpyAsync(ds + off * 32, scalars + off * 32, (size_t)cnt * 32, cudaMemcpyHostToDevice,
                                 e.copy_stream));
+        ZK_CUDA(cudaEventRecord(e.copy_events[s], e.copy_stream));
         ZK_CUDA(cudaMemcpyAsync(dp + off * pb, points + off * pb, (size_t)cnt * pb, cudaMemcpyHostToDevice,
                                 e.copy_stream));
-        ZK_CUDA(cudaEventRecord(e.copy_events[s], e.copy_stream));
+        ZK_CUDA(cudaEventRecord(e.copy_events[S + 1 + s], e.copy_stream));
+        // the stripe's sort needs only its scalars; its bases are waited
+        // for after the sort, before the endomorphism and the accumulation
         ZK_CUDA(cudaStreamWaitEvent(e.stream, e.copy_events[s], 0));
         const uint32_t* sp = reinterpret_cast<const uint32_t*>(dp + off * pb);
         uint32_t* sphi = reinterpret_cast<uint32_t*>(dphi + off * pb);
-        if (glv) e.make_phi<C>(sp, cnt, sphi);
+        Engine::BasesWait bw;
+        bw.ready = e.copy_events[S + 1 + s];
+        bw.phi_n = glv ? cnt : 0;
+        bw.phi_out = glv ? sphi : nullptr;
         e.enqueue<C>(*plans[cnt], sp, sphi, reinterpret_cast<const uint32_t*>(ds + off * 32), nullptr,
-                     Engine::ENQ_ACC_ONLY, bk + s * nb * xs);
+                     Engine::ENQ_ACC_ONLY, bk + s * nb * xs, &bw);
     }
     e.fold_buckets<C>(bk, (uint32_t)nb, S);
     e.enqueue_reduce<C>(p0, bk, e.w_results.as<uint32_t>());
