@@ -372,3 +372,26 @@ def test_small_dropin_graph_sequence():
             assert r.x + r.y + r.z == msm_device(e, "bn254", p, sd[k], zl.SCALAR_MONT, n), (n, k)
     finally:
         e.close()
+
+
+@pytest.mark.parametrize("curve,n", [("bn254", (1 << 17) + 5), ("bn254", 1 << 20), ("bn254", 1 << 21),
+                                     ("bls12_381", 1 << 20)])
+def test_dropin_pinned_buffers_overlap(eng, curve, n):
+    """Drop-in calls from pinned host buffers, where the copies really run
+    under the computation: above 2^16 points the bases arrive on a second
+    stream while the scalars are sorted, and from 2^21 BN254 points each
+    stripe's sort waits only for its scalars.  Each call must equal the
+    device-pointer MSM of the same inputs, also when the host buffers are
+    refilled between calls."""
+    e = eng[curve]
+    C = R.CURVES[curve]
+    fn = {"bn254": zl.lib().zkmetal_bn254_msm_fr, "bls12_381": zl.lib().zkmetal_bls12_381_g1_msm_fr}[curve]
+    rx, ry, rz = (ctypes.create_string_buffer(C.fp_bytes) for _ in range(3))
+    ph = torch.empty(n * 2 * C.fp_bytes, dtype=torch.uint8).pin_memory()
+    sh = torch.empty(n * 32, dtype=torch.uint8).pin_memory()
+    for seed in (701, 702, 703):
+        p, s = gen_inputs(e, curve, seed, n, "uniform" if seed != 702 else "witness", zl.SCALAR_MONT)
+        ph.copy_(p.cpu())
+        sh.copy_(s.cpu())
+        check(fn(e.handle, ph.data_ptr(), sh.data_ptr(), n, rx, ry, rz))
+        assert rx.raw + ry.raw + rz.raw == msm_device(e, curve, p, s, zl.SCALAR_MONT, n), seed
