@@ -48,19 +48,25 @@ void Engine::enqueue(const Plan& pl, const uint32_t* d_bases, const uint32_t* d_
     ZK_CUDA(cudaMemsetAsync(tot, 0, 4, stream));
     uint2* bufA = (pl.sort_passes & 1) ? w_ents2.as<uint2>() : w_ents.as<uint2>();
     uint2* bufB = (pl.sort_passes & 1) ? w_ents.as<uint2>() : w_ents2.as<uint2>();
+    // the first pass's tile histogram is counted by the digit kernel
+    if (pl.sort_passes)
+        ZK_CUDA(cudaMemsetAsync(w_thist.p, 0, (size_t)(1u << pl.sort_bits) * pl.sort_tiles * 4, stream));
     if (pl.total_scalars) {
         const uint64_t g = (pl.total_scalars + pl.sort_spb - 1) / pl.sort_spb;
-        k_radix_digits<C><<<(unsigned)g, SORT_DTHREADS, 0, stream>>>(d_scalars, dd, nd, pl.total_scalars,
-                                                                    pl.sort_spb, bufA, tot + 0);
+        k_radix_digits<C><<<(unsigned)g, SORT_DTHREADS, 0, stream>>>(
+                d_scalars, dd, nd, pl.total_scalars, pl.sort_spb, bufA, tot + 0,
+                pl.sort_passes ? w_thist.as<uint32_t>() : nullptr, pl.sort_bits, pl.sort_tiles);
         launches++;
         ZK_CUDA(cudaGetLastError());
     }
     for (uint32_t ps = 0; ps < pl.sort_passes; ps++) {
         const uint32_t shift = ps * pl.sort_bits, nt = pl.sort_tiles;
-        k_radix_hist<<<nt, SORT_ETHREADS, 0, stream>>>(bufA, tot + 0, shift, pl.sort_bits, nt,
-                                                        w_thist.as<uint32_t>());
-        launches++;
-        ZK_CUDA(cudaGetLastError());
+        if (ps > 0) {
+            k_radix_hist<<<nt, SORT_ETHREADS, 0, stream>>>(bufA, tot + 0, shift, pl.sort_bits, nt,
+                                                            w_thist.as<uint32_t>());
+            launches++;
+            ZK_CUDA(cudaGetLastError());
+        }
         scan_u32(*this, w_thist.as<uint32_t>(), (1u << pl.sort_bits) * nt, tot + 63, nullptr);
         switch (pl.sort_bits) {
 #define ZK_SCATTER(B)                                                                                     \

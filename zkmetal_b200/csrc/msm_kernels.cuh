@@ -360,12 +360,19 @@ ZK_DEV void warp_count(uint32_t* __restrict__ ctr, bool valid, uint32_t key) {
     else if (valid && !grp) atomicAdd(ctr + key, 1u);
 }
 
+// hist0 (optional, zeroed before the launch): the first radix pass's
+// digit-major per-tile counts of the low h0bits bits of the bucket ids, for
+// tiles of SORT_ETILE entries of A ([digit][tile], ntiles tiles), added here
+// so that the first pass needs no histogram kernel.
+static_assert(SORT_DBUF <= SORT_ETILE, "a digit block's range spans at most two sort tiles");
 template <class C>
 __global__ void __launch_bounds__(SORT_DTHREADS) k_radix_digits(const uint32_t* __restrict__ scalars,
                                                                 const MsmDesc* __restrict__ descs, int nd,
                                                                 uint64_t total, uint32_t scalars_per_block,
                                                                 uint2* __restrict__ A,
-                                                                uint32_t* __restrict__ d_count) {
+                                                                uint32_t* __restrict__ d_count,
+                                                                uint32_t* __restrict__ hist0, uint32_t h0bits,
+                                                                uint32_t ntiles) {
     __shared__ uint2 buf[SORT_DBUF];
     __shared__ uint32_t cur, base_s;
     const uint32_t tid = threadIdx.x, lane = tid & 31;
@@ -416,6 +423,28 @@ __global__ void __launch_bounds__(SORT_DTHREADS) k_radix_digits(const uint32_t* 
     __syncthreads();
     const uint32_t base = base_s;
     for (uint32_t i = tid; i < cnt; i += SORT_DTHREADS) A[(size_t)base + i] = buf[i];
+    if (hist0) {
+        // counts of the range [base, base + cnt) per tile (the tile of base,
+        // and the next one from entry `split` on) and digit, then one
+        // global add per non-zero count
+        __shared__ uint32_t hc[2 * SORT_MAX_BINS];
+        for (uint32_t i = tid; i < 2 * SORT_MAX_BINS; i += SORT_DTHREADS) hc[i] = 0;
+        __syncthreads();
+        const uint32_t mask = (1u << h0bits) - 1;
+        const uint32_t split = SORT_ETILE - base % SORT_ETILE;
+        for (uint32_t i0 = 0; i0 < cnt; i0 += SORT_DTHREADS) {
+            const uint32_t i = i0 + tid;
+            const bool v = i < cnt;
+            const uint32_t key = v ? (i < split ? 0u : SORT_MAX_BINS) + (buf[i].x & mask) : 0u;
+            warp_count(hc, v, key);
+        }
+        __syncthreads();
+        const uint32_t t0 = base / SORT_ETILE;
+        for (uint32_t i = tid; i < 2 * SORT_MAX_BINS; i += SORT_DTHREADS) {
+            const uint32_t c = hc[i];
+            if (c) atomicAdd(hist0 + (size_t)(i % SORT_MAX_BINS) * ntiles + t0 + i / SORT_MAX_BINS, c);
+        }
+    }
 }
 
 // Per-warp digit counts of the warp's SORT_ETILE / SORT_WARPS entries of a
