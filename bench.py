@@ -91,126 +91,240 @@ class ClockSampler:
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
 
 
-# --------------------------------------------------------------- CPU (reference) timing
-def executed_products(n, curve_id=0, window=0):
-    """Word products k_acc_l1 executes for one plain n-point MSM: one mixed
-    XYZZ addition (8M + 2S) per sorted entry, 2L^2 + L products per field
-    multiply; the entry count is the planner's bound (every digit nonzero)."""
+# --------------------------------------------------------------- roofline arithmetic
+PRODUCTS_PER_MUL = {"bn254": 2 * 8 * 8 + 8, "bls12_381": 2 * 12 * 12 + 12}  # CIOS on 32-bit limbs: 2L^2 + L
+MADD_MULS, ADD_MULS, DBL_MULS = 10, 14, 9  # XYZZ madd-2008-s, add-2008-s, dbl-2008-s-1 (products incl. squares)
+
+
+def measured_hbm_gbs():
+    """(GB/s, source) of the copy bandwidth the HBM fractions are quoted against."""
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured (MEASURED_PEAKS.json hbm_gbs)"
+    except Exception:
+        return 6650.0, "fallback (6.65 TB/s, an earlier measurement on this pool)"
+
+
+def plan_of(n, window=0, curve=0):
     from zkmetal_b200 import lib as zl
-    buf = ctypes.create_string_buffer(1 << 20)
+    buf = ctypes.create_string_buffer(1 << 22)
     cnt = (ctypes.c_uint32 * 1)(n)
-    st = zl.lib().zkmsm_plan_describe(curve_id, cnt, 1, 1, window, 0, -1, 0, buf, len(buf))
-    if st != 0:
+    if zl.lib().zkmsm_plan_describe(curve, cnt, 1, 1, window, 0, -1, 0, buf, len(buf)) != 0:
         return None
-    limbs = 8 if curve_id == 0 else 12
-    return json.loads(buf.value.decode())["entry_bound"] * 10 * (2 * limbs * limbs + limbs)
+    return json.loads(buf.value.decode())
 
 
-def reference_cpu_msm_ms(n_sample, points_b, scalars_mont_b, repeats=1, scalars_are_int=False):
-    """Time the reference C Pippenger on host cores; returns (ms per run, threads, kind)."""
-    from oracle import lib as olib
+def reduction_products(plan, curve="bn254"):
+    """Word products k_reduce_level executes over the plan's reduction tree: a
+    node of cnt children does 2(cnt - 1) + 1 XYZZ additions, cnt more above
+    level 0 (the weighted sums), and level * log2(L) doublings."""
+    L, lg = plan["red_L"], plan["red_log2L"]
+    adds = dbls = 0
+    for lvl, tasks in enumerate(plan["red"]):
+        for (_, n_in, _, _) in tasks:
+            for cnt, k in ((L, n_in // L), (n_in % L, 1 if n_in % L else 0)):
+                adds += (2 * (cnt - 1) + 1 + (cnt if lvl else 0)) * k
+                dbls += lvl * lg * k
+    return (adds * ADD_MULS + dbls * DBL_MULS) * PRODUCTS_PER_MUL[curve]
+
+
+def sort_bytes(n, entries, plan):
+    """DRAM bytes the scalar preparation and radix sort move by design: the
+    scalars once, the entries written by the digit kernel, read and written by
+    every scatter pass, read by every histogram pass after the first (8 B per
+    entry), and the per-tile histograms through their scans."""
+    passes, bits, tiles = plan["sort"][2], plan["sort"][3], plan["sort"][4]
+    hist = (1 << bits) * tiles * 4
+    return 32 * n + 8 * entries + passes * 16 * entries + max(0, passes - 1) * 8 * entries + passes * 3 * hist
+
+
+def roofline_report(n, ms, phases, entries, peak_g, window, clk):
+    """The dominant kernel's roofline in the unit it executes (word products
+    of the mixed additions it runs), the canonical-work figure beside it, and
+    per-phase fractions: prep + sort against HBM, the bucket reduction
+    against the product peak."""
+    plan = plan_of(n, window)
+    if not entries:
+        entries = plan["entry_bound"] if plan else 0
+    ppm = PRODUCTS_PER_MUL["bn254"]
+    acc_ms, red_ms, sort_ms = phases[1], phases[3], phases[0]
+    executed = entries * MADD_MULS * ppm
+    achieved = executed / (acc_ms * 1e-3) / 1e9 if acc_ms > 0 else None
+    canon = CANON_PRODUCTS_PER_POINT["bn254"] * n
+    hbm, hbm_src = measured_hbm_gbs()
+    out = {"bound": "int-mul", "kernel": "k_acc_l1 (bucket accumulation)", "unit": "G word-products/s",
+           "achieved": round(achieved, 1) if achieved else None, "peak": round(peak_g, 1),
+           "frac": round(achieved / peak_g, 4) if achieved else None,
+           "work": "executed: %d sorted entries x %d products per XYZZ mixed addition (8M + 2S, %d-product "
+                   "Montgomery multiplies)" % (entries, MADD_MULS * ppm, ppm),
+           "canonical_frac": round(canon / (acc_ms * 1e-3) / 1e9 / peak_g, 4) if acc_ms > 0 else None,
+           "canonical_unit": "23,936 products per point (16 Jacobian mixed additions of 11 multiplies) x n, "
+                             "over the k_acc_l1 time: above 1 because the kernel does less than the canonical work",
+           "msm_canonical_frac": round(canon / (ms * 1e-3) / 1e9 / peak_g, 4),
+           "traffic": None}
+    prof_json = os.path.join(ROOT, "profiles", "acc_l1_bn254_traffic.json")
+    if os.path.exists(prof_json):
+        try:
+            with open(prof_json) as f:
+                out["traffic"] = json.load(f).get("dram_bytes_per_launch_at_2p24")
+        except Exception:
+            pass
+    phase = {}
+    if plan and sort_ms > 0:
+        sb = sort_bytes(n, entries, plan)
+        phase["prep_sort"] = {"bound": "hbm", "bytes": sb, "achieved_gbs": round(sb / (sort_ms * 1e-3) / 1e9, 1),
+                              "peak_gbs": hbm, "frac": round(sb / (sort_ms * 1e-3) / 1e9 / hbm, 4),
+                              "peak_source": hbm_src}
+    if plan and red_ms > 0:
+        rp = reduction_products(plan)
+        phase["bucket_reduce"] = {"bound": "int-mul", "products": rp,
+                                  "achieved": round(rp / (red_ms * 1e-3) / 1e9, 1), "peak": round(peak_g, 1),
+                                  "frac": round(rp / (red_ms * 1e-3) / 1e9 / peak_g, 4),
+                                  "buckets": plan["nbuckets"]}
+    out["phases"] = phase
+    if clk and clk.get("sm_mhz") and clk.get("sm_max_mhz"):
+        out["clock_normalised"] = {"sm_mhz_median": clk["sm_mhz"],
+                                   "sm_cycles_per_msm": round(ms * 1e-3 * clk["sm_mhz"] * 1e6),
+                                   "ms_at_max_clock": round(ms * clk["sm_mhz"] / clk["sm_max_mhz"], 3)}
+    return out
+
+
+# --------------------------------------------------------------- CPU (reference) timing
+# Host threads the reference C Pippenger can use: one task per window
+# (bn254_msm.c:1145-1187 dispatches num_windows = ceil(256 / wb) workers; wb
+# = 16 above 2^19 points), so at most 16 of the host's threads work at once.
+def ref_threads(n):
+    from oracle.pyref import _ref_window_bits
+    windows = (256 + _ref_window_bits(n) - 1) // _ref_window_bits(n)
+    return min(int(os.environ.get("OMP_NUM_THREADS", "1")), windows)
+
+
+def cpu_model():
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def bench_config(n, world, dist):
+    """The workload description both arms print (identical inputs: the
+    seeded generator gives the same bytes on the device and on the host)."""
+    return {"workload": "bn254_g1_msm", "n": n * world, "n_per_gpu": n, "dist": dist,
+            "scalars": "Fr uniform in [0, r)" if dist == "uniform" else
+            "witness-like: 40% 0, 20% 1, 25% below 2^32, 15% uniform in Fr",
+            "bases": "P_i = k_i*G, k_i uniform in [1,r), all distinct",
+            "parallelism": "point-range shards + all-gather of %d partial points" % world,
+            "l2": "inputs larger than L2 (%.2f GB per step per GPU)" % (n * 96 / 1e9)}
+
+
+def _oracles():
+    """(reference C Pippenger or None, C restatement), building them if needed."""
     from oracle import build as obuild
+    from oracle import lib as olib
     obuild.build_cmsm()
     if not os.path.exists(olib.REF_LIB):
         try:
             obuild.build_all()
         except Exception:
             pass
-    kind = "reference" if os.path.exists(olib.REF_LIB) else "port"
-    orc = olib.RefOracle() if kind == "reference" else olib.COracle()
-    sc_int = scalars_mont_b if scalars_are_int else \
-        orc.fr_from_mont("bn254", scalars_mont_b, n_sample)  # conversion timed separately (not here)
-    times = []
-    for _ in range(repeats):
-        t0 = time.perf_counter()
-        orc.msm_jacobian("bn254", points_b, sc_int, n_sample) if kind == "reference" else \
-            orc.msm("bn254", points_b, sc_int, n_sample)
-        times.append((time.perf_counter() - t0) * 1e3)
-    from oracle.pyref import _ref_window_bits
-    wb = _ref_window_bits(n_sample)
-    windows = (256 + wb - 1) // wb  # the reference runs one OpenMP task per window
-    threads = min(int(os.environ.get("OMP_NUM_THREADS", "1")), windows)
-    return statistics.median(times), threads, kind
+    ref = olib.RefOracle() if os.path.exists(olib.REF_LIB) else None
+    return ref, olib.COracle()
 
 
-def host_inputs(n, seed, index0=0):
-    """Synthetic inputs in host memory (bases from the device generator when a
-    GPU is present; they are plain input data for the CPU run)."""
-    import torch
-    from zkmetal_b200 import MetalMSM
-    from zkmetal_b200 import lib as zl
-    e = MetalMSM()
-    p = torch.empty(n * 64, dtype=torch.uint8, device="cuda")
-    s = torch.empty(n * 32, dtype=torch.uint8, device="cuda")
-    torch.cuda.synchronize()
-    assert zl.lib().zkmsm_gen_bases(e.handle, 0, seed, index0, n, p.data_ptr()) == 0
-    assert zl.lib().zkmsm_gen_scalars(e.handle, 0, seed, index0, n, 0, 1, s.data_ptr()) == 0
-    torch.cuda.synchronize()
-    pb, sb = p.cpu().numpy().tobytes(), s.cpu().numpy().tobytes()
-    e.close()
-    return pb, sb
+INPUT_CACHE = os.environ.get("ZKMSM_INPUT_CACHE", "/tmp/zkmsm_inputs")
 
 
-def host_inputs_cpu(n, seed, distinct_log2=16):
-    """Inputs for the reference arm made on the host alone (no GPU, none of
-    this library): 2^distinct_log2 distinct bases k_i*G from the C
-    restatement, repeated to n points (the Pippenger's cost does not depend on
-    bases repeating), and n integer scalars uniform in [0, r)."""
+def reference_inputs(n, seed, dist, spot_checks=4096):
+    """Inputs of the reference arm, made on the host alone (no GPU, none of
+    this library): n distinct bases k_i*G from the oracle's 16-bit comb and n
+    integer scalars, both from the seeded generator, so they are the same
+    bytes the library's device generator gives the GPU arm for this seed.
+    The bases are cached on disk with their SHA-256 (checked on reuse), and
+    `spot_checks` random indices are recomputed with the reference's own
+    scalar multiplication (bn254_point_scalar_mul) before use."""
+    import hashlib
     import numpy as np
-    from oracle import build as obuild
-    from oracle import lib as olib
     from oracle import pyref as R
-    obuild.build_cmsm()
+    ref, cm = _oracles()
     C = R.BN254
-    rng = np.random.default_rng(seed)
+    os.makedirs(INPUT_CACHE, exist_ok=True)
+    path = os.path.join(INPUT_CACHE, "bn254-bases-%x-%d.bin" % (seed, n))
+    t0 = time.perf_counter()
+    pb = None
+    if os.path.exists(path) and os.path.exists(path + ".sha256"):
+        data = np.fromfile(path, dtype=np.uint8)
+        with open(path + ".sha256") as f:
+            if data.size == n * 64 and hashlib.sha256(data).hexdigest() == f.read().strip():
+                pb = data
+    if pb is None:
+        pb = cm.gen_bases("bn254", C.enc_affine((C.gx, C.gy)), seed, n)
+        pb.tofile(path + ".tmp")
+        with open(path + ".sha256", "w") as f:
+            f.write(hashlib.sha256(pb).hexdigest())
+        os.replace(path + ".tmp", path)
+    gen_s = time.perf_counter() - t0
+    sb = cm.gen_scalars("bn254", seed, n, dist, fmt=0)
+    rng = np.random.default_rng(seed ^ 0xC0FFEE)
+    G = C.enc_affine((C.gx, C.gy))
+    for i in rng.integers(0, n, size=min(spot_checks, n)):
+        k = R.base_scalar(C, seed, int(i))
+        want = ref.point_scalar_mul("bn254", G, k) if ref else C.enc_affine(R.scalar_mul(C, (C.gx, C.gy), k))
+        assert pb[int(i) * 64:(int(i) + 1) * 64].tobytes() == want, "base %d differs from k_i*G" % i
+    return pb, sb, gen_s
 
-    def uniform_fr(m):
-        out = np.empty((m, 8), dtype=np.uint32)
-        filled = 0
-        while filled < m:
-            w = rng.integers(0, 1 << 32, size=(m - filled, 8), dtype=np.uint64).astype(np.uint32)
-            w[:, 7] &= (1 << (C.r.bit_length() - 224)) - 1
-            r_top = C.r >> 224
-            keep = w[:, 7] < r_top  # rows with the top limb of r need the full comparison
-            for i in np.nonzero(w[:, 7] == r_top)[0]:
-                keep[i] = int.from_bytes(w[i].tobytes(), "little") < C.r
-            k = int(keep.sum())
-            out[filled:filled + k] = w[keep]
-            filled += k
-        return out
 
-    d = min(n, 1 << distinct_log2)
-    ks = uniform_fr(d)
-    ks[ks.sum(axis=1) == 0, 0] = 1  # k_i >= 1
-    bases = np.frombuffer(olib.COracle().fixed_base_mul("bn254", C.enc_affine((C.gx, C.gy)), ks.tobytes(), d),
-                          dtype=np.uint8).reshape(d, 64)
-    pb = np.tile(bases, (-(-n // d), 1))[:n].tobytes()
-    sb = uniform_fr(n).tobytes()
-    return pb, sb
+def reference_msm_ms(orc, kind, n, pb, sb_int, runs):
+    """Wall times (ms) of `runs` calls of the reference C Pippenger on n points
+    (integer scalars), on the host's threads."""
+    times = []
+    for _ in range(runs):
+        t0 = time.perf_counter()
+        if kind == "reference":
+            orc.msm_jacobian("bn254", pb, sb_int, n)
+        else:
+            orc.msm("bn254", pb, sb_int, n)
+        times.append((time.perf_counter() - t0) * 1e3)
+    return times
 
 
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
-    n_full = 1 << args.log2n
-    n_sample = min(n_full, 1 << args.cpu_log2n)
-    pb, sb = host_inputs_cpu(n_sample, args.seed)
-    scale = n_full / n_sample
-    ms_all = []
-    for i in range(args.warmup + args.steps):
-        ms, threads, kind = reference_cpu_msm_ms(n_sample, pb, sb, scalars_are_int=True)
-        if i >= args.warmup:
-            ms_all.append(ms * scale)
-    v = statistics.mean(ms_all)
-    sample = "one %d-point BN254 MSM per step (reference C Pippenger, %d OpenMP threads), time x%g to 2^%d" % (
-        n_sample, threads, scale, args.log2n)
+    n = 1 << args.log2n
+    ref, cm = _oracles()
+    kind = "reference" if ref is not None else "port"
+    orc = ref if ref is not None else cm
+    pb, sb, gen_s = reference_inputs(n, args.seed, args.dist)
+    log("reference arm: %d bases ready in %.1f s (%s, %d host threads)" % (n, gen_s, cpu_model(), os.cpu_count()))
+    times = reference_msm_ms(orc, kind, n, pb, sb, args.warmup + args.steps)[args.warmup:]
+    v = statistics.mean(times)
+    # the Montgomery -> integer conversion of the scalars, timed on its own
+    # (bn254_fr_batch_to_limbs, bn254_msm.c:1537-1552): the GPU arm takes
+    # Montgomery scalars and converts them on the device
+    conv_ms = None
+    if ref is not None:
+        sm = cm.gen_scalars("bn254", args.seed, n, args.dist, fmt=1)
+        t0 = time.perf_counter()
+        conv = ref.fr_from_mont("bn254", sm, n)
+        conv_ms = (time.perf_counter() - t0) * 1e3
+        assert conv == sb.tobytes()
+    threads = ref_threads(n)
+    sample = ("the whole %d-point BN254 MSM every step (reference C Pippenger bn254_pippenger_msm, one "
+              "OpenMP task per window: %d threads busy of %d on %s); integer scalars; Montgomery -> integer "
+              "conversion timed separately" % (n, threads, os.cpu_count(), cpu_model()))
     line = {"metric": METRIC, "value": round(v, 3), "unit": "ms", "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(v, 3), "higher_is_better": False, "scaling": "weak",
             "vs_baseline": None, "dtype": "u64", "data": "synthetic", "impl": "reference",
-            "config": {"workload": "bn254_g1_msm", "n": n_full, "scalars": "uniform Fr (integer form)",
-                       "bases": "k_i*G, k_i uniform in [1,r): 2^16 distinct bases repeated (made on the host)"},
-            "cpu_baseline": {"value": round(v, 3), "unit": "ms", "cores": threads, "kind": kind, "sample": sample},
+            "config": bench_config(n, 1, args.dist),
+            "cpu_baseline": {"value": round(v, 3), "unit": "ms", "cores": threads, "kind": kind, "sample": sample,
+                             "host_threads": os.cpu_count(), "cpu": cpu_model(),
+                             "fr_to_int_ms": round(conv_ms, 1) if conv_ms is not None else None,
+                             "runs_ms": [round(t, 1) for t in times]},
             "e2e": {"value": round(v, 3), "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
@@ -358,48 +472,67 @@ def run_batch_config(seed=0x5EED0002, table_log2=22, n_msms=24, lo=12, hi=22):
         r = table.batch_commit(sc_h.numpy(), counts, fmt=zl.SCALAR_MONT)
         return [p.x + p.y + p.z for p in r]
 
-    def timed(fn, reps):
-        fn()  # warm-up (plans, graph capture)
-        best = 1e30
-        res = None
+    def batched_device():
+        r = table.batch_commit(sc.data_ptr(), counts, fmt=zl.SCALAR_MONT, on_device=True)
+        return [p.x + p.y + p.z for p in r]
+
+    def timed(fn, reps=5):
+        # two untimed calls (the first plans, the second captures the batch's
+        # CUDA graph), then the median of `reps` host wall times; every arm
+        # is timed this way
+        fn()
+        res = fn()
+        ts = []
         for _ in range(reps):
             t = time.perf_counter()
-            res = fn()
-            best = min(best, time.perf_counter() - t)
-        return best, res
+            r = fn()
+            ts.append(time.perf_counter() - t)
+            assert r == res
+        return statistics.median(ts), res
 
-    t_drop, r_drop = timed(plain_dropin, 2)
-    t_dev, r_dev = timed(plain_device, 2)
-    t_bat0, r_bat0 = timed(batched, 3)
+    t_drop, r_drop = timed(plain_dropin)
+    t_dev, r_dev = timed(plain_device)
+    t_bat0, r_bat0 = timed(batched)
+    t_batd0, r_batd0 = timed(batched_device)
     # fixed-base precomputation of the resident table (window shifts, spacing
     # SHIFT_SPACING bits): one-time setup, like the autotuner
     t0 = time.perf_counter()
     table.precompute(SHIFT_SPACING)
     shift_s = time.perf_counter() - t0
-    t_bat, r_bat = timed(batched, 3)
+    t_bat, r_bat = timed(batched)
+    t_batd, r_batd = timed(batched_device)
     table.close()
     e.close()
     return {"workload": "24 BN254 MSMs, sizes 2^U (U ~ uniform[12,22]), prefixes of a 2^22 resident table",
             "points": total, "msms": n_msms,
+            "timing": "median of 5 host wall times per arm, after two untimed calls",
             "plain_dropin_commits_per_s": round(n_msms / t_drop, 1),
             "plain_device_commits_per_s": round(n_msms / t_dev, 1),
             "batched_commits_per_s": round(n_msms / t_bat, 1),
+            "batched_device_commits_per_s": round(n_msms / t_batd, 1),
             "speedup_vs_plain_dropin": round(t_drop / t_bat, 2),
-            "speedup_vs_plain_device": round(t_dev / t_bat, 2),
-            "batched_ms": round(t_bat * 1e3, 2),
+            "speedup_vs_plain_device": round(t_dev / t_batd, 2),
+            "arms": "drop-in: host scalars and host bases on both sides (the batch over its resident table); "
+                    "device: scalars resident in HBM on both sides",
+            "batched_ms": round(t_bat * 1e3, 2), "batched_device_ms": round(t_batd * 1e3, 2),
             "batched_without_shift_table_ms": round(t_bat0 * 1e3, 2),
+            "batched_device_without_shift_table_ms": round(t_batd0 * 1e3, 2),
+            "plain_device_ms": round(t_dev * 1e3, 2), "plain_dropin_ms": round(t_drop * 1e3, 2),
             "shift_table": {"spacing_bits": SHIFT_SPACING, "precompute_s": round(shift_s, 3),
                             "bytes": shift_table_bytes(T, 32, 254)},
-            "bit_exact_vs_plain": r_bat == r_bat0 == r_dev == r_drop,
+            "bit_exact_vs_plain": r_bat == r_bat0 == r_batd == r_batd0 == r_dev == r_drop,
             "autotune_s": round(tune_s, 1),
             "autotune": json.loads(rep.value.decode())}
 
 
-def run_serve_config(duration_s=60.0, rate=200.0, seed=0x5EED0004, table_log2=22, plain_sample=120):
+def run_serve_config(duration_s=60.0, rate=200.0, seed=0x5EED0004, table_log2=22, capacity_k=600):
     """Poisson stream of commitment requests (70% BN254 / 30% BLS12-381, sizes
     log-uniform in [2^10, 2^22], scalars half uniform / half witness-like) to
-    the continuous-batching server; p50/p99 latency and commitments/s against
-    back-to-back plain calls of the same requests."""
+    the continuous-batching server: p50/p99 latency over the stream; capacity
+    with both sides saturated (the first `capacity_k` requests submitted at
+    once, against the same requests as back-to-back plain drop-in calls); and
+    every served result compared with a plain device call of its request
+    (which also times back-to-back plain device calls over the whole stream)."""
     import threading
     import numpy as np
     import torch
@@ -409,7 +542,7 @@ def run_serve_config(duration_s=60.0, rate=200.0, seed=0x5EED0004, table_log2=22
     T = 1 << table_log2
     engines = {0: MetalMSM(), 1: BLS12381MSM()}
     fb = {0: 32, 1: 48}
-    pts, pts_h, tables, pools = {}, {}, {}, {}
+    pts, pts_h, tables, pools, dpools = {}, {}, {}, {}, {}
     for c in (0, 1):
         pts[c] = _dev(torch, T * 2 * fb[c])
         torch.cuda.synchronize()
@@ -422,6 +555,8 @@ def run_serve_config(duration_s=60.0, rate=200.0, seed=0x5EED0004, table_log2=22
             assert L.zkmsm_gen_scalars(engines[c].handle, c, seed + 10 + 2 * c + dist, 0, 2 * T, dist, 1,
                                        s.data_ptr()) == 0
             pools[(c, dist)] = _pinned(torch, s).numpy()
+            dpools[(c, dist)] = s
+
     def poisson(rng, horizon_s):
         out, t = [], 0.0
         while True:
@@ -478,45 +613,64 @@ def run_serve_config(duration_s=60.0, rate=200.0, seed=0x5EED0004, table_log2=22
         worst = sorted(range(len(lats)), key=lambda i: -lats[i])[:25]
         for i in sorted(worst):
             log("slow request: arrival %.3f s curve %d n %d latency %.1f ms" % (reqs[i][0], reqs[i][1], reqs[i][2], lats[i]))
-    lats.sort()
-    # capacity: the same stream submitted at once (closed loop)
-    k_sat = min(len(reqs), 400)
+    lat_sorted = sorted(lats)
+    # capacity, both sides saturated, on the same first requests of the stream
+    k_sat = min(len(reqs), capacity_k)
     t0 = time.perf_counter()
     sat_ids = [srv.submit(c, pools[(c, dist)][off * 32:(off + n) * 32], zl.SCALAR_MONT)
                for (ta, c, n, dist, off) in reqs[:k_sat]]
+    sat = []
     for i in sat_ids:
-        srv.wait(i)
+        p, _ = srv.wait(i)
+        sat.append(p.x + p.y + p.z)
     t_sat = time.perf_counter() - t0
     srv.close()
-    # back-to-back plain drop-in calls on the first requests of the same stream
-    k = min(plain_sample, len(reqs))
     rx, ry, rz = (ctypes.create_string_buffer(48) for _ in range(3))
     fns = {0: L.zkmetal_bn254_msm_fr, 1: L.zkmetal_bls12_381_g1_msm_fr}
     plain = []
     for (ta, c, n, dist, off) in reqs[:2]:  # warm-up
         fns[c](engines[c].handle, pts_h[c].data_ptr(), pools[(c, dist)].ctypes.data + off * 32, n, rx, ry, rz)
     t0 = time.perf_counter()
-    for (ta, c, n, dist, off) in reqs[:k]:
+    for (ta, c, n, dist, off) in reqs[:k_sat]:
         assert fns[c](engines[c].handle, pts_h[c].data_ptr(), pools[(c, dist)].ctypes.data + off * 32, n,
                       rx, ry, rz) == 0
         plain.append(rx.raw[:fb[c]] + ry.raw[:fb[c]] + rz.raw[:fb[c]])
     t_plain = time.perf_counter() - t0
+    # every served result against a plain device call of the same request
+    out = ctypes.create_string_buffer(3 * 48)
+    mismatches = 0
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for i, (ta, c, n, dist, off) in enumerate(reqs):
+        assert L.zkmsm_msm_device(engines[c].handle, c, pts[c].data_ptr(), dpools[(c, dist)].data_ptr() + off * 32,
+                                  zl.SCALAR_MONT, n, out, None) == 0
+        mismatches += out.raw[:3 * fb[c]] != served[i]
+    t_plain_dev = time.perf_counter() - t0
     for tb in tables.values():
         tb.close()
+    for e in engines.values():
+        e.close()
+    cap = k_sat / t_sat
+    plain_rate = k_sat / t_plain
     return {"workload": "Poisson %.0f req/s for %.0f s, 70%% BN254 / 30%% BLS12-381, sizes 2^U (U ~ [10,22]), "
                         "scalars 50/50 uniform / witness-like, 2^22-point resident tables with window shifts "
                         "(spacing %d bits)" % (rate, duration_s, SHIFT_SPACING),
             "requests": len(reqs), "completed": st["completed"] - st0["completed"],
             "failed": st["failed"] - st0["failed"], "batches": st["batches"] - st0["batches"],
-            "max_batch": st["max_batch"], "p50_ms": round(lats[len(lats) // 2], 3),
-            "p99_ms": round(lats[min(len(lats) - 1, int(0.99 * len(lats)))], 3),
+            "max_batch": st["max_batch"], "p50_ms": round(lat_sorted[len(lat_sorted) // 2], 3),
+            "p99_ms": round(lat_sorted[min(len(lat_sorted) - 1, int(0.99 * len(lat_sorted)))], 3),
             "served_commits_per_s": round(len(reqs) / wall, 1),
-            "saturated_commits_per_s": round(k_sat / t_sat, 1),
-            "plain_dropin_commits_per_s": round(k / t_plain, 1),
-            "speedup_vs_plain_dropin": round((len(reqs) / wall) / (k / t_plain), 2),
-            "capacity_vs_plain_dropin": round((k_sat / t_sat) / (k / t_plain), 2),
+            "capacity_commits_per_s": round(cap, 1),
+            "plain_dropin_commits_per_s": round(plain_rate, 1),
+            "capacity_vs_plain_dropin": round(cap / plain_rate, 2),
+            "capacity_sample": "the first %d requests of the stream, submitted at once to the server and run as "
+                               "back-to-back plain drop-in calls (host bases and scalars)" % k_sat,
+            "plain_device_commits_per_s": round(len(reqs) / t_plain_dev, 1),
+            "capacity_vs_plain_device": round(cap / (len(reqs) / t_plain_dev), 2),
             "hbm_budget_gb": round(st["budget_bytes"] / 1e9, 1),
-            "bit_exact_vs_plain": served[:k] == plain}
+            "bit_exact_vs_plain": mismatches == 0 and sat == plain == served[:k_sat],
+            "compared": "all %d served results vs plain device calls; the %d capacity results vs plain drop-in "
+                        "calls" % (len(reqs), k_sat)}
 
 
 def run_bls_config(seed=0x5EED0003, log2n=22, n_batch=8, lo=14, hi=22):
@@ -745,21 +899,19 @@ def run_ours(args):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms = float(t.item())
 
-    # ---- end to end through the drop-in C ABI from pinned host buffers
-    e2e_ms = None
-    if not args.no_e2e:
-        hp = torch.empty(n * 64, dtype=torch.uint8, pin_memory=True)
-        hs = torch.empty(n * 32, dtype=torch.uint8, pin_memory=True)
-        hp.copy_(pts.cpu())
-        hs.copy_(sc.cpu())
+    entries = L.zkmsm_engine_last_entries(eng.handle)  # sorted entries of one step's MSM
+
+    # ---- end to end through the drop-in C ABI from host buffers: pinned
+    # (the headline e2e), and pageable (what a Swift [PointAffine] hands over)
+    def e2e_run(hp_ptr, hs_ptr, steps):
         rx, ry, rz = (ctypes.create_string_buffer(32) for _ in range(3))
         out_all = torch.empty(world * 96, dtype=torch.uint8)
         times = []
-        for i in range(args.warmup + args.e2e_steps):
+        for i in range(args.warmup + steps):
             if world > 1:
                 dist.barrier()
             t0 = time.perf_counter()
-            st = L.zkmetal_bn254_msm_fr(eng.handle, hp.data_ptr(), hs.data_ptr(), n, rx, ry, rz)
+            st = L.zkmetal_bn254_msm_fr(eng.handle, hp_ptr, hs_ptr, n, rx, ry, rz)
             assert st == 0, zl.last_error()
             if world > 1:
                 mine = torch.frombuffer(bytearray(rx.raw + ry.raw + rz.raw), dtype=torch.uint8).cuda()
@@ -769,11 +921,26 @@ def run_ours(args):
             dt = (time.perf_counter() - t0) * 1e3
             if i >= args.warmup:
                 times.append(dt)
-        e2e_ms = statistics.mean(times)
+        v = statistics.mean(times)
         if world > 1:
-            t = torch.tensor([e2e_ms], device="cuda")
+            t = torch.tensor([v], device="cuda")
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            e2e_ms = float(t.item())
+            v = float(t.item())
+        return v
+
+    e2e_ms = e2e_pageable_ms = None
+    host_pts = host_sc = None
+    if not args.no_e2e or (not args.no_cpu_baseline and world == 1):
+        host_pts = pts.cpu().numpy()
+        host_sc = sc.cpu().numpy()
+    if not args.no_e2e:
+        hp = torch.empty(n * 64, dtype=torch.uint8, pin_memory=True)
+        hs = torch.empty(n * 32, dtype=torch.uint8, pin_memory=True)
+        hp.numpy()[:] = host_pts
+        hs.numpy()[:] = host_sc
+        e2e_ms = e2e_run(hp.data_ptr(), hs.data_ptr(), args.e2e_steps)
+        del hp, hs
+        e2e_pageable_ms = e2e_run(host_pts.ctypes.data, host_sc.ctypes.data, args.e2e_steps)
 
     # ---- roofline of the dominant kernel (level-1 bucket accumulation)
     prod_s = ctypes.c_double()
@@ -784,19 +951,10 @@ def run_ours(args):
     # per product either way); the faster of the two is the denominator
     wide = L.zkmsm_wide_products_per_s()
     peak = max(prod_s.value, wide) / 1e9
-    acc_ms = phases[1]
-    executed = executed_products(n, 0, args.window)
-    achieved = CANON_PRODUCTS_PER_POINT["bn254"] * n / (acc_ms * 1e-3) / 1e9 if acc_ms > 0 else None
-    msm_achieved = CANON_PRODUCTS_PER_POINT["bn254"] * n / (ms * 1e-3) / 1e9
-    traffic = None
-    prof_json = os.path.join(ROOT, "profiles", "acc_l1_bn254_traffic.json")
-    if os.path.exists(prof_json):
-        try:
-            with open(prof_json) as f:
-                pj = json.load(f)
-            traffic = pj.get("dram_bytes_per_launch_at_2p24")
-        except Exception:
-            traffic = None
+    rl = roofline_report(n, ms, phases, entries, peak, args.window, clk)
+    rl["peak_source"] = ("measured live, all SMs (zkmsm_measure_peaks): lo/hi multiply-add pairs %.1f G/s, "
+                         "mad.wide.u32 %.1f G/s" % (prod_s.value / 1e9, wide / 1e9))
+    rl["bn254_fe_mul_per_s"] = round(bn_mul.value / 1e9, 2)
 
     if rank != 0:
         if world > 1:
@@ -807,39 +965,36 @@ def run_ours(args):
         "metric": METRIC, "value": round(ms, 3), "unit": "ms", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": False, "scaling": "weak",
         "vs_baseline": None, "dtype": "u32", "data": "synthetic",
-        "config": {"workload": "bn254_g1_msm", "n": n * world, "n_per_gpu": n, "dist": args.dist,
-                   "scalars": "Fr in Montgomery form", "bases": "k_i*G, k_i uniform in [1,r)",
-                   "parallelism": "point-range shards + all-gather of %d partial points" % world,
-                   "l2": "inputs larger than L2 (%.2f GB per step per GPU)" % (n * 96 / 1e9)},
+        "config": bench_config(n, world, args.dist),
         "points_per_s": round(n * world / (ms * 1e-3)),
         "phase_ms": {"prep_sort": round(phases[0], 3), "acc_level1": round(phases[1], 3),
                      "acc_levels2+": round(phases[2], 3), "bucket_reduce": round(phases[3], 3),
                      "window_combine": round(phases[4], 3)},
-        "roofline": {"bound": "int-mul", "achieved": round(achieved, 1) if achieved else None,
-                     "peak": round(peak, 1), "unit": "G word-products/s",
-                     "frac": round(achieved / peak, 4) if achieved else None, "traffic": traffic,
-                     "kernel": "k_acc_l1 (bucket accumulation)",
-                     "peak_source": "measured live, all SMs (zkmsm_measure_peaks): lo/hi multiply-add pairs "
-                                    "%.1f G/s, mad.wide.u32 %.1f G/s" % (prod_s.value / 1e9, wide / 1e9),
-                     "executed_frac": round(executed / (acc_ms * 1e-3) / 1e9 / peak, 4)
-                     if acc_ms > 0 and executed else None,
-                     "msm_achieved": round(msm_achieved, 1), "msm_frac": round(msm_achieved / peak, 4),
-                     "bn254_fe_mul_per_s": round(bn_mul.value / 1e9, 2)},
+        "roofline": rl,
         "e2e": {"value": round(e2e_ms, 3) if e2e_ms else None, "unit": "ms", "h2d_bytes_per_step": n * 96,
-                "d2h_bytes_per_step": 96},
+                "d2h_bytes_per_step": 96, "host_buffers": "pinned", "steps": args.e2e_steps,
+                "pageable_ms": round(e2e_pageable_ms, 3) if e2e_pageable_ms else None},
         "gpu_launches": int(launches),
         "clocks": clk,
     }
     if not args.no_cpu_baseline and world == 1:
-        n_sample = min(n, 1 << args.cpu_log2n)
-        pb = pts[:n_sample * 64].cpu().numpy().tobytes()
-        sb = sc[:n_sample * 32].cpu().numpy().tobytes()
-        cms, threads, kind = reference_cpu_msm_ms(n_sample, pb, sb)
-        scale = n / n_sample
+        import numpy as np
+        # the reference C Pippenger on the same inputs (the device generator's
+        # bytes), the whole 2^log2n MSM: one untimed run, then timed runs
+        ref, cm = _oracles()
+        kind = "reference" if ref is not None else "port"
+        orc = ref if ref is not None else cm
+        sb_int = (ref or cm).fr_from_mont("bn254", host_sc.tobytes(), n)
+        t_all = reference_msm_ms(orc, kind, n, host_pts, np.frombuffer(sb_int, dtype=np.uint8),
+                                 1 + args.cpu_runs)[1:]
+        threads = ref_threads(n)
         line["cpu_baseline"] = {
-            "value": round(cms * scale, 1), "unit": "ms", "cores": threads, "kind": kind,
-            "sample": "one %d-point BN254 MSM (first shard of the same inputs), reference C Pippenger, "
-                      "%d OpenMP threads, time x%g to 2^%d" % (n_sample, threads, scale, args.log2n)}
+            "value": round(statistics.mean(t_all), 1), "unit": "ms", "cores": threads, "kind": kind,
+            "sample": "the whole %d-point MSM of this run's inputs, %d timed run(s) after one untimed; reference C "
+                      "Pippenger, one OpenMP task per window (%d threads busy of %d on %s)" % (
+                          n, args.cpu_runs, threads, os.cpu_count(), cpu_model()),
+            "runs_ms": [round(t, 1) for t in t_all]}
+    del host_pts, host_sc
     if world == 1 and not args.no_extras:
         def release():
             # buffers of the previous configuration go back to the driver, so
@@ -880,7 +1035,7 @@ def run_ours(args):
             line["bn254_g2"] = {"error": repr(exc)}
         release()
         try:
-            line["serve"] = run_serve_config(duration_s=args.serve_seconds, plain_sample=40)
+            line["serve"] = run_serve_config(duration_s=args.serve_seconds)
         except Exception as exc:
             line["serve"] = {"error": repr(exc)}
     print(json.dumps(line), flush=True)
@@ -901,12 +1056,12 @@ def main():
     ap.add_argument("--seed", type=int, default=0x5EED0001)
     ap.add_argument("--window", type=int, default=0)
     ap.add_argument("--chunk", type=int, default=0)
-    ap.add_argument("--cpu-log2n", type=int, default=22)
-    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--cpu-runs", type=int, default=1, help="timed runs of the CPU baseline (after one untimed)")
+    ap.add_argument("--e2e-steps", type=int, default=10)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true", help="skip the batched and served summaries")
-    ap.add_argument("--serve-seconds", type=float, default=5.0, help="arrival window of the served summary")
+    ap.add_argument("--serve-seconds", type=float, default=60.0, help="arrival window of the served summary")
     ap.add_argument("--mode", choices=["plain", "batch", "serve"], default="plain",
                     help="batch / serve: print only that configuration's line (serve runs 60 s of arrivals)")
     args = ap.parse_args()

@@ -296,6 +296,12 @@ ZkMetalStatus zkmsm_plan_describe_shift(int curve, const uint32_t* counts, uint3
 /* Kernels launched so far by this engine (cumulative). */
 uint64_t zkmsm_engine_launch_count(ZkMetalMSMEngine engine);
 
+/* NEW (reporting helper, no counterpart in the reference): the number of
+ * sorted (bucket, point) entries of the engine's last MSM batch, i.e. the
+ * mixed additions its level-1 accumulation executed.  Waits for the whole
+ * device first (cudaDeviceSynchronize); 0 before the first batch. */
+uint64_t zkmsm_engine_last_entries(ZkMetalMSMEngine engine);
+
 /* Roofline denominators measured on device 0: 32x32->64-bit word products per
  * second (one low + one high multiply-add) with every SM occupied, and the
  * Montgomery multiplications per second of this library's BN254 and
@@ -329,10 +335,15 @@ ZkMetalStatus zkmsm_field_op(int curve, int op, const void* d_a, const void* d_b
  * 3 x 32 B (Jacobian, Z = 1 or the identity).  n_points <= 8192; larger ->
  * ZKMETAL_ERR_INVALID_INPUT.  Scratch is one static device array of about
  * 7.6 MB that every GPU loading the library holds until exit and that all
- * calls share: calls whose GPU work overlaps race, so serialise them.  The
- * first call on a device looks the array's address up (do it before any
- * stream capture).  Enqueues on `stream` (cudaStream_t; 0 = legacy default
- * stream) and returns without waiting. */
+ * calls share: calls whose GPU work overlaps race, so serialise them (calls
+ * queued one after another on one stream are already ordered).  The first
+ * call on a device looks the array's address up and caches it (make that
+ * first call before any stream capture); after a cudaDeviceReset of that
+ * device the cached address is stale, so do not call it again in that
+ * process.  A CUDA error left pending by earlier work is reported
+ * (ZKMETAL_ERR_GPU_ERROR) and left pending; nothing is enqueued then.
+ * Enqueues on `stream` (cudaStream_t; 0 = legacy default stream) and returns
+ * without waiting. */
 ZkMetalStatus zkmsm_bn254_msm_noalloc(const void* d_points, const void* d_scalars, int scalar_fmt,
                                       uint32_t n_points, void* d_result, void* stream);
 

@@ -31,7 +31,7 @@ def build_all(force=False):
     out = [build_cmsm(force)]
     sys.path.insert(0, HERE)
     import build_ref
-    ref = os.environ.get("ZKMSM_REFERENCE_ROOT", "/root/reference")
+    ref = build_ref.default_reference_root()
     if os.path.isdir(ref):
         out.append(build_ref.build(ref, force))
     elif os.path.exists(build_ref.LIB):

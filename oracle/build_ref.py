@@ -147,9 +147,20 @@ def build(ref_root, force=False, cc="gcc"):
     return LIB
 
 
+def default_reference_root():
+    """The reference checkout: $ZKMSM_REFERENCE_ROOT when set, else a
+    `reference` directory beside this repository's root."""
+    env = os.environ.get("ZKMSM_REFERENCE_ROOT")
+    if env:
+        return env
+    repo = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    return os.path.join(os.path.dirname(repo), "reference")
+
+
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default=os.environ.get("ZKMSM_REFERENCE_ROOT", "/root/reference"))
+    ap.add_argument("--ref", default=default_reference_root(),
+                    help="reference checkout (default: $ZKMSM_REFERENCE_ROOT, else ../reference beside this repository)")
     ap.add_argument("--force", action="store_true")
     a = ap.parse_args()
     if not os.path.isdir(a.ref):

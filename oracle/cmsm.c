@@ -180,3 +180,250 @@ void cm_affine_add(int curve, const uint64_t *a, const uint64_t *b, uint64_t *r)
         bl_to_affine(P, &R, (bl_aff *)r);
     }
 }
+
+/* ---------------------------------------------------------------- inputs
+ * The seeded counter-based generator of the synthetic inputs, restated for
+ * the host (the same words as the Python restatement's draw_word, so host
+ * and device inputs of one seed are the same bytes):
+ *   word = splitmix64(splitmix64(seed*FNV + stream*golden ^ (index*8 + w)) ^ attempt*C)
+ * uniform values below r by masked rejection (64 attempts, then 1). */
+static uint64_t sm64(uint64_t x) {
+    x += 0x9E3779B97F4A7C15ULL;
+    uint64_t z = x;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+    return z ^ (z >> 31);
+}
+
+static uint64_t draw_word(uint64_t seed, uint64_t stream, uint64_t index, uint64_t attempt, uint64_t w) {
+    uint64_t ctr = seed * 0x100000001B3ULL + stream * 0x9E3779B1ULL;
+    ctr = sm64(ctr ^ (index * 8 + w));
+    return sm64(ctr ^ (attempt * 0xD1B54A32D192ED03ULL));
+}
+
+static int lt4(const uint64_t *a, const uint64_t *b) {
+    for (int i = 3; i >= 0; i--) {
+        if (a[i] < b[i]) return 1;
+        if (a[i] > b[i]) return 0;
+    }
+    return 0;
+}
+
+static void uniform_below_r(const uint64_t *r, uint64_t seed, uint64_t stream, uint64_t index, int lo,
+                            uint64_t *out) {
+    int nbits = 256;
+    while (nbits > 0 && !((r[(nbits - 1) / 64] >> ((nbits - 1) % 64)) & 1)) nbits--;
+    for (uint64_t att = 0; att < 64; att++) {
+        uint64_t v[4];
+        for (int w = 0; w < 4; w++) v[w] = draw_word(seed, stream, index, att, w);
+        if (nbits < 256) v[3] &= (nbits - 192) >= 64 ? ~0ULL : ((1ULL << (nbits - 192)) - 1);
+        int nz = (v[0] | v[1] | v[2] | v[3]) != 0;
+        if (lt4(v, r) && (!lo || nz)) { memcpy(out, v, 32); return; }
+    }
+    out[0] = 1; out[1] = out[2] = out[3] = 0;
+}
+
+/* s * 2^256 mod r by 256 modular doublings (s < r) */
+static void fr_to_mont_slow(const uint64_t *r, const uint64_t *s, uint64_t *out) {
+    uint64_t v[4];
+    memcpy(v, s, 32);
+    for (int k = 0; k < 256; k++) {
+        uint64_t top = v[3] >> 63;
+        for (int i = 3; i > 0; i--) v[i] = (v[i] << 1) | (v[i - 1] >> 63);
+        v[0] <<= 1;
+        if (top || !lt4(v, r)) {
+            u128 bw = 0;
+            for (int i = 0; i < 4; i++) {
+                u128 d = (u128)v[i] - r[i] - bw;
+                v[i] = (uint64_t)d;
+                bw = (d >> 64) & 1;
+            }
+        }
+    }
+    memcpy(out, v, 32);
+}
+
+enum { ST_BASE_K = 1, ST_SCALAR = 2, ST_KIND = 3 };
+
+/* n scalars of element indices index0.. : dist 0 uniform in Fr, 1 witness-like
+ * (40% 0, 20% 1, 25% below 2^32, 15% uniform); fmt 0 integer, 1 Montgomery. */
+void cm_gen_scalars(int curve, uint64_t seed, uint64_t index0, long n, int dist, int fmt, uint64_t *out) {
+    const uint64_t *q = curve == 0 ? FR_BN : curve == 1 ? FR_BL : FR_B7;
+    #pragma omp parallel for schedule(static) num_threads(nthreads())
+    for (long i = 0; i < n; i++) {
+        uint64_t gi = index0 + (uint64_t)i, s[4] = {0, 0, 0, 0};
+        if (dist == 0) {
+            uniform_below_r(q, seed, ST_SCALAR, gi, 0, s);
+        } else {
+            uint64_t u = draw_word(seed, ST_KIND, gi, 0, 0) % 100;
+            if (u < 40) {
+            } else if (u < 60) {
+                s[0] = 1;
+            } else if (u < 85) {
+                s[0] = draw_word(seed, ST_SCALAR, gi, 0, 0) & 0xFFFFFFFFULL;
+            } else {
+                uniform_below_r(q, seed, ST_SCALAR, gi, 0, s);
+            }
+        }
+        if (fmt == 1) fr_to_mont_slow(q, s, s);
+        memcpy(out + 4 * i, s, 32);
+    }
+}
+
+/* n bases P_i = k_i * G, k_i uniform in [1, r) (element indices index0..),
+ * affine Montgomery in the reference layout; 16-bit comb.  Returns 0, or -1
+ * when the comb table cannot be allocated. */
+int cm_gen_bases(int curve, const uint64_t *gen_affine, uint64_t seed, uint64_t index0, long n, uint64_t *out) {
+    const uint64_t *q = curve == 0 ? FR_BN : curve == 1 ? FR_BL : FR_B7;
+    uint64_t *ks = (uint64_t *)malloc(32 * (size_t)(n > 0 ? n : 1));
+    if (!ks) return -1;
+    #pragma omp parallel for schedule(static) num_threads(nthreads())
+    for (long i = 0; i < n; i++) uniform_below_r(q, seed, ST_BASE_K, index0 + (uint64_t)i, 1, ks + 4 * i);
+    int rc = 0;
+    if (curve == 0) {
+        bn_aff *tab = bn_comb_table(&BN, (const bn_aff *)gen_affine, nthreads());
+        if (!tab) rc = -1;
+        else bn_comb_mul(&BN, tab, (const uint32_t *)ks, n, (bn_aff *)out, nthreads());
+        free(tab);
+    } else {
+        const bl_params *P = bl_of(curve);
+        bl_aff *tab = bl_comb_table(P, (const bl_aff *)gen_affine, nthreads());
+        if (!tab) rc = -1;
+        else bl_comb_mul(P, tab, (const uint32_t *)ks, n, (bl_aff *)out, nthreads());
+        free(tab);
+    }
+    free(ks);
+    return rc;
+}
+
+/* ---------------------------------------------------------------- GLV bound
+ * The largest bit length of |k1|, |k2| over n scalars k uniform in [0, r)
+ * (seeded generator, stream ST_SCALAR) for the Babai split
+ *   c_j = (k * g_j + 2^255) >> 256,  k1 = k - c1 a1 - c2 a2,  k2 = -c1 b1 - c2 b2
+ * (the device's decomposition and the Python restatement's glv_split).
+ * Constants are 256-bit two's complement (4 x u64 little endian); all
+ * arithmetic is exact: k * g as a 512-bit product, the rest modulo 2^256,
+ * which holds every true value here (|c_j a_i| < 2^255). */
+typedef struct { uint64_t w[4]; } i256;
+
+static int i256_neg_p(const i256 *a) { return (int)(a->w[3] >> 63); }
+
+static i256 i256_negate(i256 a) {
+    u128 c = 1;
+    for (int i = 0; i < 4; i++) {
+        c += (u128)(~a.w[i]);
+        a.w[i] = (uint64_t)c;
+        c >>= 64;
+    }
+    return a;
+}
+
+static i256 i256_add(i256 a, const i256 *b) {
+    u128 c = 0;
+    for (int i = 0; i < 4; i++) {
+        c += (u128)a.w[i] + b->w[i];
+        a.w[i] = (uint64_t)c;
+        c >>= 64;
+    }
+    return a;
+}
+
+static i256 i256_mul_lo(const i256 *a, const i256 *b) { /* a * b mod 2^256 */
+    uint64_t t[4] = {0, 0, 0, 0};
+    for (int i = 0; i < 4; i++) {
+        u128 c = 0;
+        for (int j = 0; i + j < 4; j++) {
+            c += (u128)a->w[i] * b->w[j] + t[i + j];
+            t[i + j] = (uint64_t)c;
+            c >>= 64;
+        }
+    }
+    i256 r;
+    memcpy(r.w, t, 32);
+    return r;
+}
+
+/* floor((k * g + 2^255) / 2^256) for k >= 0, g signed */
+static i256 babai_c(const uint64_t *k, i256 g) {
+    int neg = i256_neg_p(&g);
+    if (neg) g = i256_negate(g);
+    uint64_t p[8] = {0};
+    for (int i = 0; i < 4; i++) {
+        u128 c = 0;
+        for (int j = 0; j < 4; j++) {
+            c += (u128)k[i] * g.w[j] + p[i + j];
+            p[i + j] = (uint64_t)c;
+            c >>= 64;
+        }
+        p[i + 4] = (uint64_t)c;
+    }
+    i256 hi;
+    if (!neg) { /* (P + 2^255) >> 256 */
+        u128 c = (u128)p[3] + (1ULL << 63);
+        c >>= 64;
+        for (int i = 0; i < 4; i++) {
+            c += p[4 + i];
+            hi.w[i] = (uint64_t)c;
+            c >>= 64;
+        }
+        return hi;
+    }
+    /* floor((2^255 - P) / 2^256) = -ceil((P - 2^255) / 2^256) */
+    uint64_t q[8];
+    u128 bw = 0;
+    for (int i = 0; i < 8; i++) {
+        u128 d = (u128)p[i] - (i == 3 ? (1ULL << 63) : 0) - bw;
+        q[i] = (uint64_t)d;
+        bw = (d >> 64) & 1;
+    }
+    if (bw) { /* P < 2^255: the quotient is 0 */
+        memset(hi.w, 0, 32);
+        return hi;
+    }
+    int frac = (q[0] | q[1] | q[2] | q[3]) != 0;
+    for (int i = 0; i < 4; i++) hi.w[i] = q[4 + i];
+    if (frac) {
+        i256 one = {{1, 0, 0, 0}};
+        hi = i256_add(hi, &one);
+    }
+    return i256_negate(hi);
+}
+
+static int bits_of_abs(i256 v) {
+    if (i256_neg_p(&v)) v = i256_negate(v);
+    for (int i = 3; i >= 0; i--)
+        if (v.w[i]) return 64 * i + 64 - __builtin_clzll(v.w[i]);
+    return 0;
+}
+
+/* consts: g1, g2, a1, a2, b1, b2 (6 x 4 u64).  Returns the largest bit length
+ * of |k1|, |k2| over n seeded scalars and the m extra scalars in `extra`. */
+int cm_glv_max_bits(int curve, const uint64_t *consts, uint64_t seed, long n, const uint64_t *extra, long m) {
+    const uint64_t *q = curve == 0 ? FR_BN : curve == 1 ? FR_BL : FR_B7;
+    i256 g1, g2, a1, a2, b1, b2;
+    memcpy(g1.w, consts, 32);
+    memcpy(g2.w, consts + 4, 32);
+    memcpy(a1.w, consts + 8, 32);
+    memcpy(a2.w, consts + 12, 32);
+    memcpy(b1.w, consts + 16, 32);
+    memcpy(b2.w, consts + 20, 32);
+    int best = 0;
+    #pragma omp parallel for schedule(static) reduction(max : best) num_threads(nthreads())
+    for (long i = 0; i < n + m; i++) {
+        uint64_t k[4];
+        if (i < n) uniform_below_r(q, seed, ST_SCALAR, (uint64_t)i, 0, k);
+        else memcpy(k, extra + 4 * (i - n), 32);
+        i256 c1 = babai_c(k, g1), c2 = babai_c(k, g2);
+        i256 kk;
+        memcpy(kk.w, k, 32);
+        i256 t1 = i256_negate(i256_mul_lo(&c1, &a1)), t2 = i256_negate(i256_mul_lo(&c2, &a2));
+        i256 k1 = i256_add(i256_add(kk, &t1), &t2);
+        i256 u1 = i256_negate(i256_mul_lo(&c1, &b1)), u2 = i256_negate(i256_mul_lo(&c2, &b2));
+        i256 k2 = i256_add(u1, &u2);
+        int b = bits_of_abs(k1);
+        int b2v = bits_of_abs(k2);
+        if (b2v > b) b = b2v;
+        if (b > best) best = b;
+    }
+    return best;
+}

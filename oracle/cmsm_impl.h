@@ -275,3 +275,83 @@ static void FN(scalar_mul)(const FN(params) *P, const FN(aff) *G, const uint32_t
     }
     *out = acc;
 }
+
+/* Jacobian -> affine for m points with one inversion (Montgomery's trick:
+ * prefix products of the Z, one Fermat inverse, then back-substitution);
+ * identities (Z = 0) become the all-zero affine point.  bn254_msm.c:544-599
+ * batch-normalises the same way. */
+static void FN(batch_to_affine)(const FN(params) *P, const FN(jac) *in, FN(aff) *out, long m, uint64_t *pre) {
+    uint64_t acc[NL];
+    memcpy(acc, P->one, sizeof acc);
+    for (long i = 0; i < m; i++) {
+        memcpy(pre + i * NL, acc, sizeof acc);
+        if (!FN(jac_is_id)(&in[i])) FN(mul)(P, acc, in[i].z, acc);
+    }
+    uint64_t inv[NL];
+    FN(inv)(P, acc, inv);
+    for (long i = m - 1; i >= 0; i--) {
+        if (FN(jac_is_id)(&in[i])) { memset(&out[i], 0, sizeof out[i]); continue; }
+        uint64_t zi[NL], zi2[NL], zi3[NL];
+        FN(mul)(P, inv, pre + i * NL, zi);     /* 1 / Z_i */
+        FN(mul)(P, inv, in[i].z, inv);         /* drop Z_i from the running inverse */
+        FN(mul)(P, zi, zi, zi2);
+        FN(mul)(P, zi2, zi, zi3);
+        FN(mul)(P, in[i].x, zi2, out[i].x);
+        FN(mul)(P, in[i].y, zi3, out[i].y);
+    }
+}
+
+/* Fixed-base comb of 16 rows of 16-bit digits: tab[j * 65536 + d] = d * 2^(16 j) * G
+ * (affine, d = 0 is the zero point).  Rows are built in parallel. */
+#define FN_COMB_ROWS 16
+#define FN_COMB_SPAN 65536L
+static FN(aff) *FN(comb_table)(const FN(params) *P, const FN(aff) *G, int threads) {
+    FN(aff) *tab = (FN(aff) *)malloc(sizeof(FN(aff)) * FN_COMB_ROWS * FN_COMB_SPAN);
+    if (!tab) return NULL;
+    #pragma omp parallel for schedule(dynamic, 1) num_threads(threads)
+    for (int j = 0; j < FN_COMB_ROWS; j++) {
+        FN(jac) b;
+        FN(set_id)(P, &b);
+        FN(add_aff)(P, &b, G, &b);
+        for (int s = 0; s < 16 * j; s++) FN(dbl)(P, &b, &b);
+        FN(aff) ba;
+        FN(to_affine)(P, &b, &ba);
+        FN(jac) *row = (FN(jac) *)malloc(sizeof(FN(jac)) * FN_COMB_SPAN);
+        uint64_t *pre = (uint64_t *)malloc(8 * NL * FN_COMB_SPAN);
+        FN(set_id)(P, &row[0]);
+        for (long d = 1; d < FN_COMB_SPAN; d++) FN(add_aff)(P, &row[d - 1], &ba, &row[d]);
+        FN(batch_to_affine)(P, row, tab + j * FN_COMB_SPAN, FN_COMB_SPAN, pre);
+        free(pre);
+        free(row);
+    }
+    return tab;
+}
+
+/* out[i] = k_i * G (affine) for integer scalars k_i < 2^256 (8x u32): 16 comb
+ * additions per point, then one batch inversion per block of points. */
+static void FN(comb_mul)(const FN(params) *P, const FN(aff) *tab, const uint32_t *ks, long n, FN(aff) *out,
+                         int threads) {
+    const long BLK = 1024;
+    #pragma omp parallel num_threads(threads)
+    {
+        FN(jac) *acc = (FN(jac) *)malloc(sizeof(FN(jac)) * BLK);
+        uint64_t *pre = (uint64_t *)malloc(8 * NL * BLK);
+        #pragma omp for schedule(dynamic, 1)
+        for (long b0 = 0; b0 < n; b0 += BLK) {
+            long m = n - b0 < BLK ? n - b0 : BLK;
+            for (long i = 0; i < m; i++) {
+                const uint32_t *k = ks + 8 * (b0 + i);
+                FN(set_id)(P, &acc[i]);
+                for (int j = 0; j < FN_COMB_ROWS; j++) {
+                    uint32_t d = (k[j / 2] >> (16 * (j % 2))) & 0xffffu;
+                    if (d) FN(add_aff)(P, &acc[i], &tab[j * FN_COMB_SPAN + d], &acc[i]);
+                }
+            }
+            FN(batch_to_affine)(P, acc, out + b0, m, pre);
+        }
+        free(pre);
+        free(acc);
+    }
+}
+#undef FN_COMB_ROWS
+#undef FN_COMB_SPAN

@@ -23,6 +23,9 @@ CURVE_ID = {"bn254": 0, "bls12_381": 1, "bls12_377": 2}
 FP_BYTES = {"bn254": 32, "bls12_381": 48, "bls12_377": 48}
 
 _u64p = ctypes.POINTER(ctypes.c_uint64)
+_BN254_P = 0x30644e72e131a029b85045b68181585d97816a916871ca8d3c208c16d87cfd47
+_BLS381_P = int("1a0111ea397fe69a4b1ba7b6434bacd764774b84f38512bf6730d2a0f6b0f624"
+                "1eabfffeb153ffffb9feffffffffaaab", 16)
 _u32p = ctypes.POINTER(ctypes.c_uint32)
 
 
@@ -52,6 +55,14 @@ class COracle:
         L.cm_jacobian_to_affine.argtypes = [ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p]
         L.cm_affine_add.argtypes = [ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
         L.cm_set_threads.argtypes = [ctypes.c_int]
+        L.cm_gen_scalars.argtypes = [ctypes.c_int, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_long, ctypes.c_int,
+                                     ctypes.c_int, ctypes.c_void_p]
+        L.cm_gen_bases.argtypes = [ctypes.c_int, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_long,
+                                   ctypes.c_void_p]
+        L.cm_gen_bases.restype = ctypes.c_int
+        L.cm_glv_max_bits.argtypes = [ctypes.c_int, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_long, ctypes.c_void_p,
+                                      ctypes.c_long]
+        L.cm_glv_max_bits.restype = ctypes.c_int
 
     def set_threads(self, t):
         self.lib.cm_set_threads(int(t))
@@ -70,6 +81,35 @@ class COracle:
         out = np.zeros(n * 2 * FP_BYTES[curve], dtype=np.uint8)
         self.lib.cm_fixed_base_mul(CURVE_ID[curve], g.ctypes.data, k.ctypes.data, int(n), out.ctypes.data)
         return out.tobytes()
+
+    def gen_scalars(self, curve, seed, n, dist="uniform", fmt=1, index0=0):
+        """n synthetic scalars (8x u32 each) of the seeded generator: the same
+        bytes as the Python restatement's make_scalars (and the library's
+        device generator); fmt 0 integer, 1 Montgomery."""
+        out = np.zeros(32 * n, dtype=np.uint8)
+        self.lib.cm_gen_scalars(CURVE_ID[curve], int(seed), int(index0), int(n), 0 if dist == "uniform" else 1,
+                                int(fmt), out.ctypes.data)
+        return out
+
+    def gen_bases(self, curve, gen_affine, seed, n, index0=0):
+        """n synthetic bases k_i*G (affine Montgomery, reference layout) of the
+        seeded generator, by a 16-bit fixed-base comb on all host threads."""
+        g = np.frombuffer(gen_affine, dtype=np.uint8)
+        out = np.zeros(n * 2 * FP_BYTES[curve], dtype=np.uint8)
+        if self.lib.cm_gen_bases(CURVE_ID[curve], g.ctypes.data, int(seed), int(index0), int(n), out.ctypes.data):
+            raise MemoryError("cm_gen_bases: comb table allocation failed")
+        return out
+
+    def glv_max_bits(self, curve, glv, seed, n, extra=()):
+        """Largest bit length of |k1|, |k2| of the Babai GLV split (constants
+        `glv`: g1, g2, a1, a2, b1, b2 as Python ints) over n seeded uniform
+        scalars plus the scalars in `extra`."""
+        def tc(v):
+            return (v % (1 << 256)).to_bytes(32, "little")
+        consts = np.frombuffer(b"".join(tc(glv[k]) for k in ("g1", "g2", "a1", "a2", "b1", "b2")), dtype=np.uint8)
+        ex = np.frombuffer(b"".join(int(k).to_bytes(32, "little") for k in extra) or bytes(32), dtype=np.uint8)
+        return self.lib.cm_glv_max_bits(CURVE_ID[curve], consts.ctypes.data, int(seed), int(n), ex.ctypes.data,
+                                        len(extra))
 
     def fr_from_mont(self, curve, mont, n):
         m = np.frombuffer(mont, dtype=np.uint8)
@@ -138,6 +178,27 @@ class RefOracle:
             return out.tobytes()
         # the reference exports no BLS12-381 Jacobian->affine; normalise with the restatement
         return self._conv().jacobian_to_affine(curve, jac)
+
+    def point_scalar_mul(self, curve, point_affine, k_int):
+        """k*P (affine bytes) by the reference's own double-and-add
+        (bn254_point_scalar_mul, bn254_msm.c:1333; bls12_381_g1_scalar_mul,
+        bls12_381_ops.c:946), for k an integer below 2^256."""
+        f = FP_BYTES[curve]
+        nl = f // 8
+        jac = np.zeros(3 * nl, dtype=np.uint64)
+        jac[:2 * nl] = np.frombuffer(point_affine, dtype=np.uint64)
+        one = (1 << (8 * f)) % {"bn254": _BN254_P, "bls12_381": _BLS381_P}[curve]
+        jac[2 * nl:] = np.frombuffer(one.to_bytes(f, "little"), dtype=np.uint64)
+        out = np.zeros(3 * nl, dtype=np.uint64)
+        if curve == "bn254":
+            k = np.frombuffer(int(k_int).to_bytes(32, "little"), dtype=np.uint32).copy()
+            self.lib.bn254_point_scalar_mul(jac.ctypes.data, k.ctypes.data, out.ctypes.data)
+            aff = np.zeros(8, dtype=np.uint64)
+            self.lib.bn254_projective_to_affine(out.ctypes.data, aff.ctypes.data)
+            return aff.tobytes()
+        k = np.frombuffer(int(k_int).to_bytes(32, "little"), dtype=np.uint64).copy()
+        self.lib.bls12_381_g1_scalar_mul(jac.ctypes.data, k.ctypes.data, out.ctypes.data)
+        return self._conv().jacobian_to_affine(curve, out.tobytes())
 
     def fr_from_mont(self, curve, mont, n):
         m = np.frombuffer(mont, dtype=np.uint8)

@@ -79,11 +79,29 @@ def test_glv_split_bound(curve):
     g = C.glv
     for v in (g["a1"], g["a2"], g["b1"], g["b2"]):
         ks += [abs(v) % C.r, (C.r - abs(v)) % C.r, (abs(v) * C.lam) % C.r]
-    ks += [rng.randrange(C.r) for _ in range(200000)]
+    ks += [rng.randrange(C.r) for _ in range(20000)]
     for k in ks:
         k1, k2 = R.glv_split(C, k)
         assert (k1 + k2 * C.lam - k) % C.r == 0
         assert abs(k1) < (1 << bits) and abs(k2) < (1 << bits)
+
+
+@pytest.mark.parametrize("curve", ["bn254", "bls12_381", "bls12_377"])
+def test_glv_split_bound_1e7_in_c(curve, oracles):
+    """The same bound over 4*10^7 seeded uniform scalars, by the oracle's C
+    restatement of the split (exact 256/512-bit integer arithmetic),
+    cross-checked against the Python split on the edge scalars and 2000
+    random ones.  k1 + k2*lambda = k (mod r) holds for any c1, c2 because
+    the lattice vectors satisfy a + b*lambda = 0 (mod r), checked once in
+    the constant derivation."""
+    _, cm = oracles
+    C = R.CURVES[curve]
+    bits = R.glv_half_bits(C)
+    rng = random.Random(11)
+    ks = [0, 1, 2, C.r - 1, C.r - 2, C.lam, C.r - C.lam, C.r // 2] + [rng.randrange(C.r) for _ in range(2000)]
+    want = max(max(abs(a).bit_length(), abs(b).bit_length()) for a, b in (R.glv_split(C, k) for k in ks))
+    assert cm.glv_max_bits(curve, C.glv, 0, 0, ks) == want
+    assert cm.glv_max_bits(curve, C.glv, 0x61C, 4 * 10 ** 7) <= bits
 
 
 def test_endomorphism_constants():
@@ -159,3 +177,19 @@ def test_g2_restatement_group_laws():
     assert G2.add(G2.scalar_mul(G, 5), G2.scalar_mul(G, 7)) == G2.scalar_mul(G, 12)
     assert G2.dec_affine(G2.enc_affine(P)) == P
     assert G2.enc_affine(None) == bytes(128)
+
+
+@pytest.mark.parametrize("curve", ["bn254", "bls12_381", "bls12_377"])
+def test_host_generator_matches_restatement(curve, oracles):
+    """The oracle's C generator (used for the CPU-only reference inputs) gives
+    the same bytes as the Python restatement of the seeded generator, which
+    the library's device generator matches (test_generator_matches_restatement):
+    scalars in both forms and distributions, and bases k_i*G from the comb."""
+    _, cm = oracles
+    C = R.CURVES[curve]
+    for dist in ("uniform", "witness"):
+        sc = [R.scalar_uniform(C, 77, i) if dist == "uniform" else R.scalar_witness(C, 77, i) for i in range(5, 45)]
+        assert cm.gen_scalars(curve, 77, 40, dist, 0, index0=5).tobytes() == R.pack_scalars_int(sc)
+        assert cm.gen_scalars(curve, 77, 40, dist, 1, index0=5).tobytes() == R.pack_scalars_mont(C, sc)
+    got = cm.gen_bases(curve, C.enc_affine((C.gx, C.gy)), 77, 24, index0=3).tobytes()
+    assert got == R.pack_points(C, [R.scalar_mul(C, (C.gx, C.gy), R.base_scalar(C, 77, i)) for i in range(3, 27)])

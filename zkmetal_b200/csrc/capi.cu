@@ -964,6 +964,19 @@ ZkMetalStatus zkmsm_plan_describe_shift(int curve, const uint32_t* counts, uint3
 
 uint64_t zkmsm_engine_launch_count(ZkMetalMSMEngine engine) { return engine ? ENG(engine).launches : 0; }
 
+uint64_t zkmsm_engine_last_entries(ZkMetalMSMEngine engine) {
+    if (!engine) return 0;
+    Engine& e = ENG(engine);
+    if (!e.w_totals.p) return 0;
+    uint32_t v = 0;
+    if (cudaDeviceSynchronize() != cudaSuccess ||
+        cudaMemcpy(&v, e.w_totals.p, sizeof v, cudaMemcpyDeviceToHost) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return v;
+}
+
 void* zkmsm_device_alloc(uint64_t bytes) {
     void* p = nullptr;
     if (cudaMalloc(&p, bytes) != cudaSuccess) {

@@ -17,11 +17,17 @@
 // Host code cannot use the array's name as a device address, so the first
 // call on each device (with that device current) looks its address up with
 // cudaGetSymbolAddress and caches it; make that first call before any stream
-// capture.  Limits: n <= N_MAX (8192), fixed window width 10 with GLV.
-// Every call shares the one array and it keeps the last call's contents:
-// the parts that must start at zero are cleared on each call, and two calls
-// whose GPU work overlaps (different streams, or different host threads)
-// race on it -- serialise them.
+// capture.  The cached address belongs to the device's context: after a
+// cudaDeviceReset of that device in the same process it is stale, so do not
+// call this entry point again after such a reset.  The call's own launch
+// tables (MSM descriptor, reduction tasks) are written into the array by a
+// one-thread kernel from by-value arguments, so the call reads no host memory
+// after it returns.  Limits: n <= N_MAX (8192), fixed window width 10 with
+// GLV.  Every call shares the one array and it keeps the last call's
+// contents: the parts that must start at zero are cleared on each call, and
+// two calls whose GPU work overlaps (different streams, or different host
+// threads) race on it -- serialise them.  Calls queued one after another on
+// one stream are ordered by the stream and need nothing more.
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -84,6 +90,41 @@ static __device__ __align__(256) unsigned char g_scratch[SCRATCH_BYTES];
 static std::mutex g_mu;
 static unsigned char* g_addr[64];
 
+// The launch tables of one call, built on the device from by-value
+// arguments: the MSM descriptor (one MSM, window width CB, GLV) and the
+// reduction tasks (RED_LEVELS levels of NWIN windows, L = RED_L).
+static __global__ void k_noalloc_tables(MsmDesc* __restrict__ desc, RedTask* __restrict__ tasks, uint32_t n,
+                                        uint32_t fmt) {
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    MsmDesc d{};
+    d.scalar_off = 0;
+    d.n = n;
+    d.base_off = 0;
+    d.c = CB;
+    d.nwin = NWIN;
+    d.glv = 1;
+    d.bucket_off = 0;
+    d.fmt = fmt;
+    d.win_off = 0;
+    d.wstep = 0;
+    d.nred = NWIN;
+    d.nlo = NWIN;
+    *desc = d;
+    uint32_t nin = BPW;
+    for (int l = 0; l < RED_LEVELS; l++) {
+        const uint32_t nout = (nin + RED_L - 1) / RED_L;
+        for (uint32_t w = 0; w < NWIN; w++) {
+            RedTask t;
+            t.in_off = l == 0 ? w * BPW : w * nin;
+            t.n_in = nin;
+            t.out_off = w * nout;
+            t.n_out = nout;
+            tasks[l * NWIN + w] = t;
+        }
+        nin = nout;
+    }
+}
+
 static void scan(unsigned char* base, uint32_t* d, uint32_t n, uint32_t* d_total, uint32_t* copy, cudaStream_t s) {
     uint32_t tiles = (n + SCAN_TILE - 1) / SCAN_TILE;
     if (tiles == 0) tiles = 1;
@@ -101,15 +142,39 @@ using namespace zkmsm::noalloc;
 
 extern "C" ZkMetalStatus zkmsm_bn254_msm_noalloc(const void* d_points, const void* d_scalars, int fmt,
                                                  uint32_t n_points, void* d_result, void* stream) {
-    if (!d_points || !d_scalars || !d_result || n_points == 0) return ZKMETAL_ERR_INVALID_INPUT;
-    if (fmt != ZKMSM_SCALAR_INT && fmt != ZKMSM_SCALAR_MONT) return ZKMETAL_ERR_INVALID_INPUT;
+    if (!d_points || !d_scalars || !d_result) {
+        set_error("zkmsm_bn254_msm_noalloc: null device pointer");
+        return ZKMETAL_ERR_INVALID_INPUT;
+    }
+    if (n_points == 0) {
+        set_error("zkmsm_bn254_msm_noalloc: n_points is 0");
+        return ZKMETAL_ERR_INVALID_INPUT;
+    }
+    if (fmt != ZKMSM_SCALAR_INT && fmt != ZKMSM_SCALAR_MONT) {
+        set_error("zkmsm_bn254_msm_noalloc: scalar_fmt must be 0 (integer) or 1 (Montgomery)");
+        return ZKMETAL_ERR_INVALID_INPUT;
+    }
     if (n_points > N_MAX) {
         set_error("zkmsm_bn254_msm_noalloc: n_points exceeds the allocation-free limit of 8192");
         return ZKMETAL_ERR_INVALID_INPUT;
     }
+    // a launch error left pending by the caller's own work would otherwise be
+    // reported below as this call's: refuse, and leave it pending for them
+    const cudaError_t pending = cudaPeekAtLastError();
+    if (pending != cudaSuccess) {
+        set_error(std::string("zkmsm_bn254_msm_noalloc: a CUDA error was pending before the call: ") +
+                  cudaGetErrorString(pending));
+        return ZKMETAL_ERR_GPU_ERROR;
+    }
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return ZKMETAL_ERR_NO_GPU;
+    cudaError_t de = cudaGetDevice(&dev);
+    if (de != cudaSuccess || dev < 0 || dev >= 64) {
+        if (de != cudaSuccess) cudaGetLastError();
+        set_error(std::string("zkmsm_bn254_msm_noalloc: no usable current device: ") +
+                  (de != cudaSuccess ? cudaGetErrorString(de) : "device index out of range"));
+        return ZKMETAL_ERR_NO_GPU;
+    }
     unsigned char* base;
     {
         std::lock_guard<std::mutex> lk(g_mu);
@@ -117,6 +182,7 @@ extern "C" ZkMetalStatus zkmsm_bn254_msm_noalloc(const void* d_points, const voi
             void* ptr = nullptr;
             cudaError_t e = cudaGetSymbolAddress(&ptr, g_scratch);
             if (e != cudaSuccess || !ptr) {
+                cudaGetLastError();
                 set_error(std::string("zkmsm_bn254_msm_noalloc: cudaGetSymbolAddress failed: ") +
                           cudaGetErrorString(e));
                 return ZKMETAL_ERR_GPU_ERROR;
@@ -126,33 +192,6 @@ extern "C" ZkMetalStatus zkmsm_bn254_msm_noalloc(const void* d_points, const voi
         base = g_addr[dev];
     }
     const uint32_t n = n_points;
-    // launch tables, built on the host stack and copied into the scratch array
-    MsmDesc desc{};
-    desc.scalar_off = 0;
-    desc.n = n;
-    desc.base_off = 0;
-    desc.c = CB;
-    desc.nwin = NWIN;
-    desc.glv = 1;
-    desc.bucket_off = 0;
-    desc.fmt = (uint32_t)fmt;
-    desc.win_off = 0;
-    desc.wstep = 0;
-    desc.nred = NWIN;
-    desc.nlo = NWIN;
-    RedTask tasks[RED_LEVELS * NWIN];
-    uint32_t nin = BPW;
-    for (int l = 0; l < RED_LEVELS; l++) {
-        uint32_t nout = (nin + RED_L - 1) / RED_L;
-        for (uint32_t w = 0; w < NWIN; w++) {
-            RedTask& t = tasks[l * NWIN + w];
-            t.in_off = l == 0 ? w * BPW : w * nin;
-            t.n_in = nin;
-            t.out_off = w * nout;
-            t.n_out = nout;
-        }
-        nin = nout;
-    }
     uint32_t accK[MAX_ACC_LEVELS], accT[MAX_ACC_LEVELS];
     int nacc = 0;
     uint64_t M = 2ull * n * NWIN;
@@ -167,12 +206,15 @@ extern "C" ZkMetalStatus zkmsm_bn254_msm_noalloc(const void* d_points, const voi
         M = 2 * T;
         K = KJ;
     }
-    auto ck = [](cudaError_t e) { return e == cudaSuccess; };
-    bool ok = ck(cudaMemcpyAsync(base + OFF_DESC, &desc, sizeof desc, cudaMemcpyHostToDevice, s)) &&
-              ck(cudaMemcpyAsync(base + OFF_TASKS, tasks, sizeof tasks, cudaMemcpyHostToDevice, s)) &&
-              ck(cudaMemsetAsync(base + OFF_COUNTS, 0, (NB + 1) * 4, s)) &&
-              ck(cudaMemsetAsync(base + OFF_BUCKETS, 0, NB * XS, s));
-    if (!ok) return ZKMETAL_ERR_GPU_ERROR;
+    k_noalloc_tables<<<1, 32, 0, s>>>(reinterpret_cast<MsmDesc*>(base + OFF_DESC),
+                                      reinterpret_cast<RedTask*>(base + OFF_TASKS), n, (uint32_t)fmt);
+    cudaError_t me = cudaMemsetAsync(base + OFF_COUNTS, 0, (NB + 1) * 4, s);
+    if (me == cudaSuccess) me = cudaMemsetAsync(base + OFF_BUCKETS, 0, NB * XS, s);
+    if (me != cudaSuccess) {
+        cudaGetLastError();
+        set_error(std::string("zkmsm_bn254_msm_noalloc: clearing the scratch failed: ") + cudaGetErrorString(me));
+        return ZKMETAL_ERR_GPU_ERROR;
+    }
 
     const uint32_t* pts = static_cast<const uint32_t*>(d_points);
     const uint32_t* sc = static_cast<const uint32_t*>(d_scalars);
