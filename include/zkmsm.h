@@ -95,6 +95,17 @@ ZkMetalStatus zkmetal_bn254_msm_batch_auto(const uint8_t* all_points, const uint
 ZkMetalStatus zkmetal_bn254_msm_fr(ZkMetalMSMEngine engine, const uint8_t* points, const uint8_t* scalars_mont,
                                    uint32_t n_points, uint8_t* result_x, uint8_t* result_y, uint8_t* result_z);
 
+/* NEW: n_msms independent MSMs in one batched launch sequence, for any curve
+ * and either scalar form -- the general form of zkmetal_bn254_msm_batch
+ * (zkmetal.h:499), behind the Swift batch front-ends batchMSMAsync
+ * (MSM/MultiMSM.swift:175), innerProductMSM (:90) and multiMSM with Fr scalar
+ * sets (:63).  MSM i runs over the i-th consecutive run of counts[i] points
+ * and scalars of all_points / all_scalars (host memory); results as in the
+ * batch call (n_msms x 3 coordinates, counts[i] == 0 -> zero bytes). */
+ZkMetalStatus zkmsm_msm_batch(ZkMetalMSMEngine engine, int curve, const uint8_t* all_points,
+                              const uint8_t* all_scalars, int scalar_fmt, const uint32_t* counts, uint32_t n_msms,
+                              uint8_t* results);
+
 /* ---- BLS12-381 G1 MSM ---------------------------------------------------
  * NEW symbols: the reference FFI has none.  They replace the Swift API
  * BLS12381MSM.msm / msmFr (MSM/BLS12381MSMEngine.swift:260, 517) and the C
@@ -249,6 +260,41 @@ ZkMetalStatus zkmsm_server_stats(ZkMsmServer server, char* buf, uint64_t buflen)
 /* Test hook: make the next `batches` batches fail on the host before any GPU work. */
 ZkMetalStatus zkmsm_server_inject_failures(ZkMsmServer server, int batches);
 void zkmsm_server_destroy(ZkMsmServer server);
+
+/* NEW: request-level replicas for serving on several GPUs.  Each replica is a
+ * server created (zkmsm_server_create) with its own device current and its
+ * own resident tables on that device; the pool routes every submitted
+ * request whole to one replica -- no collective, no data crossing GPUs.
+ * Routing (zkmsm_route_pick): among replicas holding a table for the curve
+ * that is long enough and a budget that can ever hold the request, one with
+ * free budget for it now beats one without; then the shallowest queue
+ * (points submitted and not finished, divided by relative_speed); then the
+ * most free budget; then the first in cyclic order from `first` (the pool
+ * advances it with every request, so ties rotate over the replicas).  The
+ * pool does not own the servers: destroy the pool first.  Ids are the
+ * pool's own. */
+typedef struct {
+    int32_t has_table;       /* a table for the request's curve */
+    uint64_t table_points;   /* its length */
+    uint64_t queued_points;  /* points of requests submitted and not finished */
+    uint64_t budget_bytes;   /* admission budget */
+    uint64_t in_use_bytes;   /* admitted and running */
+    double relative_speed;   /* 1.0 for identical GPUs */
+} ZkMsmReplicaLoad;
+typedef void* ZkMsmPool;
+/* index of the replica for a request, or -1 when none can take it (pure host
+ * logic: the rule the pool applies, callable without a GPU) */
+int zkmsm_route_pick(const ZkMsmReplicaLoad* loads, uint32_t n_replicas, uint32_t request_points,
+                     uint64_t request_bytes, uint32_t first);
+ZkMetalStatus zkmsm_pool_create(const ZkMsmServer* servers, uint32_t n_servers, ZkMsmPool* out);
+/* ZKMETAL_ERR_BUSY when no replica can take the request */
+ZkMetalStatus zkmsm_pool_submit(ZkMsmPool pool, int curve, const void* scalars, int scalar_fmt, uint32_t n_points,
+                                uint64_t* request_id);
+ZkMetalStatus zkmsm_pool_wait(ZkMsmPool pool, uint64_t request_id, int timeout_ms, uint8_t* result,
+                              double* latency_ms);
+/* {"replicas": [server stats + "routed" (requests sent there) + "device"]} */
+ZkMetalStatus zkmsm_pool_stats(ZkMsmPool pool, char* buf, uint64_t buflen);
+void zkmsm_pool_destroy(ZkMsmPool pool);
 
 /* Tuning overrides (0 = automatic): window bits, chunk length, GLV on/off.
  * window_bits >= 2^16 is a two-width layout c | nlo << 16: nlo windows of

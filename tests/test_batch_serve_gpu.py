@@ -203,3 +203,40 @@ def test_grouped_batch_from_host_scalars(eng, shift):
         else:
             assert got == plain(e, "bn254", p, sc[off * 32:], c), (i, c)
         off += c
+
+
+def test_replica_pool_routes_and_matches_plain(eng):
+    """Two replicas (servers with their own tables; both on device 0 here, one
+    per GPU in production) behind one pool: requests are spread over both
+    and every result equals the plain MSM of its request."""
+    from zkmetal_b200 import CommitmentServerPool
+    T = 1 << 14
+    reps, tabs, pts = [], [], {}
+    try:
+        for k in range(2):
+            for curve, cid in (("bn254", 0), ("bls12_381", 1)):
+                p, _ = gen_inputs(eng[curve], curve, 340 + cid, T, "uniform", zl.SCALAR_MONT)
+                pts[curve] = p
+                tabs.append(CommitmentTable(eng[curve], p.data_ptr(), on_device=True, n=T))
+            reps.append(CommitmentServer(tabs[-2], tabs[-1], workers=2))
+        pool = CommitmentServerPool(reps)
+        rng = random.Random(5)
+        reqs, ids = [], []
+        for i in range(40):
+            curve = "bn254" if rng.random() < 0.7 else "bls12_381"
+            n = rng.randint(1, T)
+            sc = scalars_host(eng[curve], curve, 350 + i, n, "uniform" if i % 2 else "witness")
+            reqs.append((curve, n, sc))
+            ids.append(pool.submit(0 if curve == "bn254" else 1, sc, zl.SCALAR_MONT))
+        for (curve, n, sc), rid in zip(reqs, ids):
+            r, _ = pool.wait(rid)
+            assert r.x + r.y + r.z == plain(eng[curve], curve, pts[curve], sc, n)
+        st = pool.stats()
+        assert [x["routed"] for x in st["replicas"]] and all(x["routed"] > 0 for x in st["replicas"])
+        assert sum(x["completed"] for x in st["replicas"]) == 40
+        pool.close()
+    finally:
+        for s in reps:
+            s.close()
+        for t in tabs:
+            t.close()

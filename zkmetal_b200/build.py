@@ -63,20 +63,39 @@ def build(force=False, ptxas_verbose=False, extra=None, out=None):
     if ptxas_verbose:
         base += ["-Xptxas", "-v"]
     base += extra or []
+    digest = _digest()  # of the sources as they are now, before compiling them
+    # a unit is recompiled when its source, any header or the flags changed
+    common = hashlib.sha256()
+    for f in sorted(_inputs()):
+        if not f.endswith(".cu"):
+            with open(f, "rb") as fh:
+                common.update(os.path.basename(f).encode() + fh.read())
+    common.update(" ".join(base).encode())
     procs, objs = [], []
     for s in SOURCES:
         obj = os.path.join(objdir, s.replace(".cu", ".o"))
         objs.append(obj)
-        procs.append((s, subprocess.Popen(base + ["-c", os.path.join(CSRC, s), "-o", obj])))
-    bad = [s for s, p in procs if p.wait() != 0]
+        h = common.copy()
+        with open(os.path.join(CSRC, s), "rb") as fh:
+            h.update(fh.read())
+        unit_digest = h.hexdigest()
+        if not force and os.path.exists(obj) and os.path.exists(obj + ".stamp"):
+            with open(obj + ".stamp") as fh:
+                if fh.read().strip() == unit_digest:
+                    continue
+        procs.append((s, subprocess.Popen(base + ["-c", os.path.join(CSRC, s), "-o", obj]), obj, unit_digest))
+    bad = [s for s, p, _, _ in procs if p.wait() != 0]
     if bad:
         raise RuntimeError("nvcc failed for " + ", ".join(bad))
+    for _, _, obj, unit_digest in procs:
+        with open(obj + ".stamp", "w") as fh:
+            fh.write(unit_digest)
     tmp = lib + ".tmp"
     subprocess.check_call([NVCC, "-shared"] + ARCH + objs + ["-o", tmp, "-lcudart"])
     os.replace(tmp, lib)
     if lib == LIB and not extra:
         with open(STAMP, "w") as f:
-            f.write(_digest())
+            f.write(digest)
     return lib
 
 

@@ -554,6 +554,20 @@ ZkMetalStatus zkmetal_bn254_msm_batch_auto(const uint8_t* all_points, const uint
     });
 }
 
+ZkMetalStatus zkmsm_msm_batch(ZkMetalMSMEngine engine, int curve, const uint8_t* all_points,
+                              const uint8_t* all_scalars, int fmt, const uint32_t* counts, uint32_t n_msms,
+                              uint8_t* results) {
+    if (!engine || !curve_ok(curve)) return ZKMETAL_ERR_INVALID_INPUT;
+    if (fmt != ZKMSM_SCALAR_INT && fmt != ZKMSM_SCALAR_MONT) return ZKMETAL_ERR_INVALID_INPUT;
+    return guarded([&] {
+        ZkMetalStatus st = ZKMETAL_SUCCESS;
+        with_curve(curve, [&](auto cv) {
+            st = msm_batch_host<decltype(cv)>(ENG(engine), all_points, all_scalars, counts, n_msms, fmt, results);
+        });
+        return st;
+    });
+}
+
 ZkMetalStatus zkmetal_bls12_381_g1_msm(ZkMetalMSMEngine engine, const uint8_t* points, const uint8_t* scalars,
                                        uint32_t n, uint8_t* rx, uint8_t* ry, uint8_t* rz) {
     if (!engine) return ZKMETAL_ERR_INVALID_INPUT;

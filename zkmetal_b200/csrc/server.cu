@@ -1,5 +1,6 @@
 // Commitment server: continuous batching of MSM requests over resident base
-// tables (one per curve).
+// tables (one per curve); and a pool of such servers, one per GPU, that
+// routes whole requests to replicas by queue depth and free HBM.
 //
 // The reference has no concurrent or persistent batching: its "async" batch
 // runs MSMs one after another (Sources/zkMetal/MSM/MultiMSM.swift:175-238).
@@ -64,6 +65,9 @@ struct Server {
     std::atomic<uint64_t> next_id{1};
     bool stop = false;
     std::vector<std::thread> workers;
+    // points of requests submitted and not yet finished (pending or running):
+    // the queue depth a replica pool routes by
+    uint64_t queued_points = 0;
     // stats
     uint64_t batches = 0, completed = 0, failed = 0, max_batch = 0;
     std::vector<double> latencies_ms;
@@ -230,6 +234,7 @@ struct Server {
                 for (auto& r : batch) {
                     r->t_done = now;
                     r->status = st;
+                    queued_points -= r->n;
                     if (st == ZKMETAL_SUCCESS) {
                         completed++;
                         latencies_ms.push_back(std::chrono::duration<double, std::milli>(now - r->t_submit).count());
@@ -251,12 +256,154 @@ struct Server {
     }
 };
 
+// A pool of servers, one per GPU (each with its own resident tables): whole
+// requests are routed to one replica, with no collective and no data moving
+// between GPUs.
+struct Pool {
+    std::vector<Server*> reps;
+    std::mutex mu;
+    std::unordered_map<uint64_t, std::pair<uint32_t, uint64_t>> ids;  // pool id -> (replica, server id)
+    uint64_t next_id = 1;
+    std::vector<uint64_t> routed;
+    uint32_t rr = 0;  // first replica of the tie order, advanced per request
+};
+
 }  // namespace
 }  // namespace zkmsm
 
 using namespace zkmsm;
 
 extern "C" {
+
+int zkmsm_route_pick(const ZkMsmReplicaLoad* loads, uint32_t n_replicas, uint32_t request_points,
+                     uint64_t request_bytes, uint32_t first) {
+    if (!loads || n_replicas == 0) return -1;
+    int best = -1;
+    bool best_room = false;
+    double best_depth = 0;
+    uint64_t best_free = 0;
+    // replicas in cyclic order from `first`: on a full tie the earliest wins,
+    // so a caller that advances `first` spreads ties over the replicas
+    for (uint32_t k = 0; k < n_replicas; k++) {
+        const uint32_t i = (first + k) % n_replicas;
+        const ZkMsmReplicaLoad& l = loads[i];
+        if (!l.has_table || request_points > l.table_points || request_bytes > l.budget_bytes) continue;
+        const double speed = l.relative_speed > 0 ? l.relative_speed : 1.0;
+        const double depth = (double)(l.queued_points + request_points) / speed;
+        const uint64_t free_b = l.budget_bytes > l.in_use_bytes ? l.budget_bytes - l.in_use_bytes : 0;
+        const bool room = free_b >= request_bytes;
+        // a replica with room for the request now beats one without; then the
+        // shallower queue (in points, scaled by speed); then more free memory
+        bool better = best < 0 || (room && !best_room) ||
+                      (room == best_room && (depth < best_depth || (depth == best_depth && free_b > best_free)));
+        if (better) {
+            best = (int)i;
+            best_room = room;
+            best_depth = depth;
+            best_free = free_b;
+        }
+    }
+    return best;
+}
+
+ZkMetalStatus zkmsm_pool_create(const ZkMsmServer* servers, uint32_t n_servers, ZkMsmPool* out) {
+    if (!servers || !out || n_servers == 0 || n_servers > 64) return ZKMETAL_ERR_INVALID_INPUT;
+    std::unique_ptr<Pool> p(new Pool());
+    for (uint32_t i = 0; i < n_servers; i++) {
+        if (!servers[i]) return ZKMETAL_ERR_INVALID_INPUT;
+        p->reps.push_back(static_cast<Server*>(servers[i]));
+    }
+    p->routed.assign(n_servers, 0);
+    *out = p.release();
+    return ZKMETAL_SUCCESS;
+}
+
+ZkMetalStatus zkmsm_pool_submit(ZkMsmPool pool, int curve, const void* scalars, int scalar_fmt, uint32_t n_points,
+                                uint64_t* request_id) {
+    if (!pool || !request_id || (curve != ZKMSM_BN254 && curve != ZKMSM_BLS12_381)) return ZKMETAL_ERR_INVALID_INPUT;
+    Pool& p = *static_cast<Pool*>(pool);
+    const uint32_t R = (uint32_t)p.reps.size();
+    std::vector<ZkMsmReplicaLoad> loads(R);
+    for (uint32_t i = 0; i < R; i++) {
+        Server& s = *p.reps[i];
+        std::lock_guard<std::mutex> lk(s.mu);
+        loads[i].has_table = s.has_table[curve] ? 1 : 0;
+        loads[i].table_points = s.has_table[curve] ? s.tables[curve].n : 0;
+        loads[i].queued_points = s.queued_points;
+        loads[i].budget_bytes = s.budget;
+        loads[i].in_use_bytes = s.in_use;
+        loads[i].relative_speed = 1.0;
+    }
+    const uint64_t bytes = Server::estimate(curve, n_points);
+    uint32_t first;
+    {
+        std::lock_guard<std::mutex> lk(p.mu);
+        first = p.rr++ % R;
+    }
+    // the best replica first; on refusal (e.g. the budget changed) the next best
+    for (uint32_t tries = 0; tries < R; tries++) {
+        const int pick = zkmsm_route_pick(loads.data(), R, n_points, bytes, first);
+        if (pick < 0) break;
+        uint64_t sid = 0;
+        const ZkMetalStatus st = zkmsm_server_submit(p.reps[pick], curve, scalars, scalar_fmt, n_points, &sid);
+        if (st == ZKMETAL_SUCCESS) {
+            std::lock_guard<std::mutex> lk(p.mu);
+            const uint64_t id = p.next_id++;
+            p.ids[id] = {(uint32_t)pick, sid};
+            p.routed[pick]++;
+            *request_id = id;
+            return ZKMETAL_SUCCESS;
+        }
+        if (st != ZKMETAL_ERR_BUSY) return st;
+        loads[pick].has_table = 0;
+    }
+    set_error("no replica can take the request (no table for the curve, table too short, or over every budget)");
+    return ZKMETAL_ERR_BUSY;
+}
+
+ZkMetalStatus zkmsm_pool_wait(ZkMsmPool pool, uint64_t request_id, int timeout_ms, uint8_t* result,
+                              double* latency_ms) {
+    if (!pool) return ZKMETAL_ERR_INVALID_INPUT;
+    Pool& p = *static_cast<Pool*>(pool);
+    std::pair<uint32_t, uint64_t> where;
+    {
+        std::lock_guard<std::mutex> lk(p.mu);
+        auto it = p.ids.find(request_id);
+        if (it == p.ids.end()) return ZKMETAL_ERR_INVALID_INPUT;
+        where = it->second;
+    }
+    const ZkMetalStatus st = zkmsm_server_wait(p.reps[where.first], where.second, timeout_ms, result, latency_ms);
+    if (st != ZKMETAL_ERR_BUSY || timeout_ms < 0) {
+        std::lock_guard<std::mutex> lk(p.mu);
+        p.ids.erase(request_id);
+    }
+    return st;
+}
+
+ZkMetalStatus zkmsm_pool_stats(ZkMsmPool pool, char* buf, uint64_t buflen) {
+    if (!pool || !buf || !buflen) return ZKMETAL_ERR_INVALID_INPUT;
+    Pool& p = *static_cast<Pool*>(pool);
+    std::string js = "{\"replicas\":[";
+    for (size_t i = 0; i < p.reps.size(); i++) {
+        char tmp[1024];
+        if (zkmsm_server_stats(p.reps[i], tmp, sizeof tmp) != ZKMETAL_SUCCESS) return ZKMETAL_ERR_INVALID_INPUT;
+        uint64_t routed;
+        {
+            std::lock_guard<std::mutex> lk(p.mu);
+            routed = p.routed[i];
+        }
+        std::string one(tmp);
+        one.insert(1, "\"routed\":" + std::to_string(routed) + ",\"device\":" + std::to_string(p.reps[i]->device) +
+                              ",");
+        js += (i ? "," : "") + one;
+    }
+    js += "]}";
+    if (js.size() + 1 > buflen) return ZKMETAL_ERR_INVALID_INPUT;
+    memcpy(buf, js.c_str(), js.size() + 1);
+    return ZKMETAL_SUCCESS;
+}
+
+void zkmsm_pool_destroy(ZkMsmPool pool) { delete static_cast<Pool*>(pool); }
 
 ZkMetalStatus zkmsm_server_create(ZkMsmTable bn254_table, ZkMsmTable bls12_381_table, uint64_t hbm_budget_bytes,
                                   int workers, uint64_t max_batch_points, ZkMsmServer* out) {
@@ -338,6 +485,7 @@ ZkMetalStatus zkmsm_server_submit(ZkMsmServer server, int curve, const void* sca
         r->id = s.next_id++;
         s.all[r->id] = r;
         s.pending.push_back(r);
+        s.queued_points += n_points;
     }
     s.cv_work.notify_one();
     *request_id = r->id;
@@ -353,6 +501,7 @@ ZkMetalStatus zkmsm_server_cancel(ZkMsmServer server, uint64_t request_id) {
     auto& r = it->second;
     if (r->status != 1) return ZKMETAL_ERR_BUSY;  // already running or done
     s.pending.erase(std::remove(s.pending.begin(), s.pending.end(), r), s.pending.end());
+    s.queued_points -= r->n;
     r->status = ZKMETAL_ERR_BUSY;
     r->t_done = Clock::now();
     s.cv_done.notify_all();

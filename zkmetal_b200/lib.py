@@ -30,6 +30,30 @@ SCALAR_INT = 0
 SCALAR_MONT = 1
 
 FP_BYTES = {BN254: 32, BLS12_381: 48, BLS12_377: 48, BN254_G2: 64}  # bytes per coordinate
+# base-field moduli (the curves' published parameters)
+FP_MODULUS = {
+    BN254: 0x30644e72e131a029b85045b68181585d97816a916871ca8d3c208c16d87cfd47,
+    BLS12_381: int("1a0111ea397fe69a4b1ba7b6434bacd764774b84f38512bf6730d2a0f6b0f624"
+                   "1eabfffeb153ffffb9feffffffffaaab", 16),
+    BLS12_377: int("1ae3a4617c510eac63b05c06ca1493b1a22d9f300f5138f1ef3622fba094800"
+                   "170b5d44300000008508c00000000001", 16),
+}
+
+
+class ReplicaLoad(ctypes.Structure):
+    """ZkMsmReplicaLoad (include/zkmsm.h): one replica's state for routing."""
+    _fields_ = [("has_table", ctypes.c_int32), ("table_points", ctypes.c_uint64),
+                ("queued_points", ctypes.c_uint64), ("budget_bytes", ctypes.c_uint64),
+                ("in_use_bytes", ctypes.c_uint64), ("relative_speed", ctypes.c_double)]
+
+
+def mont_one(curve):
+    """1 in the Montgomery form of the curve's coordinate field (R mod p,
+    R = 2^(bits of a coordinate)); for BN254 G2 the Fp2 element 1 + 0u."""
+    if curve == BN254_G2:
+        return ((1 << 256) % FP_MODULUS[BN254]).to_bytes(32, "little") + bytes(32)
+    fb = FP_BYTES[curve]
+    return ((1 << (8 * fb)) % FP_MODULUS[curve]).to_bytes(fb, "little")
 
 c_u8p = ctypes.c_void_p
 c_vp = ctypes.c_void_p
@@ -88,6 +112,12 @@ _SIGS = {
     "zkmsm_server_stats": (c_i32, [c_vp, ctypes.c_char_p, c_u64]),
     "zkmsm_server_inject_failures": (c_i32, [c_vp, c_int]),
     "zkmsm_server_destroy": (None, [c_vp]),
+    "zkmsm_route_pick": (c_int, [c_vp, c_u32, c_u32, c_u64, c_u32]),
+    "zkmsm_pool_create": (c_i32, [c_vp, c_u32, ctypes.POINTER(c_vp)]),
+    "zkmsm_pool_submit": (c_i32, [c_vp, c_int, c_vp, c_int, c_u32, ctypes.POINTER(c_u64)]),
+    "zkmsm_pool_wait": (c_i32, [c_vp, c_u64, c_int, c_vp, ctypes.POINTER(ctypes.c_double)]),
+    "zkmsm_pool_stats": (c_i32, [c_vp, ctypes.c_char_p, c_u64]),
+    "zkmsm_pool_destroy": (None, [c_vp]),
     "zkmsm_autotune": (c_i32, [c_vp, c_int, c_int, c_int, ctypes.c_char_p, c_u64]),
     "zkmsm_tuning_save": (c_i32, [c_vp, ctypes.c_char_p]),
     "zkmsm_tuning_load": (c_i32, [c_vp, ctypes.c_char_p]),
@@ -95,6 +125,7 @@ _SIGS = {
     "zkmsm_gen_scalars": (c_i32, [c_vp, c_int, c_u64, c_u64, c_u64, c_int, c_int, c_vp]),
     "zkmsm_engine_launch_count": (c_u64, [c_vp]),
     "zkmsm_engine_last_entries": (c_u64, [c_vp]),
+    "zkmsm_msm_batch": (c_i32, [c_vp, c_int, c_vp, c_vp, c_int, c_vp, c_u32, c_vp]),
     "zkmsm_plan_describe": (c_i32, [c_int, c_vp, c_u32, c_int, c_int, c_int, c_int, c_int, ctypes.c_char_p, c_u64]),
     "zkmsm_plan_describe_shift": (c_i32, [c_int, c_vp, c_u32, c_int, c_int, c_int, c_u32, ctypes.c_char_p, c_u64]),
     "zkmsm_engine_profile": (c_i32, [c_vp, c_int]),

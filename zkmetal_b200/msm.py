@@ -5,7 +5,9 @@ Same names, argument meaning and errors as the reference engines, so code
 
 * ``MetalMSM().msm(points, scalars)``        MSM/MSMEngine.swift:17, 287
 * ``BLS12381MSM().msm / msmFr``               MSM/BLS12381MSMEngine.swift:10, 260, 517
-* ``multiMSM(engine, points, scalar_sets)``  MSM/MultiMSM.swift:21-72
+* ``multiMSM(engine, points, scalar_sets | frScalarSets=)``, ``multiMSMPipelined``,
+  ``innerProductMSM``, ``innerProductMSMHalves``, ``batchMSMAsync`` / ``MSMTask``
+                                               MSM/MultiMSM.swift:21-260
 * ``MSMError`` (noGPU, invalidInput, gpuError) MSM/MSMEngine.swift:8-15
 
 Points are the reference byte layout (affine, Montgomery, little endian);
@@ -193,23 +195,136 @@ class BN254G2MSM(_Engine):
         return self._call(_l.lib().zkmetal_bn254_g2_msm_fr, p, s, n)
 
 
-def multiMSM(engine, points, scalar_sets):
+def _identity(curve):
+    """The reference's pointIdentity() (PointOperations.swift:40-42): (1, 1, 0)
+    with 1 in Montgomery form."""
+    fb = _l.FP_BYTES[curve]
+    one = _l.mont_one(curve)
+    return PointProjective(one, one, bytes(fb))
+
+
+def _batch(engine, points, scalars, counts, fmt):
+    """One zkmsm_msm_batch call: MSM i over the i-th run of counts[i] points
+    and scalars; empty runs give the identity."""
+    fb = _l.FP_BYTES[engine.curve]
+    counts = np.ascontiguousarray(np.asarray(counts, dtype=np.uint32))
+    out = ctypes.create_string_buffer(len(counts) * 3 * fb)
+    _raise_for(_l.lib().zkmsm_msm_batch(engine.handle, engine.curve, points.ctypes.data, scalars.ctypes.data, fmt,
+                                        counts.ctypes.data, len(counts), out))
+    raw = out.raw
+    res = []
+    for i, c in enumerate(counts):
+        if c == 0:
+            res.append(_identity(engine.curve))
+        else:
+            o = i * 3 * fb
+            res.append(PointProjective(raw[o:o + fb], raw[o + fb:o + 2 * fb], raw[o + 2 * fb:o + 3 * fb]))
+    return res
+
+
+def multiMSM(engine, points, scalar_sets=None, frScalarSets=None):
     """k MSMs over the same bases (MultiMSM.swift:21-72), run as one batch.
 
-    The reference runs them one after another; here they are one batch over a
-    resident copy of the bases.
+    ``scalar_sets``: k integer scalar vectors (8 x u32 each); or
+    ``frScalarSets``: k Montgomery Fr vectors (the ``multiMSM(engine:points:
+    frScalarSets:)`` overload, MultiMSM.swift:63-72; the conversion runs on
+    the device).  The reference runs the k MSMs one after another; here they
+    are one batch over a resident copy of the bases.  No sets -> [];
+    mismatched lengths -> MSMError("invalidInput").
     """
+    if (scalar_sets is None) == (frScalarSets is None):
+        raise MSMError("invalidInput", "give exactly one of scalar_sets / frScalarSets")
+    fmt = _l.SCALAR_INT if frScalarSets is None else _l.SCALAR_MONT
+    sets = scalar_sets if frScalarSets is None else frScalarSets
+    if len(sets) == 0:
+        return []
     fb = _l.FP_BYTES[engine.curve]
     p = as_bytes_array(points, 2 * fb)
     n = p.size // (2 * fb)
-    sets = [as_bytes_array(s, 32) for s in scalar_sets]
-    if not sets or any(s.size // 32 != n for s in sets) or n == 0:
+    sets = [as_bytes_array(s, 32) for s in sets]
+    if any(s.size // 32 != n for s in sets) or n == 0:
         raise MSMError("invalidInput", "empty or mismatched scalar sets")
     table = CommitmentTable(engine, p)
     try:
-        return table.batch_commit(np.concatenate(sets), [n] * len(sets))
+        return table.batch_commit(np.concatenate(sets), [n] * len(sets), fmt=fmt)
     finally:
         table.close()
+
+
+def multiMSMPipelined(engine, points, scalar_sets):
+    """MultiMSM.swift:250-260: the same k MSMs over shared bases; the
+    reference delegates to multiMSM, and so does this (the batch already
+    shares one sort, accumulation and reduction across the k MSMs)."""
+    return multiMSM(engine, points, scalar_sets)
+
+
+def innerProductMSM(engine, points, scalars, partitions, fr=False):
+    """Partitioned MSM for IPA rounds (MultiMSM.swift:90-128):
+    result[j] = MSM(points[p[j]:p[j+1]], scalars[p[j]:p[j+1]]), all parts in
+    one batch.  ``partitions`` must be non-decreasing, start at 0 and end at
+    n, with at least two boundaries; an empty part gives the identity.
+    ``fr``: scalars are Montgomery Fr."""
+    fb = _l.FP_BYTES[engine.curve]
+    p = as_bytes_array(points, 2 * fb)
+    s = as_bytes_array(scalars, 32)
+    n = p.size // (2 * fb)
+    parts = [int(x) for x in partitions]
+    if s.size // 32 != n or len(parts) < 2 or parts[0] != 0 or parts[-1] != n:
+        raise MSMError("invalidInput", "points/scalars mismatch or partitions not [0, ..., n]")
+    if any(b < a for a, b in zip(parts, parts[1:])):
+        raise MSMError("invalidInput", "partitions must be non-decreasing")
+    counts = [b - a for a, b in zip(parts, parts[1:])]
+    if n == 0:
+        return [_identity(engine.curve) for _ in counts]
+    return _batch(engine, p, s, counts, _l.SCALAR_MONT if fr else _l.SCALAR_INT)
+
+
+def innerProductMSMHalves(engine, points, scalars, fr=False):
+    """(MSM over [0, n/2), MSM over [n/2, n)) -- MultiMSM.swift:134-150;
+    n < 2 -> MSMError("invalidInput")."""
+    fb = _l.FP_BYTES[engine.curve]
+    n = as_bytes_array(points, 2 * fb).size // (2 * fb)
+    if n < 2:
+        raise MSMError("invalidInput", "need at least two points")
+    l, r = innerProductMSM(engine, points, scalars, [0, n // 2, n], fr=fr)
+    return l, r
+
+
+@dataclass
+class MSMTask:
+    """One MSM of batchMSMAsync (MultiMSM.swift:155-172): points with integer
+    ``scalars`` or Montgomery ``frScalars``."""
+    points: object
+    scalars: object = None
+    frScalars: object = None
+
+
+def batchMSMAsync(engine, tasks):
+    """Independent MSMs (MultiMSM.swift:175-246), all in one batch per scalar
+    form instead of the reference's sequential GPU loop.  Results in task
+    order; no tasks -> []; a task with no points or mismatched counts ->
+    MSMError("invalidInput")."""
+    if len(tasks) == 0:
+        return []
+    fb = _l.FP_BYTES[engine.curve]
+    groups = {}
+    for i, t in enumerate(tasks):
+        if (t.scalars is None) == (t.frScalars is None):
+            raise MSMError("invalidInput", "task %d: give exactly one of scalars / frScalars" % i)
+        p = as_bytes_array(t.points, 2 * fb)
+        s = as_bytes_array(t.scalars if t.frScalars is None else t.frScalars, 32)
+        n = p.size // (2 * fb)
+        if n == 0 or s.size // 32 != n:
+            raise MSMError("invalidInput", "task %d: empty or points/scalars count mismatch" % i)
+        fmt = _l.SCALAR_INT if t.frScalars is None else _l.SCALAR_MONT
+        groups.setdefault(fmt, []).append((i, p, s, n))
+    out = [None] * len(tasks)
+    for fmt, items in groups.items():
+        res = _batch(engine, np.concatenate([it[1] for it in items]), np.concatenate([it[2] for it in items]),
+                     [it[3] for it in items], fmt)
+        for it, r in zip(items, res):
+            out[it[0]] = r
+    return out
 
 
 class CommitmentTable:
@@ -371,3 +486,72 @@ class CommitmentServer:
         except Exception:
             pass
 
+
+
+class CommitmentServerPool:
+    """Request-level replicas for serving on several GPUs (new API): one
+    ``CommitmentServer`` per device, each over its own resident tables, and
+    every request routed whole to one of them by queue depth and free HBM
+    (``zkmsm_route_pick``).  No collective: nothing crosses GPUs.  The pool
+    does not own the servers; close it before them."""
+
+    def __init__(self, servers):
+        if not servers:
+            raise MSMError("invalidInput", "no servers")
+        arr = (ctypes.c_void_p * len(servers))(*[s._h.value for s in servers])
+        h = ctypes.c_void_p()
+        _raise_for(_l.lib().zkmsm_pool_create(arr, len(servers), ctypes.byref(h)))
+        self._h = h
+        self._servers = list(servers)
+        self._keep = {}
+        self._curve = {}
+
+    def submit(self, curve, scalars, fmt=_l.SCALAR_INT):
+        s = as_bytes_array(scalars, 32)
+        rid = ctypes.c_uint64()
+        _raise_for(_l.lib().zkmsm_pool_submit(self._h, curve, s.ctypes.data, fmt, s.size // 32, ctypes.byref(rid)))
+        self._keep[rid.value] = s
+        self._curve[rid.value] = curve
+        return rid.value
+
+    def wait(self, rid, timeout_ms=-1):
+        fb = _l.FP_BYTES[self._curve[rid]]
+        out = ctypes.create_string_buffer(3 * fb)
+        lat = ctypes.c_double()
+        st = _l.lib().zkmsm_pool_wait(self._h, rid, timeout_ms, out, ctypes.byref(lat))
+        if st != _l.ERR_BUSY or timeout_ms < 0:
+            self._keep.pop(rid, None)
+            self._curve.pop(rid, None)
+        _raise_for(st)
+        raw = out.raw
+        return PointProjective(raw[:fb], raw[fb:2 * fb], raw[2 * fb:3 * fb]), lat.value
+
+    def stats(self):
+        import json
+        buf = ctypes.create_string_buffer(1 << 16)
+        _raise_for(_l.lib().zkmsm_pool_stats(self._h, buf, len(buf)))
+        return json.loads(buf.value.decode())
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _l.lib().zkmsm_pool_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def route_pick(loads, request_points, request_bytes, first=0):
+    """The pool's routing rule on host data (no GPU): ``loads`` is a list of
+    dicts with the ZkMsmReplicaLoad fields; full ties go to the first replica
+    in cyclic order from ``first``.  Returns a replica index or -1."""
+    arr = (_l.ReplicaLoad * max(1, len(loads)))()
+    for i, d in enumerate(loads):
+        for k, v in d.items():
+            setattr(arr[i], k, v)
+        if "relative_speed" not in d:
+            arr[i].relative_speed = 1.0
+    return _l.lib().zkmsm_route_pick(arr, len(loads), int(request_points), int(request_bytes), int(first))
