@@ -130,9 +130,16 @@ def reduction_products(plan, curve="bn254"):
 
 def sort_bytes(n, entries, plan):
     """DRAM bytes the scalar preparation and radix sort move by design: the
-    scalars once, the entries written by the digit kernel, read and written by
-    every scatter pass, read by every histogram pass after the first (8 B per
-    entry), and the per-tile histograms through their scans."""
+    scalars once and the entries written by the digit kernel; then per MSD
+    pass the entries read by the count kernel and read and written by the
+    scatter (24 B per entry), or per LSD pass read and written by the scatter
+    and read by every histogram pass after the first; and the per-tile
+    histograms written once and read and written by their scans."""
+    msd = plan.get("msd", [0])
+    if msd[0]:
+        passes, b1, b2, t1, t2 = msd
+        hist = (1 << b1) * t1 * 4 + ((1 << b2) * t2 * 4 if passes == 2 else 0)
+        return 32 * n + 8 * entries + passes * 24 * entries + 5 * hist
     passes, bits, tiles = plan["sort"][2], plan["sort"][3], plan["sort"][4]
     hist = (1 << bits) * tiles * 4
     return 32 * n + 8 * entries + passes * 16 * entries + max(0, passes - 1) * 8 * entries + passes * 3 * hist

@@ -268,9 +268,10 @@ void zkmsm_server_destroy(ZkMsmServer server);
  * Routing (zkmsm_route_pick): among replicas holding a table for the curve
  * that is long enough and a budget that can ever hold the request, one with
  * free budget for it now beats one without; then the shallowest queue
- * (points submitted and not finished, divided by relative_speed); then the
- * most free budget; then the first in cyclic order from `first` (the pool
- * advances it with every request, so ties rotate over the replicas).  The
+ * (points submitted and not finished, divided by relative_speed); among
+ * replicas that all lack room, then the most free budget; then the first in
+ * cyclic order from `first` (the pool advances it with every request, so
+ * ties rotate over the replicas).  The
  * pool does not own the servers: destroy the pool first.  Ids are the
  * pool's own. */
 typedef struct {
@@ -300,6 +301,20 @@ void zkmsm_pool_destroy(ZkMsmPool pool);
  * window_bits >= 2^16 is a two-width layout c | nlo << 16: nlo windows of
  * c bits, then (c + 1)-bit windows up to the scalar width. */
 ZkMetalStatus zkmsm_engine_set_tuning(ZkMetalMSMEngine engine, int window_bits, int chunk, int glv);
+/* NEW: window layout from a sample of the scalars (on by default).  For a
+ * single MSM of at least 2^20 points on a GLV curve, with no window width
+ * forced or autotuned for its size, the engine first profiles 4096 of the
+ * scalars on the device (bit lengths of their prepared halves) and picks the
+ * window layout that minimises sorted entries plus bucket-reduction work for
+ * that profile: skewed scalar sets (many zeros, ones or short values) get
+ * fewer, narrower buckets; uniform ones keep the layout chosen from n.  The
+ * result never depends on it.  The sample makes the call wait for the work
+ * already queued on its stream (also in zkmsm_msm_device_async; skipped while
+ * the stream is being captured).  The reference samples a window-0 bucket
+ * histogram for its window choice (MSM/MSMEngine.swift:565-593, 768-783).
+ * enable: 1 on, 0 off. */
+ZkMetalStatus zkmsm_engine_set_sampling(ZkMetalMSMEngine engine, int enable);
+
 /* NEW: host-buffer MSMs (zkmetal_*_msm and their _fr forms) are streamed in
  * stripes (consecutive point ranges from 2^(stripe_log2-2) points, growing
  * 1.6x per stripe up to 2^stripe_log2): each stripe's host-to-device copy

@@ -221,13 +221,13 @@ def test_replica_pool_routes_and_matches_plain(eng):
             reps.append(CommitmentServer(tabs[-2], tabs[-1], workers=2))
         pool = CommitmentServerPool(reps)
         rng = random.Random(5)
-        reqs, ids = [], []
+        reqs = []
         for i in range(40):
             curve = "bn254" if rng.random() < 0.7 else "bls12_381"
             n = rng.randint(1, T)
-            sc = scalars_host(eng[curve], curve, 350 + i, n, "uniform" if i % 2 else "witness")
-            reqs.append((curve, n, sc))
-            ids.append(pool.submit(0 if curve == "bn254" else 1, sc, zl.SCALAR_MONT))
+            reqs.append((curve, n, scalars_host(eng[curve], curve, 350 + i, n, "uniform" if i % 2 else "witness")))
+        # all submitted before the first wait, so the replicas' queues fill
+        ids = [pool.submit(0 if c == "bn254" else 1, sc, zl.SCALAR_MONT) for c, _, sc in reqs]
         for (curve, n, sc), rid in zip(reqs, ids):
             r, _ = pool.wait(rid)
             assert r.x + r.y + r.z == plain(eng[curve], curve, pts[curve], sc, n)

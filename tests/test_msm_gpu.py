@@ -395,3 +395,28 @@ def test_dropin_pinned_buffers_overlap(eng, curve, n):
         sh.copy_(s.cpu())
         check(fn(e.handle, ph.data_ptr(), sh.data_ptr(), n, rx, ry, rz))
         assert rx.raw + ry.raw + rz.raw == msm_device(e, curve, p, s, zl.SCALAR_MONT, n), seed
+
+
+@pytest.mark.parametrize("dist", ["uniform", "witness"])
+def test_sampled_layout_same_result(eng, dist):
+    """The window layout chosen from a sample of the scalars (on by default
+    from 2^20 points) changes the schedule, never the result: device calls
+    (synchronous and on a stream) and a drop-in host call with sampling on
+    equal the call with sampling off."""
+    e = eng["bn254"]
+    n = (1 << 20) + 123
+    p, s = gen_inputs(e, "bn254", 881, n, dist, zl.SCALAR_MONT)
+    L = zl.lib()
+    check(L.zkmsm_engine_set_sampling(e.handle, 0))
+    want = msm_device(e, "bn254", p, s, zl.SCALAR_MONT, n)
+    check(L.zkmsm_engine_set_sampling(e.handle, 1))
+    assert msm_device(e, "bn254", p, s, zl.SCALAR_MONT, n) == want
+    out = torch.zeros(96, dtype=torch.uint8, device="cuda")
+    stream = torch.cuda.Stream()
+    torch.cuda.synchronize()
+    check(L.zkmsm_msm_device_async(e.handle, 0, p.data_ptr(), None, s.data_ptr(), zl.SCALAR_MONT, n, out.data_ptr(),
+                                   ctypes.c_void_p(stream.cuda_stream)))
+    stream.synchronize()
+    assert out.cpu().numpy().tobytes() == want
+    r = e.msmFr(to_host(p), to_host(s))
+    assert r.x + r.y + r.z == want

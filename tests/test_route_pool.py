@@ -6,9 +6,9 @@ tables; a request goes whole to one replica.  The rule: replicas without a
 table for the curve, with a table shorter than the request or with a budget
 that can never hold it are skipped; one with free budget for the request now
 beats one without; then the shallowest queue (points submitted and not
-finished, divided by the replica's relative speed); then the most free
-budget; then the first replica in cyclic order from a rotating start (so full ties
-spread over the replicas).
+finished, divided by the replica's relative speed); among replicas that all
+lack room, then the most free budget; then the first replica in cyclic order
+from a rotating start (so full ties spread over the replicas).
 """
 import random
 
@@ -48,8 +48,12 @@ def test_free_memory_now_beats_a_shallower_queue():
     # neither has room now: the shallower queue waits for memory
     assert route_pick([rep(queued=9, budget=8 * GB, in_use=7 * GB), rep(queued=5, budget=8 * GB, in_use=7 * GB)],
                       10, 2 * GB) == 1
-    # equal depth: more free budget
-    assert route_pick([rep(in_use=3 * GB), rep(in_use=GB)], 10, GB) == 1
+    # equal depth, neither with room: more free budget
+    assert route_pick([rep(budget=8 * GB, in_use=7 * GB), rep(budget=8 * GB, in_use=int(6.5 * GB))], 10,
+                      2 * GB) == 1
+    # equal depth, both with room: the rotation decides, not the free budget
+    assert route_pick([rep(in_use=3 * GB), rep(in_use=GB)], 10, GB) == 0
+    assert route_pick([rep(in_use=3 * GB), rep(in_use=GB)], 10, GB, first=1) == 1
 
 
 def test_relative_speed_scales_the_queue():

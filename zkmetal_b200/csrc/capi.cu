@@ -239,13 +239,12 @@ static ZkMetalStatus msm_host(Engine& e, const uint8_t* points, const uint8_t* s
         // the scalars go first on the engine stream and the bases on the
         // copy stream: the scalar preparation and sort, which read only the
         // scalars, run while the bases arrive
-        Plan& pl = e.get_plan<C>({n}, {0}, fmt, scalar_bits);
-        const bool glv = pl.descs[0].glv;
+        Plan* pl = &e.get_plan<C>({n}, {0}, fmt, scalar_bits);
+        const bool glv = pl->descs[0].glv;
         bool grew = e.w_points.ensure((size_t)n * 2 * fb + 16);
         grew |= e.w_scalars.ensure((size_t)n * 32 + 16);
         if (glv) grew |= e.w_phi.ensure((size_t)n * 2 * fb + 16);
         if (grew) e.drop_graphs();
-        e.ensure_workspace<C>(pl);
         e.ensure_copy_resources(2);
         // buffers (re)allocated in the engine stream's order: the copy waits for that
         ZK_CUDA(cudaEventRecord(e.copy_events[0], e.stream));
@@ -253,12 +252,18 @@ static ZkMetalStatus msm_host(Engine& e, const uint8_t* points, const uint8_t* s
         ZK_CUDA(cudaMemcpyAsync(e.w_scalars.p, scalars, (size_t)n * 32, cudaMemcpyHostToDevice, e.stream));
         ZK_CUDA(cudaMemcpyAsync(e.w_points.p, points, (size_t)n * 2 * fb, cudaMemcpyHostToDevice, e.copy_stream));
         ZK_CUDA(cudaEventRecord(e.copy_events[1], e.copy_stream));
+        // window layout from a sample of the scalars (the bases keep arriving)
+        if (!scalar_bits && glv) {
+            const auto sl = e.sampled_layout<C>(e.w_scalars.as<uint32_t>(), n, fmt);
+            if (sl.window) pl = &e.get_plan<C>({n}, {0}, fmt, 0, sl.window, {}, sl.entries);
+        }
+        e.ensure_workspace<C>(*pl);
         Engine::BasesWait bw;
         bw.ready = e.copy_events[1];
         bw.phi_n = glv ? n : 0;
         bw.phi_out = glv ? e.w_phi.as<uint32_t>() : nullptr;
         const uint32_t* phi = glv ? e.w_phi.as<uint32_t>() : e.w_points.as<uint32_t>();
-        e.enqueue<C>(pl, e.w_points.as<uint32_t>(), phi, e.w_scalars.as<uint32_t>(), e.w_results.as<uint32_t>(), 0,
+        e.enqueue<C>(*pl, e.w_points.as<uint32_t>(), phi, e.w_scalars.as<uint32_t>(), e.w_results.as<uint32_t>(), 0,
                      nullptr, &bw);
         ZK_CUDA(cudaMemcpyAsync(out, e.w_results.p, 3 * P::N * 4, cudaMemcpyDeviceToHost, e.stream));
         ZK_CUDA(cudaStreamSynchronize(e.stream));
@@ -653,7 +658,8 @@ ZkMetalStatus zkmsm_msm_device(ZkMetalMSMEngine engine, int curve, const void* d
         const uint32_t* sc = static_cast<const uint32_t*>(d_scalars);
         with_curve(curve, [&](auto cv) {
             using C = decltype(cv);
-            Plan& pl = e.get_plan<C>({n}, {0}, fmt);
+            const auto sl = e.sampled_layout<C>(sc, n, fmt);
+            Plan& pl = e.get_plan<C>({n}, {0}, fmt, 0, sl.window, {}, sl.entries);
             e.w_phi.ensure((size_t)n * 2 * fp_bytes(curve) + 16);
             e.make_phi<C>(pts, n, e.w_phi.as<uint32_t>());
             e.run_device<C>(pl, pts, e.w_phi.as<uint32_t>(), sc, result);
@@ -682,7 +688,8 @@ ZkMetalStatus zkmsm_msm_device_async(ZkMetalMSMEngine engine, int curve, const v
         uint32_t* res = static_cast<uint32_t*>(d_result);
         with_curve(curve, [&](auto cv) {
             using C = decltype(cv);
-            Plan& pl = e.get_plan<C>({n}, {0}, fmt);
+            const auto sl = e.sampled_layout<C>(sc, n, fmt);
+            Plan& pl = e.get_plan<C>({n}, {0}, fmt, 0, sl.window, {}, sl.entries);
             e.ensure_workspace<C>(pl);
             if (!phi) {
                 e.w_phi.ensure((size_t)n * 2 * fp_bytes(curve) + 16);
@@ -866,6 +873,12 @@ ZkMetalStatus zkmsm_engine_set_tuning(ZkMetalMSMEngine engine, int window_bits, 
     return ZKMETAL_SUCCESS;
 }
 
+ZkMetalStatus zkmsm_engine_set_sampling(ZkMetalMSMEngine engine, int enable) {
+    if (!engine || enable < 0 || enable > 1) return ZKMETAL_ERR_INVALID_INPUT;
+    ENG(engine).scalar_sampling = enable;
+    return ZKMETAL_SUCCESS;
+}
+
 ZkMetalStatus zkmsm_engine_set_stripe(ZkMetalMSMEngine engine, int stripe_log2) {
     if (!engine || stripe_log2 < -1 || stripe_log2 > 30) return ZKMETAL_ERR_INVALID_INPUT;
     ENG(engine).stripe_log2 = stripe_log2;
@@ -941,7 +954,9 @@ static ZkMetalStatus plan_json(int curve, const uint32_t* counts, uint32_t n_msm
         s += "],\"entry_bound\":" + std::to_string(pl.entry_bound) + ",\"nbuckets\":" + std::to_string(pl.nbuckets) +
              ",\"sort\":[" + std::to_string(pl.sort_maxd) + "," + std::to_string(pl.sort_spb) + "," +
              std::to_string(pl.sort_passes) + "," + std::to_string(pl.sort_bits) + "," +
-             std::to_string(pl.sort_tiles) + "],\"acc\":[";
+             std::to_string(pl.sort_tiles) + "],\"msd\":[" + std::to_string(pl.msd_passes) + "," +
+             std::to_string(pl.msd_bits1) + "," + std::to_string(pl.msd_bits2) + "," + std::to_string(pl.msd_tiles1) +
+             "," + std::to_string(pl.msd_tiles2) + "],\"acc\":[";
         for (size_t l = 0; l < pl.acc_K.size(); l++)
             s += (l ? "," : "") + std::string("[") + std::to_string(pl.acc_K[l]) + "," + std::to_string(pl.acc_T[l]) +
                  "," + std::to_string(pl.acc_Mbound[l]) + "]";

@@ -122,6 +122,10 @@ struct Plan {
     // per scalar, sort_spb scalars per digit block, sort_passes passes of
     // sort_bits-bit digits over sort_tiles tiles of SORT_ETILE entries
     uint32_t sort_maxd = 0, sort_spb = 0, sort_passes = 0, sort_bits = 0, sort_tiles = 0;
+    // MSD sort instead (msd_passes 1 or 2; 0: the LSD passes above): digit
+    // widths of the passes (the first takes the top bits), tile-count
+    // bounds of the passes (pass 2: one partial tile more per segment)
+    uint32_t msd_passes = 0, msd_bits1 = 0, msd_bits2 = 0, msd_tiles1 = 0, msd_tiles2 = 0;
     // segmented-sum levels: chunk length and chunk-count bound per level
     std::vector<uint32_t> acc_K, acc_T;
     std::vector<uint64_t> acc_Mbound;
@@ -140,6 +144,7 @@ struct Plan {
         total_scalars = entry_bound = 0;
         nbuckets = nwin_total = 0;
         sort_maxd = sort_spb = sort_passes = sort_bits = sort_tiles = 0;
+        msd_passes = msd_bits1 = msd_bits2 = msd_tiles1 = msd_tiles2 = 0;
         acc_K.clear();
         acc_T.clear();
         acc_Mbound.clear();
@@ -209,6 +214,69 @@ inline WinLayout choose_layout(uint64_t entries_per_window, uint32_t bits) {
         }
     }
     return best;
+}
+
+// Nonzero signed digits of one scalar half of bit length b under a layout:
+// one per window that starts below bit b, and one more for the carry out of
+// the top such window when b reaches that window's top bit (its digit is
+// then above 2^(width-1) and is recoded with a carry into the next window).
+inline double layout_digits(uint32_t b, uint32_t c, uint32_t nlo, uint32_t nwin) {
+    uint32_t k = 0, end = 0;
+    for (uint32_t w = 0; w < nwin; w++) {
+        const uint32_t start = w * c + (w > nlo ? w - nlo : 0u);
+        if (start < b) {
+            k++;
+            end = start + c + (w >= nlo ? 1u : 0u);
+        }
+    }
+    if (k && k < nwin && b == end) k++;
+    return (double)k;
+}
+
+// The window layout for an MSM of n scalars whose sampled half lengths are
+// `hist` (k_scalar_profile; `halves` = sampled halves in total): the cost of
+// choose_layout with the entry count taken from the sample instead of every
+// digit being nonzero, over the two-width layouts and equal windows of 4..22
+// bits.  Scalar sets with many zero, one or short values then get fewer,
+// narrower buckets (BN254 witness-like scalars at 2^24: 7 windows of 19 bits
+// rather than 6 of 21-22).  Returns c | nlo << 16 (nlo = 0: equal windows).
+inline uint32_t choose_layout_sampled(const uint32_t* hist, uint64_t halves, uint64_t n, uint32_t bits,
+                                      uint32_t halves_per_scalar, uint64_t* expected_entries = nullptr) {
+    const uint32_t cover = bits + 1;
+    double best_cost = 1e300, best_entries = 0;
+    uint32_t best = 0;
+    auto consider = [&](uint32_t c, uint32_t nlo, uint32_t nwin, double buckets) {
+        double per_half = 0;
+        for (uint32_t b = 0; b < PROFILE_BINS; b++)
+            if (hist[b]) per_half += (double)hist[b] * layout_digits(b, c, nlo, nwin);
+        const double entries = (double)n * halves_per_scalar * per_half / (double)std::max<uint64_t>(1, halves);
+        const double cost = entries + 3.0 * buckets + 2.0e5 * (c + 6) + 4.0e4 * (double)nwin * c;
+        if (cost < best_cost) {
+            best_cost = cost;
+            best_entries = entries;
+            best = c | (nlo < nwin ? nlo << 16 : 0u);
+        }
+    };
+    for (uint32_t W = 1; W <= cover; W++) {  // two-width layouts, as choose_layout
+        const uint32_t c = cover / W, nhi = cover - W * c;
+        if (c < 2) break;
+        if (c + (nhi ? 1 : 0) > 22) continue;
+        consider(c, W - nhi, W, (double)(W - nhi) * (double)(1u << (c - 1)) + (double)nhi * (double)(1u << c));
+    }
+    for (uint32_t c = 4; c <= 22; c++) {  // equal windows
+        const uint32_t W = windows_for(bits, c);
+        consider(c, W, W, (double)W * (double)(1u << (c - 1)));
+    }
+    if (expected_entries) *expected_entries = (uint64_t)best_entries;
+    return best;
+}
+
+// Expected sorted entries of a sampled MSM, rounded to a power of 2^(1/8)
+// (so that similar samples share one cached plan).
+inline uint64_t quantize_entries(uint64_t e) {
+    if (e < 16) return 16;
+    const double q = std::round(std::log2((double)e) * 8.0) / 8.0;
+    return (uint64_t)std::exp2(q);
 }
 
 // Window width for an MSM over a shift table with spacing s (copy k of the
@@ -303,6 +371,11 @@ class Engine {
     std::vector<std::vector<cudaEvent_t>> prof_pending;
     double phase_ms[NPHASE] = {0, 0, 0, 0, 0};
     uint64_t phase_calls = 0;
+    // Sample the scalars of MSMs of at least 2^20 points and choose their
+    // window layout from the sample (k_scalar_profile); 0 = layout from n
+    // alone.  Sampling waits for the stream the call runs on.
+    int scalar_sampling = 1;
+    static constexpr uint64_t SAMPLE_MIN_POINTS = 1ull << 20;
     std::vector<cudaEvent_t> prof_begin() {
         std::vector<cudaEvent_t> ev;
         if (!profile) return ev;
@@ -333,9 +406,10 @@ class Engine {
 
     // workspace
     DevBuf w_points, w_phi, w_scalars, w_counts, w_offsets, w_cursor, w_ents, w_buckets;
-    DevBuf w_ents2, w_thist, w_stripe_buckets;
+    DevBuf w_ents2, w_thist, w_stripe_buckets, w_seg;
     DevBuf w_cnt, w_pos, w_tiles, w_totals, w_pkeys[2], w_pvals[2], w_redS[2], w_redW[2];
-    DevBuf w_results, w_comb;
+    DevBuf w_results, w_comb, w_profile;
+    uint32_t* h_profile = nullptr;  // pinned, PROFILE_BINS words
     bool comb_ready[NCURVES] = {};
     uint32_t* h_results = nullptr;  // pinned
     size_t h_results_cap = 0;
@@ -345,9 +419,10 @@ class Engine {
     // setting, e.g. a server's reservation, is left as it is).
     void bind_workspace_stream() {
         DevBuf* bufs[] = {&w_points, &w_phi, &w_scalars, &w_counts, &w_offsets, &w_cursor, &w_ents, &w_buckets,
-                          &w_ents2, &w_thist, &w_stripe_buckets, &w_cnt, &w_pos, &w_tiles, &w_totals,
+                          &w_ents2, &w_thist, &w_stripe_buckets, &w_seg, &w_cnt, &w_pos, &w_tiles, &w_totals,
                           &w_pkeys[0], &w_pkeys[1], &w_pvals[0], &w_pvals[1], &w_redS[0], &w_redS[1],
-                          &w_redW[0], &w_redW[1], &w_results, &w_comb, &transient.d_descs, &transient.d_tasks};
+                          &w_redW[0], &w_redW[1], &w_results, &w_comb, &w_profile, &transient.d_descs,
+                          &transient.d_tasks};
         for (DevBuf* b : bufs) b->sp = &stream;
         cudaMemPool_t pool;
         if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
@@ -388,13 +463,15 @@ class Engine {
         if (copy_stream) cudaStreamDestroy(copy_stream);
         if (stream) cudaStreamDestroy(stream);
         if (h_results) cudaFreeHost(h_results);
+        if (h_profile) cudaFreeHost(h_profile);
     }
 
     // ------------------------------------------------------------ planning
     template <class C>
     void make_plan(Plan& pl, const std::vector<uint32_t>& counts, const std::vector<uint32_t>& base_offs,
-                   int fmt, uint32_t scalar_bits, uint32_t window_override = 0, ShiftSpec sh = {}) const {
-        plan_shape<C>(pl, tuning, counts, base_offs, fmt, scalar_bits, window_override, sh);
+                   int fmt, uint32_t scalar_bits, uint32_t window_override = 0, ShiftSpec sh = {},
+                   uint64_t entries_hint = 0) const {
+        plan_shape<C>(pl, tuning, counts, base_offs, fmt, scalar_bits, window_override, sh, entries_hint);
     }
 
     // Pure host planning (no device needed): window widths, bucket layout,
@@ -404,9 +481,12 @@ class Engine {
     // striped MSM share one bucket layout).  `sh`: the bases are a shift
     // table; an MSM whose points lie in it uses the precomputed shifts (no
     // GLV, window width a multiple of sh.bits, one bucket set).
+    // entries_hint: the expected number of sorted entries (from a scalar
+    // sample; 0: unknown, every digit counted as nonzero): sizes the level-1
+    // chunks for the entries there will be rather than for the bound.
     static void plan_shape(Plan& pl, const Tuning& tuning, const std::vector<uint32_t>& counts,
                            const std::vector<uint32_t>& base_offs, int fmt, uint32_t scalar_bits,
-                           uint32_t window_override = 0, ShiftSpec sh = {}) {
+                           uint32_t window_override = 0, ShiftSpec sh = {}, uint64_t entries_hint = 0) {
         pl.curve = CurveTraits<C>::id;
         uint64_t soff = 0;
         uint32_t boff = 0, woff = 0;
@@ -502,6 +582,15 @@ class Engine {
             pl.sort_passes = passes;
             pl.sort_bits = passes ? (kb + passes - 1) / passes : 0;
             pl.sort_tiles = (uint32_t)std::max<uint64_t>((pl.entry_bound + SORT_ETILE - 1) / SORT_ETILE, 1);
+            // large entry sets: MSD passes of up to 12 bits (two cover bucket
+            // ids of up to 24 bits), the first pass over the top bits
+            if (pl.entry_bound >= MSD_MIN_ENTRIES && kb >= 1 && kb <= 2 * MSD_MAX_BITS) {
+                pl.msd_passes = kb <= MSD_MAX_BITS ? 1 : 2;
+                pl.msd_bits1 = pl.msd_passes == 1 ? kb : (kb + 1) / 2;
+                pl.msd_bits2 = kb - (pl.msd_passes == 1 ? kb : pl.msd_bits1);
+                pl.msd_tiles1 = (uint32_t)((pl.entry_bound + MSD_TILE - 1) / MSD_TILE);
+                pl.msd_tiles2 = pl.msd_passes == 2 ? pl.msd_tiles1 + (1u << pl.msd_bits1) : 0;
+            }
         }
         // segmented-sum levels
         uint64_t M = pl.entry_bound;
@@ -512,8 +601,11 @@ class Engine {
             // small: at 2^24 with ~24 entries per bucket, chunks of 192 beat
             // chunks of 48 by 0.9 ms), short enough to give at least 8 waves
             // of resident threads
-            uint64_t waves8 = M / (8ull * 148 * 512);
-            uint64_t avg = pl.nbuckets ? M / pl.nbuckets : 1;
+            // (a hint within 10% of the bound is the bound: dense scalar sets
+            // keep the plan they get without a sample)
+            const uint64_t Me = entries_hint && entries_hint < M - M / 10 ? entries_hint : M;
+            uint64_t waves8 = Me / (8ull * 148 * 512);
+            uint64_t avg = pl.nbuckets ? Me / pl.nbuckets : 1;
             uint64_t k = std::min<uint64_t>(std::max<uint64_t>(8, waves8), std::max<uint64_t>(192, 2 * avg));
             K1 = (uint32_t)std::min<uint64_t>(k, 512);
             // then round the thread count to a whole number of waves of
@@ -521,9 +613,9 @@ class Engine {
             // almost idle device for a full chunk time
             const uint64_t W = tuning.acc_wave[CurveTraits<C>::id];
             if (W) {
-                const double waves = (double)M / ((double)K1 * (double)W);
+                const double waves = (double)Me / ((double)K1 * (double)W);
                 const uint64_t w = (uint64_t)(waves + 0.5);
-                if (waves >= 1.0 && w >= 1) K1 = (uint32_t)std::max<uint64_t>(8, (M + w * W - 1) / (w * W));
+                if (waves >= 1.0 && w >= 1) K1 = (uint32_t)std::max<uint64_t>(8, (Me + w * W - 1) / (w * W));
             }
         }
         uint32_t K = K1;
@@ -582,13 +674,15 @@ class Engine {
 
     template <class C>
     Plan& get_plan(const std::vector<uint32_t>& counts, const std::vector<uint32_t>& base_offs, int fmt,
-                   uint32_t scalar_bits = 0, uint32_t window_override = 0, ShiftSpec sh = {}) {
+                   uint32_t scalar_bits = 0, uint32_t window_override = 0, ShiftSpec sh = {},
+                   uint64_t entries_hint = 0) {
         std::string key;
         auto put = [&](uint64_t v) { key.append(reinterpret_cast<const char*>(&v), sizeof v); };
         put(CurveTraits<C>::id);
         put(fmt);
         put(scalar_bits);
         put(window_override);
+        put(entries_hint);
         put((uint64_t)sh.bits << 32 | sh.points);
         put((uint64_t)(uint32_t)tuning.window_bits << 32 | (uint32_t)tuning.chunk);
         put((uint64_t)(int64_t)tuning.glv);
@@ -602,7 +696,7 @@ class Engine {
             plan_cache.clear();
         }
         std::unique_ptr<Plan> pl(new Plan());
-        make_plan<C>(*pl, counts, base_offs, fmt, scalar_bits, window_override, sh);
+        make_plan<C>(*pl, counts, base_offs, fmt, scalar_bits, window_override, sh, entries_hint);
         upload_plan(*pl, false);
         Plan& ref = *pl;
         plan_cache.emplace(key, std::move(pl));
@@ -654,7 +748,12 @@ class Engine {
         grew |= w_counts.ensure(((size_t)pl.nbuckets + 1) * 4);
         grew |= w_cursor.ensure(((size_t)pl.nbuckets + 1) * 4);
         grew |= w_ents.ensure(pl.entry_bound * 8 + 16);
-        const uint64_t hsz = (uint64_t)(1u << pl.sort_bits) * pl.sort_tiles;
+        uint64_t hsz = (uint64_t)(1u << pl.sort_bits) * pl.sort_tiles;
+        if (pl.msd_passes) {
+            hsz = std::max<uint64_t>((uint64_t)(1u << pl.msd_bits1) * pl.msd_tiles1,
+                                     pl.msd_passes == 2 ? (uint64_t)(1u << pl.msd_bits2) * pl.msd_tiles2 : 0);
+            grew |= w_seg.ensure(((size_t)2 << pl.msd_bits1) * 4 + 64);
+        }
         grew |= w_ents2.ensure(pl.entry_bound * 8 + 16);
         grew |= w_thist.ensure(hsz * 4 + 16);
         grew |= w_buckets.ensure((size_t)pl.nbuckets * xs + xs);
@@ -721,6 +820,9 @@ class Engine {
     template <class C>
     void enqueue_reduce(const Plan& pl, const void* bucket_base, uint32_t* d_results,
                         std::vector<cudaEvent_t>* ev = nullptr);
+    // MSD sort of the entries (k_msd_*), defined in engine_impl.cuh
+    template <class C>
+    void msd_sort(const Plan& pl, uint2* A, uint2* B, uint32_t* tot);
     template <class C>
     void fold_buckets(void* base, uint32_t nb, uint32_t S);
     template <class C>
@@ -735,6 +837,39 @@ class Engine {
     uint32_t acc_resident_threads();
     template <class C>
     void gen_bases(uint64_t seed, uint64_t index0, uint64_t n, uint32_t* d_out);
+    // Histogram of the prepared half lengths of PROFILE_SAMPLES scalars of
+    // d_scalars (k_scalar_profile) into h_profile; waits for the stream.
+    template <class C>
+    void profile_scalars(const uint32_t* d_scalars, uint64_t n, int fmt, bool glv);
+    // The window override (c | nlo << 16) and the expected entry count for a
+    // single n-point MSM of device scalars, chosen from a sample of them; {0,
+    // 0} (layout from n alone) unless sampling is on, n >= SAMPLE_MIN_POINTS,
+    // the curve splits with GLV, no window width is forced or autotuned for
+    // n, and the stream is not being captured into a graph.
+    struct SampledLayout {
+        uint32_t window = 0;
+        uint64_t entries = 0;
+    };
+    template <class C>
+    SampledLayout sampled_layout(const uint32_t* d_scalars, uint64_t n, int fmt) {
+        SampledLayout out;
+        if (!scalar_sampling || n < SAMPLE_MIN_POINTS || !CurveTraits<C>::glv || tuning.glv == 0 ||
+            tuning.window_bits != 0)
+            return out;
+        if (tuning.window_table.count({CurveTraits<C>::id * 2 + 1, nearest_log2(n)})) return out;
+        cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+        if (cudaStreamIsCapturing(stream, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) {
+            cudaGetLastError();
+            return out;
+        }
+        profile_scalars<C>(d_scalars, n, fmt, true);
+        uint64_t halves = 0;
+        for (uint32_t b = 0; b < PROFILE_BINS; b++) halves += h_profile[b];
+        uint64_t e = 0;
+        out.window = choose_layout_sampled(h_profile, halves, n, CurveTraits<C>::half_bits, 2, &e);
+        out.entries = quantize_entries(e);
+        return out;
+    }
     template <class C>
     void gen_scalars(uint64_t seed, uint64_t index0, uint64_t n, int dist, int fmt, uint32_t* d_out);
 
@@ -814,10 +949,12 @@ class Engine {
     EXT template void Engine::enqueue_reduce<C>(const Plan&, const void*, uint32_t*,                     \
                                                 std::vector<cudaEvent_t>*);                             \
     EXT template void Engine::fold_buckets<C>(void*, uint32_t, uint32_t);                               \
+    EXT template void Engine::msd_sort<C>(const Plan&, uint2*, uint2*, uint32_t*);                     \
     EXT template void Engine::make_phi<C>(const uint32_t*, uint64_t, uint32_t*);                        \
     EXT template void Engine::make_shifts<C>(uint32_t*, uint64_t, uint32_t, uint32_t);                  \
     EXT template uint32_t Engine::acc_resident_threads<C>();                                              \
     EXT template void Engine::gen_bases<C>(uint64_t, uint64_t, uint64_t, uint32_t*);                    \
+    EXT template void Engine::profile_scalars<C>(const uint32_t*, uint64_t, int, bool);                 \
     EXT template void Engine::gen_scalars<C>(uint64_t, uint64_t, uint64_t, int, int, uint32_t*);
 
 }  // namespace zkmsm

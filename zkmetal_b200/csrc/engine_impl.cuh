@@ -4,6 +4,7 @@
 #include "engine.cuh"
 #include "msm_kernels.cuh"
 
+#include <mutex>
 #include <stdexcept>
 #include <utility>
 
@@ -28,6 +29,54 @@ static void scan_u32(Engine& e, uint32_t* d_in_out, uint32_t n, uint32_t* d_tota
 }
 
 
+// MSD sort of the entries in A by bucket id (tot[0] entries): one or two
+// passes, each k_msd_count, an exclusive scan of the tile counts and
+// k_msd_scatter; after two passes the result is back in A, after one in B.
+static void msd_scatter_attr(int device) {
+    // the staged tile needs more than the default 48 KB of dynamic shared
+    // memory; set once per device for this unit's copy of the kernel
+    static std::mutex mu;
+    static bool done[64] = {};
+    std::lock_guard<std::mutex> lk(mu);
+    if (device < 0 || device >= 64 || done[device]) return;
+    ZK_CUDA(cudaFuncSetAttribute(k_msd_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)MSD_SCATTER_SMEM));
+    done[device] = true;
+}
+
+template <class C>
+void Engine::msd_sort(const Plan& pl, uint2* A, uint2* B, uint32_t* tot) {
+    msd_scatter_attr(device);
+    uint32_t* H = w_thist.as<uint32_t>();
+    const uint32_t b1 = pl.msd_bits1, b2 = pl.msd_bits2, t1 = pl.msd_tiles1, t2 = pl.msd_tiles2;
+    const uint32_t shift1 = pl.msd_passes == 2 ? b2 : 0;
+    k_msd_count<<<t1, MSD_THREADS, 0, stream>>>(A, tot + 0, shift1, b1, t1, nullptr, nullptr, 0, H);
+    launches++;
+    ZK_CUDA(cudaGetLastError());
+    scan_u32(*this, H, (1u << b1) * t1, tot + 63, nullptr);
+    k_msd_scatter<<<t1, MSD_THREADS, MSD_SCATTER_SMEM, stream>>>(A, tot + 0, shift1, b1, t1, nullptr, nullptr, 0, H,
+                                                                    B);
+    launches++;
+    ZK_CUDA(cudaGetLastError());
+    if (pl.msd_passes < 2) return;
+    const uint32_t nseg = 1u << b1;
+    uint32_t* seg_start = w_seg.as<uint32_t>();
+    uint32_t* seg_tile = seg_start + nseg + 1;
+    k_msd_tiles<<<1, MSD_THREADS, 0, stream>>>(H, t1, nseg, tot + 0, seg_start, seg_tile);
+    launches++;
+    ZK_CUDA(cudaGetLastError());
+    // pass-2 counts occupy a prefix of H (tiles in segment order); the scan
+    // runs over the bound and whatever lies past the prefix only shifts
+    // slots past it
+    k_msd_count<<<t2, MSD_THREADS, 0, stream>>>(B, tot + 0, 0, b2, 0, seg_start, seg_tile, nseg, H);
+    launches++;
+    ZK_CUDA(cudaGetLastError());
+    scan_u32(*this, H, (1u << b2) * t2, tot + 63, nullptr);
+    k_msd_scatter<<<t2, MSD_THREADS, MSD_SCATTER_SMEM, stream>>>(B, tot + 0, 0, b2, 0, seg_start, seg_tile, nseg, H,
+                                                                    A);
+    launches++;
+    ZK_CUDA(cudaGetLastError());
+}
+
 // ------------------------------------------------------------ pipeline
 // Enqueue the whole batch; results (n_msms x 3 field elements) land in
 // d_results.  No host synchronisation inside (graph capturable).
@@ -46,20 +95,25 @@ void Engine::enqueue(const Plan& pl, const uint32_t* d_bases, const uint32_t* d_
     // The digit pass writes to whichever buffer makes the last pass land in
     // w_ents; slot 63 of w_totals takes the (unused) totals of the scans.
     ZK_CUDA(cudaMemsetAsync(tot, 0, 4, stream));
-    uint2* bufA = (pl.sort_passes & 1) ? w_ents2.as<uint2>() : w_ents.as<uint2>();
-    uint2* bufB = (pl.sort_passes & 1) ? w_ents.as<uint2>() : w_ents2.as<uint2>();
-    // the first pass's tile histogram is counted by the digit kernel
-    if (pl.sort_passes)
-        ZK_CUDA(cudaMemsetAsync(w_thist.p, 0, (size_t)(1u << pl.sort_bits) * pl.sort_tiles * 4, stream));
+    const uint32_t npass = pl.msd_passes ? pl.msd_passes : pl.sort_passes;
+    uint2* bufA = (npass & 1) ? w_ents2.as<uint2>() : w_ents.as<uint2>();
+    uint2* bufB = (npass & 1) ? w_ents.as<uint2>() : w_ents2.as<uint2>();
+    // the first LSD pass's tile histogram is counted by the digit kernel
+    const bool hist0 = pl.sort_passes && !pl.msd_passes;
+    if (hist0) ZK_CUDA(cudaMemsetAsync(w_thist.p, 0, (size_t)(1u << pl.sort_bits) * pl.sort_tiles * 4, stream));
     if (pl.total_scalars) {
         const uint64_t g = (pl.total_scalars + pl.sort_spb - 1) / pl.sort_spb;
         k_radix_digits<C><<<(unsigned)g, SORT_DTHREADS, 0, stream>>>(
                 d_scalars, dd, nd, pl.total_scalars, pl.sort_spb, bufA, tot + 0,
-                pl.sort_passes ? w_thist.as<uint32_t>() : nullptr, pl.sort_bits, pl.sort_tiles);
+                hist0 ? w_thist.as<uint32_t>() : nullptr, pl.sort_bits, pl.sort_tiles);
         launches++;
         ZK_CUDA(cudaGetLastError());
     }
-    for (uint32_t ps = 0; ps < pl.sort_passes; ps++) {
+    if (pl.msd_passes) {
+        msd_sort<C>(pl, bufA, bufB, tot);
+        bufA = bufB = nullptr;
+    }
+    for (uint32_t ps = 0; ps < (pl.msd_passes ? 0u : pl.sort_passes); ps++) {
         const uint32_t shift = ps * pl.sort_bits, nt = pl.sort_tiles;
         if (ps > 0) {
             k_radix_hist<<<nt, SORT_ETHREADS, 0, stream>>>(bufA, tot + 0, shift, pl.sort_bits, nt,
@@ -243,6 +297,22 @@ void Engine::gen_bases(uint64_t seed, uint64_t index0, uint64_t n, uint32_t* d_o
     if (n) k_gen_bases<C><<<(unsigned)((n + 127) / 128), 128, 0, stream>>>(tab, d_out, n, seed, index0);
     launches += (n) ? 1 : 0;
     ZK_CUDA(cudaGetLastError());
+    ZK_CUDA(cudaStreamSynchronize(stream));
+}
+
+template <class C>
+void Engine::profile_scalars(const uint32_t* d_scalars, uint64_t n, int fmt, bool glv) {
+    w_profile.ensure(PROFILE_BINS * 4);
+    if (!h_profile) ZK_CUDA(cudaMallocHost(&h_profile, PROFILE_BINS * 4));
+    ZK_CUDA(cudaMemsetAsync(w_profile.p, 0, PROFILE_BINS * 4, stream));
+    const uint32_t m = (uint32_t)std::min<uint64_t>(n, PROFILE_SAMPLES);
+    if (m) {
+        k_scalar_profile<C><<<(m + 255) / 256, 256, 0, stream>>>(d_scalars, n, m, (uint32_t)fmt, glv ? 1u : 0u,
+                                                                  w_profile.as<uint32_t>());
+        launches++;
+        ZK_CUDA(cudaGetLastError());
+    }
+    ZK_CUDA(cudaMemcpyAsync(h_profile, w_profile.p, PROFILE_BINS * 4, cudaMemcpyDeviceToHost, stream));
     ZK_CUDA(cudaStreamSynchronize(stream));
 }
 

@@ -274,6 +274,31 @@ __global__ void __launch_bounds__(256) k_digit_hist(const uint32_t* __restrict__
     }
 }
 
+// Scalar profile: the bit lengths of the prepared halves (after the
+// Montgomery reduce or mod-r reduction and the GLV split) of m scalars spread
+// evenly over [0, n): hist[b] counts halves of bit length b.  The host turns
+// it into the expected number of nonzero digits of a window layout, so that
+// skewed scalar sets (many zeros, ones or short scalars) get a layout with
+// fewer buckets.  The reference samples a window-0 bucket histogram for the
+// same purpose (MSM/MSMEngine.swift:565-593, 768-783).
+template <class C>
+__global__ void __launch_bounds__(256) k_scalar_profile(const uint32_t* __restrict__ scalars, uint64_t n, uint32_t m,
+                                                        uint32_t fmt, uint32_t glv, uint32_t* __restrict__ hist) {
+    const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= m) return;
+    const uint64_t i = (uint64_t)j * n / m;
+    Halves h;
+    prepare_scalar<C>(h, scalars + i * 8, fmt, glv);
+#pragma unroll 1
+    for (int k = 0; k < h.count; k++) {
+        uint32_t b = 0;
+#pragma unroll
+        for (int l = 0; l < 9; l++)
+            if (h.k[k][l]) b = 32u * l + 32u - __clz(h.k[k][l]);
+        atomicAdd(hist + min(b, PROFILE_BINS - 1), 1u);
+    }
+}
+
 // Counting-sort scatter: entry = (global bucket id, base index | endo << 30 | negate << 31)
 template <class C>
 __global__ void __launch_bounds__(256) k_digit_scatter(const uint32_t* __restrict__ scalars,
@@ -1298,6 +1323,269 @@ static __global__ void __launch_bounds__(SCAN_THREADS) k_scan_add(uint32_t* __re
             out[j] = v;
             if (copy) copy[j] = v;
         }
+    }
+}
+
+// ------------------------------------------------------------ MSD radix sort
+// Large entry sets are sorted most-significant digit first, in two passes of
+// up to 12 bits (one pass for keys of up to 12 bits).  An MSD pass needs no
+// stability -- entries of one bucket may come out in any order, since bucket
+// sums do not depend on it -- so a tile ranks its entries by digit with
+// shared-memory atomics (one atomic per warp for a key the warp shares)
+// instead of the per-bit ballots the stable LSD passes above need.  Per
+// pass, over tiles of at most MSD_TILE entries that never straddle a
+// segment (pass 1: the whole array is one segment; pass 2: one segment per
+// pass-1 digit):
+//  k_msd_count    digit counts of every tile, stored segment by segment and
+//                 digit-major inside a segment: [seg][digit][tile of seg];
+//  scan           exclusive: that layout is the output order, so each
+//                 (seg, digit, tile) count becomes the tile's first slot;
+//  k_msd_tiles    (between the passes) the segment starts, read from the
+//                 pass-1 scan, and the pass-2 tile table;
+//  k_msd_scatter  counts again, places the tile in digit order in shared
+//                 memory, writes it out as one run per digit.
+// Replaces the reference's CPU counting sort per window (MSMEngine.swift:595-661).
+
+// Tile t of a pass.  Pass 1 (seg_tile == nullptr): [t*MSD_TILE, ...) of
+// [0, E), histogram laid out for `ntiles` tiles (tiles past E are empty and
+// count zeros).  Pass 2: the segment owning t in the tile table seg_tile
+// (exclusive prefix of tiles per segment, nseg + 1 entries) with segment
+// starts seg_start (nseg + 1 entries, the last one E).  False past the last
+// tile.
+struct MsdGeom {
+    uint32_t lo, hi, k, nt;
+    uint64_t hbase;
+};
+
+ZK_DEV bool msd_geom(uint32_t t, uint32_t E, uint32_t ntiles, const uint32_t* __restrict__ seg_start,
+                     const uint32_t* __restrict__ seg_tile, uint32_t nseg, uint32_t nb, MsdGeom& g) {
+    if (!seg_tile) {
+        if (t >= ntiles) return false;
+        const uint64_t lo = (uint64_t)t * MSD_TILE;
+        g.lo = (uint32_t)(lo < E ? lo : E);
+        g.hi = (uint32_t)(lo + MSD_TILE < E ? lo + MSD_TILE : E);
+        g.k = t;
+        g.nt = ntiles;
+        g.hbase = 0;
+        return true;
+    }
+    if (t >= seg_tile[nseg]) return false;
+    // the last segment whose first tile is at or below t (empty segments
+    // before it share its first-tile index and are skipped)
+    uint32_t a = 0, b = nseg - 1;
+    while (a < b) {
+        const uint32_t mid = (a + b + 1) >> 1;
+        if (seg_tile[mid] <= t) a = mid;
+        else b = mid - 1;
+    }
+    g.k = t - seg_tile[a];
+    g.nt = seg_tile[a + 1] - seg_tile[a];
+    g.hbase = (uint64_t)seg_tile[a] * nb;
+    g.lo = seg_start[a] + g.k * MSD_TILE;
+    const uint32_t end = seg_start[a + 1];
+    g.hi = g.lo + MSD_TILE < end ? g.lo + MSD_TILE : end;
+    return true;
+}
+
+// Exclusive scan over a block of NW warps (sh: NW words).
+template <int NW>
+ZK_DEV uint32_t block_excl_scan_w(uint32_t v, uint32_t* sh, uint32_t& total) {
+    const uint32_t lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    uint32_t x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= (uint32_t)o) x += y;
+    }
+    if (lane == 31) sh[wid] = x;
+    __syncthreads();
+    if (wid == 0) {
+        uint32_t s = lane < (uint32_t)NW ? sh[lane] : 0;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, s, o);
+            if (lane >= (uint32_t)o) s += y;
+        }
+        if (lane < (uint32_t)NW) sh[lane] = s;
+    }
+    __syncthreads();
+    total = sh[NW - 1];
+    const uint32_t pre = wid ? sh[wid - 1] : 0;
+    __syncthreads();
+    return pre + x - v;
+}
+
+// Shared-memory slot claim on ctr[key], the hot-key case aggregated as in
+// warp_count (lanes sharing the first valid lane's key take one atomic);
+// returns this lane's slot.  All 32 lanes of the warp call it together.
+ZK_DEV uint32_t warp_claim(uint32_t* __restrict__ ctr, bool valid, uint32_t key) {
+    const uint32_t lane = threadIdx.x & 31;
+    const uint32_t m = __ballot_sync(0xffffffffu, valid);
+    if (!m) return 0;
+    const uint32_t leader = __ffs(m) - 1;
+    const uint32_t lk = __shfl_sync(0xffffffffu, key, leader);
+    const bool grp = valid && key == lk;
+    const uint32_t same = __ballot_sync(0xffffffffu, grp);
+    uint32_t b = 0;
+    if (lane == leader) b = atomicAdd(ctr + lk, (uint32_t)__popc(same));
+    b = __shfl_sync(0xffffffffu, b, leader);
+    if (grp) return b + __popc(same & ((1u << lane) - 1));
+    return valid ? atomicAdd(ctr + key, 1u) : 0u;
+}
+
+constexpr uint32_t MSD_ROUNDS = (MSD_TILE + MSD_THREADS - 1) / MSD_THREADS;
+constexpr uint32_t MSD_BATCH = 8;  // keys loaded before they are counted
+static_assert(MSD_ROUNDS % MSD_BATCH == 0, "tile rounds come in whole load batches");
+
+// The block's digit counts of its tile into ctr (zeroed by the caller).
+ZK_DEV void msd_count_tile(const uint2* __restrict__ A, const MsdGeom& g, uint32_t shift, uint32_t mask,
+                           uint32_t* __restrict__ ctr) {
+    const uint32_t len = g.hi - g.lo;
+#pragma unroll 1
+    for (uint32_t r0 = 0; r0 < MSD_ROUNDS; r0 += MSD_BATCH) {
+        uint32_t key[MSD_BATCH];
+#pragma unroll
+        for (uint32_t q = 0; q < MSD_BATCH; q++) {
+            const uint32_t j = (r0 + q) * MSD_THREADS + threadIdx.x;
+            key[q] = j < len ? (A[(uint64_t)g.lo + j].x >> shift) & mask : 0xffffffffu;
+        }
+#pragma unroll
+        for (uint32_t q = 0; q < MSD_BATCH; q++) warp_count(ctr, key[q] != 0xffffffffu, key[q]);
+    }
+}
+
+static __global__ void __launch_bounds__(MSD_THREADS) k_msd_count(const uint2* __restrict__ A,
+                                                                 const uint32_t* __restrict__ d_total,
+                                                                 uint32_t shift, uint32_t bits, uint32_t ntiles,
+                                                                 const uint32_t* __restrict__ seg_start,
+                                                                 const uint32_t* __restrict__ seg_tile,
+                                                                 uint32_t nseg, uint32_t* __restrict__ H) {
+    __shared__ uint32_t cnt[1u << MSD_MAX_BITS];
+    const uint32_t nb = 1u << bits;
+    MsdGeom g;
+    if (!msd_geom(blockIdx.x, *d_total, ntiles, seg_start, seg_tile, nseg, nb, g)) return;
+    for (uint32_t i = threadIdx.x; i < nb; i += MSD_THREADS) cnt[i] = 0;
+    __syncthreads();
+    msd_count_tile(A, g, shift, nb - 1, cnt);
+    __syncthreads();
+    for (uint32_t d = threadIdx.x; d < nb; d += MSD_THREADS) H[g.hbase + (uint64_t)d * g.nt + g.k] = cnt[d];
+}
+
+// Between the passes (one block): seg_start[s] = first output slot of pass-1
+// digit s (the scanned count of (s, tile 0)), seg_start[nseg] = E; seg_tile =
+// exclusive prefix of ceil(segment length / MSD_TILE), nseg + 1 entries.
+static __global__ void __launch_bounds__(MSD_THREADS) k_msd_tiles(const uint32_t* __restrict__ H1s,
+                                                                 uint32_t ntiles1, uint32_t nseg,
+                                                                 const uint32_t* __restrict__ d_total,
+                                                                 uint32_t* __restrict__ seg_start,
+                                                                 uint32_t* __restrict__ seg_tile) {
+    __shared__ uint32_t sh[MSD_THREADS / 32];
+    const uint32_t E = *d_total;
+    constexpr uint32_t PER = (1u << MSD_MAX_BITS) / MSD_THREADS;
+    uint32_t st[PER + 1], nt[PER], sum = 0;
+#pragma unroll
+    for (uint32_t q = 0; q <= PER; q++) {
+        const uint32_t s = threadIdx.x * PER + q;
+        st[q] = s < nseg ? H1s[(uint64_t)s * ntiles1] : E;
+    }
+#pragma unroll
+    for (uint32_t q = 0; q < PER; q++) {
+        const uint32_t s = threadIdx.x * PER + q;
+        const uint32_t len = s < nseg ? st[q + 1] - st[q] : 0;
+        nt[q] = (len + MSD_TILE - 1) / MSD_TILE;
+        sum += nt[q];
+    }
+    uint32_t total;
+    uint32_t pre = block_excl_scan_w<MSD_THREADS / 32>(sum, sh, total);
+#pragma unroll
+    for (uint32_t q = 0; q < PER; q++) {
+        const uint32_t s = threadIdx.x * PER + q;
+        if (s < nseg) {
+            seg_start[s] = st[q];
+            seg_tile[s] = pre;
+        }
+        pre += nt[q];
+    }
+    if (threadIdx.x == 0) {
+        seg_start[nseg] = E;
+        seg_tile[nseg] = total;
+    }
+}
+
+// Dynamic shared memory of k_msd_scatter: the staged tile and two counters
+// per digit.
+constexpr size_t MSD_SCATTER_SMEM = (size_t)MSD_TILE * sizeof(uint2) + 2 * (1u << MSD_MAX_BITS) * sizeof(uint32_t);
+
+static __global__ void __launch_bounds__(MSD_THREADS) k_msd_scatter(const uint2* __restrict__ A,
+                                                                   const uint32_t* __restrict__ d_total,
+                                                                   uint32_t shift, uint32_t bits, uint32_t ntiles,
+                                                                   const uint32_t* __restrict__ seg_start,
+                                                                   const uint32_t* __restrict__ seg_tile,
+                                                                   uint32_t nseg, const uint32_t* __restrict__ Hs,
+                                                                   uint2* __restrict__ B) {
+    extern __shared__ uint4 msd_smem[];
+    uint2* stage = reinterpret_cast<uint2*>(msd_smem);
+    uint32_t* cur = reinterpret_cast<uint32_t*>(stage + MSD_TILE);
+    uint32_t* off = cur + (1u << MSD_MAX_BITS);
+    __shared__ uint32_t sh[MSD_THREADS / 32];
+    const uint32_t nb = 1u << bits, mask = nb - 1;
+    MsdGeom g;
+    if (!msd_geom(blockIdx.x, *d_total, ntiles, seg_start, seg_tile, nseg, nb, g)) return;
+    const uint32_t len = g.hi - g.lo;
+    if (len == 0) return;
+    for (uint32_t i = threadIdx.x; i < nb; i += MSD_THREADS) cur[i] = 0;
+    __syncthreads();
+    msd_count_tile(A, g, shift, mask, cur);
+    __syncthreads();
+    // local offsets of the digits (exclusive scan of the counts), counters reset
+    {
+        constexpr uint32_t PER = (1u << MSD_MAX_BITS) / MSD_THREADS;
+        uint32_t c[PER], sum = 0;
+#pragma unroll
+        for (uint32_t q = 0; q < PER; q++) {
+            const uint32_t d = threadIdx.x * PER + q;
+            c[q] = d < nb ? cur[d] : 0;
+            sum += c[q];
+        }
+        uint32_t total;
+        uint32_t pre = block_excl_scan_w<MSD_THREADS / 32>(sum, sh, total);
+#pragma unroll
+        for (uint32_t q = 0; q < PER; q++) {
+            const uint32_t d = threadIdx.x * PER + q;
+            if (d < nb) {
+                off[d] = pre;
+                cur[d] = 0;
+            }
+            pre += c[q];
+        }
+    }
+    __syncthreads();
+    // place the tile in digit order (the entries are read again, from L2)
+#pragma unroll 1
+    for (uint32_t r0 = 0; r0 < MSD_ROUNDS; r0 += MSD_BATCH) {
+        uint2 e[MSD_BATCH];
+#pragma unroll
+        for (uint32_t q = 0; q < MSD_BATCH; q++) {
+            const uint32_t j = (r0 + q) * MSD_THREADS + threadIdx.x;
+            e[q] = j < len ? A[(uint64_t)g.lo + j] : make_uint2(0, 0);
+        }
+#pragma unroll
+        for (uint32_t q = 0; q < MSD_BATCH; q++) {
+            const uint32_t j = (r0 + q) * MSD_THREADS + threadIdx.x;
+            const bool v = j < len;
+            const uint32_t d = v ? (e[q].x >> shift) & mask : 0u;
+            const uint32_t slot = warp_claim(cur, v, d);
+            if (v) stage[off[d] + slot] = e[q];
+        }
+    }
+    __syncthreads();
+    // global start of each digit's run, less its local offset
+    for (uint32_t d = threadIdx.x; d < nb; d += MSD_THREADS)
+        if (cur[d]) off[d] = Hs[g.hbase + (uint64_t)d * g.nt + g.k] - off[d];
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < len; i += MSD_THREADS) {
+        const uint2 v = stage[i];
+        B[(uint64_t)off[(v.x >> shift) & mask] + i] = v;
     }
 }
 

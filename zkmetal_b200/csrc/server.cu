@@ -293,9 +293,11 @@ int zkmsm_route_pick(const ZkMsmReplicaLoad* loads, uint32_t n_replicas, uint32_
         const uint64_t free_b = l.budget_bytes > l.in_use_bytes ? l.budget_bytes - l.in_use_bytes : 0;
         const bool room = free_b >= request_bytes;
         // a replica with room for the request now beats one without; then the
-        // shallower queue (in points, scaled by speed); then more free memory
+        // shallower queue (in points, scaled by speed); between replicas that
+        // all lack room, equal queues go to the one with more free memory
         bool better = best < 0 || (room && !best_room) ||
-                      (room == best_room && (depth < best_depth || (depth == best_depth && free_b > best_free)));
+                      (room == best_room &&
+                       (depth < best_depth || (depth == best_depth && !room && free_b > best_free)));
         if (better) {
             best = (int)i;
             best_room = room;

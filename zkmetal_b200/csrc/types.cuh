@@ -68,6 +68,21 @@ constexpr uint32_t SORT_ETILE = 4096;
 constexpr uint32_t SORT_ETHREADS = 256;
 constexpr uint32_t SORT_MAX_BINS = 256;
 
+// MSD radix sort of large entry sets (k_msd_count / k_msd_scatter): entries
+// per tile (staged whole in shared memory), threads per tile block, widest
+// digit per pass (2^12 bins), and the smallest entry bound sorted this way
+// (smaller batches take the LSD sort above, whose 4096-entry tiles keep more
+// blocks busy).
+constexpr uint32_t MSD_TILE = 24576;
+constexpr uint32_t MSD_THREADS = 1024;
+constexpr uint32_t MSD_MAX_BITS = 12;
+constexpr uint64_t MSD_MIN_ENTRIES = 1ull << 21;
+
+// Scalar profile for the window-layout choice (k_scalar_profile): bins of
+// the bit length (0..288) of a prepared scalar half, and sampled scalars.
+constexpr uint32_t PROFILE_BINS = 320;
+constexpr uint32_t PROFILE_SAMPLES = 4096;
+
 // Bucket-reduction levels with at most this many output nodes run the
 // inline-product kernel (few threads: latency-bound).
 constexpr uint32_t RED_INLINE_MAX_NODES = 32768;

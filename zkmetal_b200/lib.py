@@ -125,6 +125,7 @@ _SIGS = {
     "zkmsm_gen_scalars": (c_i32, [c_vp, c_int, c_u64, c_u64, c_u64, c_int, c_int, c_vp]),
     "zkmsm_engine_launch_count": (c_u64, [c_vp]),
     "zkmsm_engine_last_entries": (c_u64, [c_vp]),
+    "zkmsm_engine_set_sampling": (c_i32, [c_vp, c_int]),
     "zkmsm_msm_batch": (c_i32, [c_vp, c_int, c_vp, c_vp, c_int, c_vp, c_u32, c_vp]),
     "zkmsm_plan_describe": (c_i32, [c_int, c_vp, c_u32, c_int, c_int, c_int, c_int, c_int, ctypes.c_char_p, c_u64]),
     "zkmsm_plan_describe_shift": (c_i32, [c_int, c_vp, c_u32, c_int, c_int, c_int, c_u32, ctypes.c_char_p, c_u64]),
