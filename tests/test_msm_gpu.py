@@ -420,3 +420,24 @@ def test_sampled_layout_same_result(eng, dist):
     assert out.cpu().numpy().tobytes() == want
     r = e.msmFr(to_host(p), to_host(s))
     assert r.x + r.y + r.z == want
+
+
+@pytest.mark.parametrize("curve,n", [("bn254", (1 << 20) + 9), ("bn254", (1 << 21) + 3), ("bls12_381", 1 << 20)])
+def test_dropin_pageable_buffers_staged(eng, curve, n):
+    """Drop-in calls from pageable host arrays (what a Swift [PointAffine] or a
+    numpy array hands over): copies of 8 MB and more go through the engine's
+    pinned staging ring, filled by host threads chunk by chunk while earlier
+    chunks are on the bus.  Each call, unstriped and striped, equals the
+    device-pointer MSM, also when the arrays are refilled between calls."""
+    e = eng[curve]
+    C = R.CURVES[curve]
+    fn = {"bn254": zl.lib().zkmetal_bn254_msm_fr, "bls12_381": zl.lib().zkmetal_bls12_381_g1_msm_fr}[curve]
+    rx, ry, rz = (ctypes.create_string_buffer(C.fp_bytes) for _ in range(3))
+    ph = np.empty(n * 2 * C.fp_bytes, dtype=np.uint8)
+    sh = np.empty(n * 32, dtype=np.uint8)
+    for seed in (711, 712):
+        p, s = gen_inputs(e, curve, seed, n, "uniform" if seed == 711 else "witness", zl.SCALAR_MONT)
+        ph[:] = p.cpu().numpy()
+        sh[:] = s.cpu().numpy()
+        check(fn(e.handle, ph.ctypes.data, sh.ctypes.data, n, rx, ry, rz))
+        assert rx.raw + ry.raw + rz.raw == msm_device(e, curve, p, s, zl.SCALAR_MONT, n), seed

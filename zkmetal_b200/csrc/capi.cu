@@ -178,11 +178,9 @@ static void msm_host_striped(Engine& e, const uint8_t* points, const uint8_t* sc
     for (uint32_t s = 0; s < S; s++) {
         const size_t off = rg[s].first;
         const uint32_t cnt = rg[s].second;
-        ZK_CUDA(cudaMemcpyAsync(ds + off * 32, scalars + off * 32, (size_t)cnt * 32, cudaMemcpyHostToDevice,
-                                e.copy_stream));
+        e.copy_h2d(ds + off * 32, scalars + off * 32, (size_t)cnt * 32, e.copy_stream);
         ZK_CUDA(cudaEventRecord(e.copy_events[s], e.copy_stream));
-        ZK_CUDA(cudaMemcpyAsync(dp + off * pb, points + off * pb, (size_t)cnt * pb, cudaMemcpyHostToDevice,
-                                e.copy_stream));
+        e.copy_h2d(dp + off * pb, points + off * pb, (size_t)cnt * pb, e.copy_stream);
         ZK_CUDA(cudaEventRecord(e.copy_events[S + 1 + s], e.copy_stream));
         // the stripe's sort needs only its scalars; its bases are waited
         // for after the sort, before the endomorphism and the accumulation
@@ -249,8 +247,8 @@ static ZkMetalStatus msm_host(Engine& e, const uint8_t* points, const uint8_t* s
         // buffers (re)allocated in the engine stream's order: the copy waits for that
         ZK_CUDA(cudaEventRecord(e.copy_events[0], e.stream));
         ZK_CUDA(cudaStreamWaitEvent(e.copy_stream, e.copy_events[0], 0));
-        ZK_CUDA(cudaMemcpyAsync(e.w_scalars.p, scalars, (size_t)n * 32, cudaMemcpyHostToDevice, e.stream));
-        ZK_CUDA(cudaMemcpyAsync(e.w_points.p, points, (size_t)n * 2 * fb, cudaMemcpyHostToDevice, e.copy_stream));
+        e.copy_h2d(e.w_scalars.p, scalars, (size_t)n * 32, e.stream);
+        e.copy_h2d(e.w_points.p, points, (size_t)n * 2 * fb, e.copy_stream);
         ZK_CUDA(cudaEventRecord(e.copy_events[1], e.copy_stream));
         // window layout from a sample of the scalars (the bases keep arriving)
         if (!scalar_bits && glv) {

@@ -13,11 +13,15 @@
 
 #include <algorithm>
 #include <cmath>
+#include <condition_variable>
 #include <cstdint>
 #include <cstring>
+#include <functional>
 #include <map>
 #include <memory>
+#include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "types.cuh"
@@ -89,7 +93,125 @@ struct DevBuf {
     ~DevBuf() { release(); }
 };
 
-// Curves with an engine instantiation (CurveTraits<C>::id = 0 .. NCURVES - 1);
+// Host-to-device copies from pageable host memory.  The driver stages a
+// pageable copy through its own small pinned buffers on one thread (about
+// 10 GB/s here); a caller handing over plain arrays (a Swift [PointAffine],
+// a numpy array) would wait that long.  The stager instead copies chunks
+// into a ring of its own pinned buffers with several host threads and DMAs
+// each chunk from there on the caller's stream, the next chunk's host copy
+// running while the previous one is on the bus.  A buffer is refilled once
+// its DMA has completed (event).  Calls return when the last chunk is
+// queued, like a pageable cudaMemcpyAsync.
+class HostStager {
+   public:
+    static constexpr size_t CHUNK = 32u << 20;
+    static constexpr int SLOTS = 3;
+
+    ~HostStager() {
+        {
+            std::lock_guard<std::mutex> lk(mu_);
+            stop_ = true;
+        }
+        cv_.notify_all();
+        for (auto& t : workers_) t.join();
+        for (int i = 0; i < SLOTS; i++) {
+            if (done_[i]) cudaEventDestroy(done_[i]);
+            if (buf_[i]) cudaFreeHost(buf_[i]);
+        }
+    }
+
+    // dst (device) <- src (pageable host), enqueued on stream s
+    cudaError_t copy(void* dst, const void* src, size_t bytes, cudaStream_t s) {
+        cudaError_t e = init();
+        if (e != cudaSuccess) return e;
+        const uint8_t* sp = static_cast<const uint8_t*>(src);
+        uint8_t* dp = static_cast<uint8_t*>(dst);
+        for (size_t off = 0; off < bytes; off += CHUNK) {
+            const size_t len = std::min(CHUNK, bytes - off);
+            const int k = next_++ % SLOTS;
+            if ((e = cudaEventSynchronize(done_[k])) != cudaSuccess) return e;
+            parallel_memcpy(buf_[k], sp + off, len);
+            if ((e = cudaMemcpyAsync(dp + off, buf_[k], len, cudaMemcpyHostToDevice, s)) != cudaSuccess) return e;
+            if ((e = cudaEventRecord(done_[k], s)) != cudaSuccess) return e;
+        }
+        return cudaSuccess;
+    }
+
+    static bool pageable(const void* p) {
+        cudaPointerAttributes a;
+        if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+            cudaGetLastError();
+            return true;
+        }
+        return a.type == cudaMemoryTypeUnregistered;
+    }
+
+   private:
+    cudaError_t init() {
+        if (buf_[0]) return cudaSuccess;
+        for (int i = 0; i < SLOTS; i++) {
+            cudaError_t e = cudaMallocHost(&buf_[i], CHUNK);
+            if (e == cudaSuccess) e = cudaEventCreateWithFlags(&done_[i], cudaEventDisableTiming);
+            if (e != cudaSuccess) return e;
+        }
+        unsigned hw = std::thread::hardware_concurrency();
+        const int nt = (int)std::max(1u, std::min(8u, hw / 2));
+        for (int i = 0; i < nt; i++) workers_.emplace_back([this] { work(); });
+        return cudaSuccess;
+    }
+
+    void work() {
+        uint64_t seen = 0;
+        for (;;) {
+            std::function<void()> job;
+            {
+                std::unique_lock<std::mutex> lk(mu_);
+                cv_.wait(lk, [&] { return stop_ || (gen_ != seen && taken_ < parts_); });
+                if (stop_) return;
+                const size_t i = taken_++;
+                if (taken_ == parts_) seen = gen_;
+                job = [this, i] { part(i); };
+            }
+            job();
+            {
+                std::lock_guard<std::mutex> lk(mu_);
+                if (++finished_ == parts_) cv_done_.notify_all();
+            }
+        }
+    }
+
+    void part(size_t i) {
+        const size_t per = (len_ + parts_ - 1) / parts_;
+        const size_t a = std::min(len_, i * per), b = std::min(len_, a + per);
+        if (b > a) memcpy(static_cast<uint8_t*>(dst_) + a, static_cast<const uint8_t*>(src_) + a, b - a);
+    }
+
+    void parallel_memcpy(void* dst, const void* src, size_t len) {
+        std::unique_lock<std::mutex> lk(mu_);
+        dst_ = dst;
+        src_ = src;
+        len_ = len;
+        parts_ = workers_.size();
+        taken_ = finished_ = 0;
+        gen_++;
+        cv_.notify_all();
+        cv_done_.wait(lk, [&] { return finished_ == parts_; });
+    }
+
+    void* buf_[SLOTS] = {};
+    cudaEvent_t done_[SLOTS] = {};
+    uint64_t next_ = 0;
+    std::vector<std::thread> workers_;
+    std::mutex mu_;
+    std::condition_variable cv_, cv_done_;
+    bool stop_ = false;
+    uint64_t gen_ = 0;
+    void* dst_ = nullptr;
+    const void* src_ = nullptr;
+    size_t len_ = 0, parts_ = 0, taken_ = 0, finished_ = 0;
+};
+
+// Curves with an engine instantiation// Curves with an engine instantiation (CurveTraits<C>::id = 0 .. NCURVES - 1);
 // every per-curve array of the engine has this many entries.
 constexpr int NCURVES = 4;
 // widest coordinate of any curve, in 32-bit words (BN254 G2: two 8-word Fp)
@@ -457,7 +579,21 @@ class Engine {
             copy_events.push_back(ev);
         }
     }
+    // pageable host-to-device copies of the streamed host calls
+    std::unique_ptr<HostStager> stager;
+    // dst <- src on stream s: through the stager when src is pageable and
+    // large, else one cudaMemcpyAsync
+    void copy_h2d(void* dst, const void* src, size_t bytes, cudaStream_t s) {
+        if (bytes >= (8u << 20) && HostStager::pageable(src)) {
+            if (!stager) stager.reset(new HostStager());
+            ZK_CUDA(stager->copy(dst, src, bytes, s));
+            return;
+        }
+        if (bytes) ZK_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s));
+    }
+
     ~Engine() {
+        stager.reset();
         drop_graphs();
         for (auto ev : copy_events) cudaEventDestroy(ev);
         if (copy_stream) cudaStreamDestroy(copy_stream);
