@@ -224,9 +224,14 @@ ZkMetalStatus zkmsm_batch_commit(ZkMetalMSMEngine engine, ZkMsmTable table, cons
  * choice, and at the model's two-width layout where it picks one (reported
  * as width 0), for every power-of-two size 2^min_log2n .. 2^max_log2n on
  * synthetic inputs and keeps the fastest per size; later plans of this
- * engine use the table (MSMs matched to the nearest power of two).  A JSON
- * summary of the timings is written to `report` (may be NULL).  Replaces the
- * reference's device tuning (Sources/zkMetal/Tuning.swift:9-127). */
+ * engine use the table (MSMs matched to the nearest power of two).  From
+ * 2^14 points it then tunes the tile schedule at that layout, one knob at a
+ * time: the level-1 chunk length (half or twice the cost rule's), 128
+ * instead of 256 threads per accumulation block, and a bucket-reduction tree
+ * of arity 4 or 16 instead of 8 (a batch plan takes the schedule of its
+ * largest MSM).  A JSON summary of the timings is written to `report` (may
+ * be NULL).  Replaces the reference's device tuning of window bits and
+ * threadgroup sizes (Sources/zkMetal/Tuning.swift:9-127). */
 ZkMetalStatus zkmsm_autotune(ZkMetalMSMEngine engine, int curve, int min_log2n, int max_log2n, char* report,
                              uint64_t report_len);
 /* Persist / restore the autotuned table (text file). */

@@ -1,10 +1,11 @@
 """The MSD radix sort of the sorted-entry stage, replayed on the CPU (no GPU).
 
-k_msd_count / k_msd_tiles / k_msd_scatter (msm_kernels.cuh) are restated
-here index for index: tile geometry (pass 1 over [0, E); pass 2 over the
-pass-1 segments through the tile table), the [segment][digit][tile]
-histogram layout, its exclusive scan, and each tile's placement (local digit
-offsets plus the scanned slot of its run).  On random key sets -- uniform,
+k_msd_count / k_msd_transpose / k_msd_tiles / k_msd_scatter (msm_kernels.cuh)
+are restated here index for index: tile geometry (pass 1 over [0, E); pass 2
+over the pass-1 segments through the tile table), the count rows, the
+[segment][digit][tile] scan layout and its exclusive scan, the slot rows, and
+each tile's placement (local digit offsets from its count row plus the slot
+of its run).  On random key sets -- uniform,
 skewed (one bucket holding a fifth of the entries, like witness scalars
 equal to 1), with fewer entries than the plan's bound, and empty -- every
 index stays inside its buffer, no output slot is written twice and the
@@ -71,42 +72,56 @@ def geom(t, E, ntiles, seg_start, seg_tile, nb):
 
 
 def msd_pass(keys, vals, E, shift, bits, ntiles, seg_start, seg_tile, hsize, grid):
+    """One pass as the device runs it: k_msd_count (rows C[tile][digit]),
+    k_msd_transpose to the scan layout S, the exclusive scan, the transpose
+    back to slot rows P, k_msd_scatter (local offsets from the tile's C row,
+    run slots from its P row)."""
     nb = 1 << bits
-    H = np.full(hsize, 7, dtype=np.int64)  # stale contents: only the prefix the layout uses may matter
-    used = np.zeros(hsize, dtype=bool)
-    for t in range(grid):  # k_msd_count
-        g = geom(t, E, ntiles, seg_start, seg_tile, nb)
+    C = np.full(hsize, 5, dtype=np.int64)  # stale contents everywhere
+    S = np.full(hsize, 7, dtype=np.int64)
+    P = np.full(hsize, 9, dtype=np.int64)
+    geoms = [geom(t, E, ntiles, seg_start, seg_tile, nb) for t in range(grid)]
+    for t, g in enumerate(geoms):  # k_msd_count
         if g is None:
             continue
         lo, hi, k, nt, hb = g
-        cnt = np.bincount((keys[lo:hi] >> shift) & (nb - 1), minlength=nb)
+        assert (t + 1) * nb <= hsize
+        C[t * nb:(t + 1) * nb] = np.bincount((keys[lo:hi] >> shift) & (nb - 1), minlength=nb)
+    used = np.zeros(hsize, dtype=bool)
+    for t, g in enumerate(geoms):  # k_msd_transpose, rows -> scan layout
+        if g is None:
+            continue
+        lo, hi, k, nt, hb = g
         idx = hb + np.arange(nb) * nt + k
         assert idx.max() < hsize and not used[idx].any()
         used[idx] = True
-        H[idx] = cnt
+        S[idx] = C[t * nb:(t + 1) * nb]
     n_used = int(used.sum())
-    assert used[:n_used].all(), "pass counts are not a prefix of the histogram"
-    Hs = excl_scan(H)
+    assert used[:n_used].all(), "pass counts are not a prefix of the scan layout"
+    S[:grid * nb] = excl_scan(S[:grid * nb])  # the scan runs over the bound
+    for t, g in enumerate(geoms):  # k_msd_transpose back, scan layout -> slot rows
+        if g is None:
+            continue
+        lo, hi, k, nt, hb = g
+        P[t * nb:(t + 1) * nb] = S[hb + np.arange(nb) * nt + k]
     outk = np.full(E, -1, dtype=np.int64)
     outv = np.full(E, -1, dtype=np.int64)
-    for t in range(grid):  # k_msd_scatter
-        g = geom(t, E, ntiles, seg_start, seg_tile, nb)
+    for t, g in enumerate(geoms):  # k_msd_scatter
         if g is None or g[0] == g[1]:
             continue
         lo, hi, k, nt, hb = g
         d = (keys[lo:hi] >> shift) & (nb - 1)
-        cnt = np.bincount(d, minlength=nb)
-        off = excl_scan(cnt)
+        off = excl_scan(C[t * nb:(t + 1) * nb])
         perm = np.random.default_rng(t).permutation(hi - lo)  # any order inside a digit
         order = perm[np.argsort(d[perm], kind="stable")]
         dd = d[order]
-        dst = Hs[hb + dd * nt + k] - off[dd] + np.arange(hi - lo)
+        dst = P[t * nb + dd] - off[dd] + np.arange(hi - lo)
         assert (dst >= 0).all() and (dst < E).all() and (outk[dst] == -1).all()
         assert len(np.unique(dst)) == len(dst)
         outk[dst] = keys[lo + order]
         outv[dst] = vals[lo + order]
     assert (outk >= 0).all()
-    return outk, outv, Hs
+    return outk, outv, S
 
 
 def msd_tiles(Hs, ntiles1, nseg, E):

@@ -410,8 +410,14 @@ static Engine& auto_engine() {
 
 // Autotuner: for each power-of-two size in [min_l2, max_l2], time the MSM at
 // window widths around the cost model's choice on synthetic inputs (the
-// library's generator) and keep the fastest.  The table feeds every later
-// plan of this engine (MSMs are matched to the nearest power of two).
+// library's generator) and keep the fastest; then, from 2^14 points, the tile
+// schedule at that layout: the level-1 chunk length (half and twice the cost
+// rule's), 128 instead of 256 threads per accumulation block, and a
+// reduction tree of arity 4 or 16 instead of 8, one knob at a time.  The
+// tables feed every later plan of this engine (MSMs are matched to the
+// nearest power of two; a batch takes the schedule of its largest MSM).
+// The reference's tuner covers window bits and threadgroup sizes
+// (Tuning.swift:9-127).
 template <class C>
 static std::string autotune(Engine& e, int min_l2, int max_l2) {
     using P = typename C::Fp;
@@ -431,11 +437,27 @@ static std::string autotune(Engine& e, int min_l2, int max_l2) {
     const int saved_w = e.tuning.window_bits;
     const bool saved_prof = e.profile;
     e.profile = false;
+    // device time of one n-point MSM under the engine's current tuning
+    auto time_plan = [&](uint32_t n) -> float {
+        Plan& pl = e.get_plan<C>({n}, {0}, ZKMSM_SCALAR_MONT);
+        e.ensure_workspace<C>(pl);
+        e.enqueue<C>(pl, pts.as<uint32_t>(), phi.as<uint32_t>(), sc.as<uint32_t>(), res.as<uint32_t>());
+        ZK_CUDA(cudaEventRecord(a, e.stream));
+        const int reps = n >= (1u << 20) ? 2 : 4;
+        for (int r = 0; r < reps; r++)
+            e.enqueue<C>(pl, pts.as<uint32_t>(), phi.as<uint32_t>(), sc.as<uint32_t>(), res.as<uint32_t>());
+        ZK_CUDA(cudaEventRecord(b, e.stream));
+        ZK_CUDA(cudaEventSynchronize(b));
+        float ms = 0;
+        ZK_CUDA(cudaEventElapsedTime(&ms, a, b));
+        return ms / reps;
+    };
     std::string rep = "{";
     for (int l2 = min_l2; l2 <= max_l2; l2++) {
         uint32_t n = 1u << l2;
         e.tuning.window_bits = 0;
         e.tuning.window_table.erase({CurveTraits<C>::id * 2 + 1, l2});
+        e.tuning.sched_table.erase({CurveTraits<C>::id * 2 + 1, l2});
         e.tuning.version++;
         const MsmDesc d0 = e.get_plan<C>({n}, {0}, ZKMSM_SCALAR_MONT).descs[0];
         const int c0 = (int)d0.c;
@@ -448,18 +470,7 @@ static std::string autotune(Engine& e, int min_l2, int max_l2) {
         for (int c = two_width ? 0 : std::max(4, c0 - 2); c <= std::min(22, c0 + 2); c++) {
             if (c > 0 && c < std::max(4, c0 - 2)) continue;
             e.tuning.window_bits = c;
-            Plan& pl = e.get_plan<C>({n}, {0}, ZKMSM_SCALAR_MONT);
-            e.ensure_workspace<C>(pl);
-            e.enqueue<C>(pl, pts.as<uint32_t>(), phi.as<uint32_t>(), sc.as<uint32_t>(), res.as<uint32_t>());
-            ZK_CUDA(cudaEventRecord(a, e.stream));
-            const int reps = l2 >= 20 ? 2 : 4;
-            for (int r = 0; r < reps; r++)
-                e.enqueue<C>(pl, pts.as<uint32_t>(), phi.as<uint32_t>(), sc.as<uint32_t>(), res.as<uint32_t>());
-            ZK_CUDA(cudaEventRecord(b, e.stream));
-            ZK_CUDA(cudaEventSynchronize(b));
-            float ms = 0;
-            ZK_CUDA(cudaEventElapsedTime(&ms, a, b));
-            ms /= reps;
+            const float ms = time_plan(n);
             row += (row.empty() ? "" : ",") + std::string("\"") + std::to_string(c) + "\":" + std::to_string(ms);
             if (ms < best) {
                 best = ms;
@@ -467,9 +478,49 @@ static std::string autotune(Engine& e, int min_l2, int max_l2) {
             }
         }
         e.tuning.window_table[{CurveTraits<C>::id * 2 + 1, l2}] = best_c;
+        e.tuning.window_bits = 0;
+        e.tuning.version++;
+        // then the tile schedule at that window layout, one knob at a time
+        // (kept when it is at least 1% faster): level-1 chunk length, threads
+        // per accumulation block, arity of the reduction tree
+        Tuning::Schedule bs;
+        std::string srow;
+        if (l2 >= 14) {
+            const std::pair<int, int> key{CurveTraits<C>::id * 2 + 1, l2};
+            auto try_sched = [&](Tuning::Schedule cand, const char* name, int v) {
+                e.tuning.sched_table[key] = cand;
+                e.tuning.version++;
+                const float ms = time_plan(n);
+                srow += (srow.empty() ? "" : ",") + std::string("\"") + name + "=" + std::to_string(v) +
+                        "\":" + std::to_string(ms);
+                if (ms < best * 0.99f) {
+                    best = ms;
+                    bs = cand;
+                }
+            };
+            for (int pct : {50, 200}) {
+                Tuning::Schedule c = bs;
+                c.chunk_pct = pct;
+                try_sched(c, "chunk_pct", pct);
+            }
+            {
+                Tuning::Schedule c = bs;
+                c.acc_threads = 128;
+                try_sched(c, "acc_threads", 128);
+            }
+            for (int L : {4, 16}) {
+                Tuning::Schedule c = bs;
+                c.red_L = L;
+                try_sched(c, "red_L", L);
+            }
+            e.tuning.sched_table[key] = bs;
+            e.tuning.version++;
+        }
         rep += (l2 == min_l2 ? "" : ",") + std::string("\"") + std::to_string(l2) + "\":{\"best\":" +
                std::to_string(best_c) + ",\"model\":" + std::to_string(two_width ? 0 : c0) + ",\"ms\":{" + row +
-               "}}";
+               "},\"schedule\":{\"chunk_pct\":" + std::to_string(bs.chunk_pct) + ",\"acc_threads\":" +
+               std::to_string(bs.acc_threads) + ",\"red_L\":" + std::to_string(bs.red_L) + ",\"ms\":{" + srow +
+               "}},\"best_ms\":" + std::to_string(best) + "}";
     }
     rep += "}";
     e.tuning.window_bits = saved_w;
@@ -830,9 +881,12 @@ ZkMetalStatus zkmsm_tuning_save(ZkMetalMSMEngine engine, const char* path) {
         set_error(std::string("cannot write ") + path);
         return ZKMETAL_ERR_INVALID_INPUT;
     }
-    fprintf(f, "zkmsm-tuning 1\n");
+    fprintf(f, "zkmsm-tuning 2\n");
     for (auto& kv : ENG(engine).tuning.window_table)
-        fprintf(f, "%d %d %d\n", kv.first.first, kv.first.second, kv.second);
+        fprintf(f, "w %d %d %d\n", kv.first.first, kv.first.second, kv.second);
+    for (auto& kv : ENG(engine).tuning.sched_table)
+        fprintf(f, "s %d %d %d %d %d\n", kv.first.first, kv.first.second, kv.second.chunk_pct, kv.second.acc_threads,
+                kv.second.red_L);
     fclose(f);
     return ZKMETAL_SUCCESS;
 }
@@ -846,16 +900,36 @@ ZkMetalStatus zkmsm_tuning_load(ZkMetalMSMEngine engine, const char* path) {
     }
     char head[32] = {0};
     int ver = 0;
-    if (fscanf(f, "%31s %d", head, &ver) != 2 || std::string(head) != "zkmsm-tuning" || ver != 1) {
+    if (fscanf(f, "%31s %d", head, &ver) != 2 || std::string(head) != "zkmsm-tuning" || (ver != 1 && ver != 2)) {
         fclose(f);
         set_error("not a zkmsm tuning file");
         return ZKMETAL_ERR_INVALID_INPUT;
     }
     Engine& e = ENG(engine);
     int k, l2, c;
-    while (fscanf(f, "%d %d %d", &k, &l2, &c) == 3)
-        if (k >= 0 && k < 6 && l2 >= 0 && l2 < 40 && (c == 0 || (c >= 2 && c <= 24)))
-            e.tuning.window_table[{k, l2}] = c;  // 0: the planner's own layout
+    if (ver == 1) {  // window lines only: "k l2 c"
+        while (fscanf(f, "%d %d %d", &k, &l2, &c) == 3)
+            if (k >= 0 && k < 2 * NCURVES && l2 >= 0 && l2 < 40 && (c == 0 || (c >= 2 && c <= 24)))
+                e.tuning.window_table[{k, l2}] = c;  // 0: the planner's own layout
+    } else {  // "w k l2 c" and "s k l2 chunk_pct acc_threads red_L"
+        char tag[4] = {0};
+        while (fscanf(f, "%3s", tag) == 1) {
+            if (tag[0] == 'w') {
+                if (fscanf(f, "%d %d %d", &k, &l2, &c) != 3) break;
+                if (k >= 0 && k < 2 * NCURVES && l2 >= 0 && l2 < 40 && (c == 0 || (c >= 2 && c <= 24)))
+                    e.tuning.window_table[{k, l2}] = c;
+            } else if (tag[0] == 's') {
+                Tuning::Schedule sc;
+                if (fscanf(f, "%d %d %d %d %d", &k, &l2, &sc.chunk_pct, &sc.acc_threads, &sc.red_L) != 5) break;
+                const bool ok = sc.chunk_pct >= 0 && sc.chunk_pct <= 1000 &&
+                                (sc.acc_threads == 0 || sc.acc_threads == 128 || sc.acc_threads == 256) &&
+                                (sc.red_L == 0 || sc.red_L == 4 || sc.red_L == 8 || sc.red_L == 16);
+                if (k >= 0 && k < 2 * NCURVES && l2 >= 0 && l2 < 40 && ok) e.tuning.sched_table[{k, l2}] = sc;
+            } else {
+                break;
+            }
+        }
+    }
     fclose(f);
     e.tuning.version++;
     return ZKMETAL_SUCCESS;

@@ -226,6 +226,15 @@ struct Tuning {
     // autotuned window width per (curve*2 + glv, nearest log2 n); filled by
     // zkmsm_autotune or zkmsm_tuning_load
     std::map<std::pair<int, int>, int> window_table;
+    // autotuned schedule per (curve*2 + glv, nearest log2 n) of the largest
+    // MSM of a plan: level-1 chunk length as a percentage of the cost
+    // rule's (0: the rule's), threads per block of the level-1
+    // accumulation (0: the curve's default), arity of the bucket-reduction
+    // tree (0: 8)
+    struct Schedule {
+        int chunk_pct = 0, acc_threads = 0, red_L = 0;
+    };
+    std::map<std::pair<int, int>, Schedule> sched_table;
     uint64_t version = 0;  // bumped whenever the table changes
     // threads of the level-1 accumulation kernel resident at once on the
     // device, per curve (0: unknown; then chunks are not wave-aligned)
@@ -253,6 +262,8 @@ struct Plan {
     std::vector<uint64_t> acc_Mbound;
     // bucket-reduction levels
     uint32_t red_L = 8, red_log2L = 3;
+    // threads per block of the level-1 accumulation (0: the curve's default)
+    uint32_t acc_threads = 0;
     std::vector<std::vector<RedTask>> red_tasks;
     std::vector<uint32_t> red_nout;
     // device copies of descs and reduction tasks (uploaded once per plan)
@@ -267,6 +278,9 @@ struct Plan {
         nbuckets = nwin_total = 0;
         sort_maxd = sort_spb = sort_passes = sort_bits = sort_tiles = 0;
         msd_passes = msd_bits1 = msd_bits2 = msd_tiles1 = msd_tiles2 = 0;
+        red_L = 8;
+        red_log2L = 3;
+        acc_threads = 0;
         acc_K.clear();
         acc_T.clear();
         acc_Mbound.clear();
@@ -728,6 +742,22 @@ class Engine {
                 pl.msd_tiles2 = pl.msd_passes == 2 ? pl.msd_tiles1 + (1u << pl.msd_bits1) : 0;
             }
         }
+        // autotuned schedule of the plan's largest MSM, if any
+        Tuning::Schedule sc;
+        {
+            const MsmDesc* big = nullptr;
+            for (auto& d : pl.descs)
+                if (!big || d.n > big->n) big = &d;
+            if (big && big->n && !big->wstep) {
+                auto it = tuning.sched_table.find({CurveTraits<C>::id * 2 + (int)big->glv, nearest_log2(big->n)});
+                if (it != tuning.sched_table.end()) sc = it->second;
+            }
+        }
+        pl.acc_threads = sc.acc_threads > 0 ? (uint32_t)sc.acc_threads : 0;
+        if (sc.red_L == 4 || sc.red_L == 8 || sc.red_L == 16) {
+            pl.red_L = (uint32_t)sc.red_L;
+            pl.red_log2L = sc.red_L == 4 ? 2 : sc.red_L == 8 ? 3 : 4;
+        }
         // segmented-sum levels
         uint64_t M = pl.entry_bound;
         uint32_t K1 = tuning.chunk > 0 ? (uint32_t)tuning.chunk : 0;
@@ -753,6 +783,8 @@ class Engine {
                 const uint64_t w = (uint64_t)(waves + 0.5);
                 if (waves >= 1.0 && w >= 1) K1 = (uint32_t)std::max<uint64_t>(8, (Me + w * W - 1) / (w * W));
             }
+            if (sc.chunk_pct > 0)
+                K1 = (uint32_t)std::min<uint64_t>(4096, std::max<uint64_t>(8, (uint64_t)K1 * sc.chunk_pct / 100));
         }
         uint32_t K = K1;
         for (int lvl = 0; lvl < 40; lvl++) {
@@ -890,8 +922,10 @@ class Engine {
                                      pl.msd_passes == 2 ? (uint64_t)(1u << pl.msd_bits2) * pl.msd_tiles2 : 0);
             grew |= w_seg.ensure(((size_t)2 << pl.msd_bits1) * 4 + 64);
         }
+        // the MSD sort keeps three histogram-sized arrays (rows, scan layout, slots)
+        const uint64_t hwords = pl.msd_passes ? 3 * hsz : hsz;
         grew |= w_ents2.ensure(pl.entry_bound * 8 + 16);
-        grew |= w_thist.ensure(hsz * 4 + 16);
+        grew |= w_thist.ensure(hwords * 4 + 16);
         grew |= w_buckets.ensure((size_t)pl.nbuckets * xs + xs);
         uint64_t tmax = 1, m2 = 1, m3 = 1;
         for (size_t l = 0; l < pl.acc_T.size(); l++) tmax = std::max<uint64_t>(tmax, pl.acc_T[l]);

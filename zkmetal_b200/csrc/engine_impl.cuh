@@ -46,35 +46,40 @@ static void msd_scatter_attr(int device) {
 template <class C>
 void Engine::msd_sort(const Plan& pl, uint2* A, uint2* B, uint32_t* tot) {
     msd_scatter_attr(device);
-    uint32_t* H = w_thist.as<uint32_t>();
     const uint32_t b1 = pl.msd_bits1, b2 = pl.msd_bits2, t1 = pl.msd_tiles1, t2 = pl.msd_tiles2;
-    const uint32_t shift1 = pl.msd_passes == 2 ? b2 : 0;
-    k_msd_count<<<t1, MSD_THREADS, 0, stream>>>(A, tot + 0, shift1, b1, t1, nullptr, nullptr, 0, H);
-    launches++;
-    ZK_CUDA(cudaGetLastError());
-    scan_u32(*this, H, (1u << b1) * t1, tot + 63, nullptr);
-    k_msd_scatter<<<t1, MSD_THREADS, MSD_SCATTER_SMEM, stream>>>(A, tot + 0, shift1, b1, t1, nullptr, nullptr, 0, H,
-                                                                    B);
-    launches++;
-    ZK_CUDA(cudaGetLastError());
-    if (pl.msd_passes < 2) return;
+    // three arrays of the larger pass's histogram size: counts as rows (C),
+    // the scan layout (S), the scanned slots as rows (P)
+    const uint64_t hsz = std::max<uint64_t>((uint64_t)(1u << b1) * t1, pl.msd_passes == 2 ? (uint64_t)(1u << b2) * t2 : 0);
+    uint32_t* Cr = w_thist.as<uint32_t>();
+    uint32_t* S = Cr + hsz;
+    uint32_t* P = S + hsz;
     const uint32_t nseg = 1u << b1;
     uint32_t* seg_start = w_seg.as<uint32_t>();
     uint32_t* seg_tile = seg_start + nseg + 1;
-    k_msd_tiles<<<1, MSD_THREADS, 0, stream>>>(H, t1, nseg, tot + 0, seg_start, seg_tile);
+    auto pass = [&](const uint2* src, uint2* dst, uint32_t shift, uint32_t bits, uint32_t grid, uint32_t ntiles,
+                    const uint32_t* ss, const uint32_t* st, uint32_t ns) {
+        const uint32_t nb = 1u << bits;
+        const dim3 tg((grid + MSD_TR - 1) / MSD_TR, (nb + MSD_TR - 1) / MSD_TR), tb(MSD_TR, 8);
+        k_msd_count<<<grid, MSD_THREADS, 0, stream>>>(src, tot + 0, shift, bits, ntiles, ss, st, ns, Cr);
+        k_msd_transpose<<<tg, tb, 0, stream>>>(Cr, S, tot + 0, bits, ntiles, ss, st, ns, 1);
+        launches += 2;
+        ZK_CUDA(cudaGetLastError());
+        // pass-2 counts fill a prefix of S (tiles in segment order); the scan
+        // runs over the bound, and whatever lies past the prefix only shifts
+        // slots past it
+        scan_u32(*this, S, nb * grid, tot + 63, nullptr);
+        k_msd_transpose<<<tg, tb, 0, stream>>>(P, S, tot + 0, bits, ntiles, ss, st, ns, 0);
+        k_msd_scatter<<<grid, MSD_THREADS, MSD_SCATTER_SMEM, stream>>>(src, tot + 0, shift, bits, ntiles, ss, st,
+                                                                      ns, Cr, P, dst);
+        launches += 2;
+        ZK_CUDA(cudaGetLastError());
+    };
+    pass(A, B, pl.msd_passes == 2 ? b2 : 0, b1, t1, t1, nullptr, nullptr, 0);
+    if (pl.msd_passes < 2) return;
+    k_msd_tiles<<<1, MSD_THREADS, 0, stream>>>(S, t1, nseg, tot + 0, seg_start, seg_tile);
     launches++;
     ZK_CUDA(cudaGetLastError());
-    // pass-2 counts occupy a prefix of H (tiles in segment order); the scan
-    // runs over the bound and whatever lies past the prefix only shifts
-    // slots past it
-    k_msd_count<<<t2, MSD_THREADS, 0, stream>>>(B, tot + 0, 0, b2, 0, seg_start, seg_tile, nseg, H);
-    launches++;
-    ZK_CUDA(cudaGetLastError());
-    scan_u32(*this, H, (1u << b2) * t2, tot + 63, nullptr);
-    k_msd_scatter<<<t2, MSD_THREADS, MSD_SCATTER_SMEM, stream>>>(B, tot + 0, 0, b2, 0, seg_start, seg_tile, nseg, H,
-                                                                    A);
-    launches++;
-    ZK_CUDA(cudaGetLastError());
+    pass(B, A, 0, b2, t2, 0, seg_start, seg_tile, nseg);
 }
 
 // ------------------------------------------------------------ pipeline
@@ -157,7 +162,9 @@ void Engine::enqueue(const Plan& pl, const uint32_t* d_bases, const uint32_t* d_
         uint32_t* okeys = w_pkeys[cur].as<uint32_t>();
         Xyzz<P>* ovals = w_pvals[cur].as<Xyzz<P>>();
         if (l == 0) {
-            constexpr int AT = AccLaunch<C>::THREADS;
+            const uint32_t AT = pl.acc_threads && pl.acc_threads <= (uint32_t)AccLaunch<C>::THREADS
+                                        ? pl.acc_threads
+                                        : (uint32_t)AccLaunch<C>::THREADS;
             k_acc_l1<C><<<(T + AT - 1) / AT, AT, 0, stream>>>(
                     w_ents.as<uint2>(), d_len, K, d_bases,
                                                              d_phi, w_cnt.as<uint32_t>(),

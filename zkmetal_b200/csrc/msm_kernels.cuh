@@ -1331,27 +1331,34 @@ static __global__ void __launch_bounds__(SCAN_THREADS) k_scan_add(uint32_t* __re
 // up to 12 bits (one pass for keys of up to 12 bits).  An MSD pass needs no
 // stability -- entries of one bucket may come out in any order, since bucket
 // sums do not depend on it -- so a tile ranks its entries by digit with
-// shared-memory atomics (one atomic per warp for a key the warp shares)
-// instead of the per-bit ballots the stable LSD passes above need.  Per
-// pass, over tiles of at most MSD_TILE entries that never straddle a
-// segment (pass 1: the whole array is one segment; pass 2: one segment per
-// pass-1 digit):
-//  k_msd_count    digit counts of every tile, stored segment by segment and
-//                 digit-major inside a segment: [seg][digit][tile of seg];
-//  scan           exclusive: that layout is the output order, so each
-//                 (seg, digit, tile) count becomes the tile's first slot;
-//  k_msd_tiles    (between the passes) the segment starts, read from the
-//                 pass-1 scan, and the pass-2 tile table;
-//  k_msd_scatter  counts again, places the tile in digit order in shared
-//                 memory, writes it out as one run per digit.
+// shared-memory atomics instead of the per-bit ballots a stable LSD pass
+// needs.  Per pass, over tiles of at most MSD_TILE entries that never
+// straddle a segment (pass 1: the whole array is one segment; pass 2: one
+// segment per pass-1 digit):
+//  k_msd_count      each tile's digit counts, one contiguous row per tile:
+//                   C[tile][digit];
+//  k_msd_transpose  (to the scan layout) segment by segment, digit-major
+//                   inside a segment: S[seg][digit][tile of seg], the output
+//                   order, so that an exclusive scan of S gives each
+//                   (seg, digit, tile) its first output slot;
+//  scan;
+//  k_msd_transpose  (back) the slots as rows again: P[tile][digit];
+//  k_msd_tiles      (between the passes) the segment starts, read from the
+//                   pass-1 scan, and the pass-2 tile table;
+//  k_msd_scatter    reads its tile's two rows (counts -> local offsets, and
+//                   slots), places the tile in digit order in shared memory
+//                   and writes it out as one run per digit.
+// Rows keep every per-tile read and write contiguous; the transposes move
+// 32 x 32 blocks through shared memory.
 // Replaces the reference's CPU counting sort per window (MSMEngine.swift:595-661).
 
 // Tile t of a pass.  Pass 1 (seg_tile == nullptr): [t*MSD_TILE, ...) of
-// [0, E), histogram laid out for `ntiles` tiles (tiles past E are empty and
-// count zeros).  Pass 2: the segment owning t in the tile table seg_tile
-// (exclusive prefix of tiles per segment, nseg + 1 entries) with segment
-// starts seg_start (nseg + 1 entries, the last one E).  False past the last
-// tile.
+// [0, E) in the scan layout of one segment of `ntiles` tiles (tiles past E
+// are empty and count zeros).  Pass 2: the segment owning t in the tile
+// table seg_tile (exclusive prefix of tiles per segment, nseg + 1 entries)
+// with segment starts seg_start (nseg + 1 entries, the last one E).  hbase,
+// nt and k place the tile's counts in the scan layout: S[hbase + digit*nt +
+// k].  False past the last tile.
 struct MsdGeom {
     uint32_t lo, hi, k, nt;
     uint64_t hbase;
@@ -1415,31 +1422,54 @@ ZK_DEV uint32_t block_excl_scan_w(uint32_t v, uint32_t* sh, uint32_t& total) {
     return pre + x - v;
 }
 
-// Shared-memory slot claim on ctr[key], the hot-key case aggregated as in
-// warp_count (lanes sharing the first valid lane's key take one atomic);
-// returns this lane's slot.  All 32 lanes of the warp call it together.
-ZK_DEV uint32_t warp_claim(uint32_t* __restrict__ ctr, bool valid, uint32_t key) {
+// Shared-memory counter bump / slot claim on ctr[key].  A warp whose valid
+// lanes all hold one key (a hot bucket, e.g. many scalars equal to 1) takes
+// one atomic; otherwise every valid lane takes its own, and the few lanes
+// that share a key are serialised by the hardware.  All 32 lanes call it.
+ZK_DEV void msd_count_one(uint32_t* __restrict__ ctr, bool valid, uint32_t key) {
+    const uint32_t m = __ballot_sync(0xffffffffu, valid);
+    if (!m) return;
+    const uint32_t leader = __ffs(m) - 1;
+    const uint32_t lk = __shfl_sync(0xffffffffu, key, leader);
+    if (__all_sync(0xffffffffu, !valid || key == lk)) {
+        if ((threadIdx.x & 31) == leader) atomicAdd(ctr + lk, (uint32_t)__popc(m));
+    } else if (valid) {
+        atomicAdd(ctr + key, 1u);
+    }
+}
+
+ZK_DEV uint32_t msd_claim_one(uint32_t* __restrict__ ctr, bool valid, uint32_t key) {
     const uint32_t lane = threadIdx.x & 31;
     const uint32_t m = __ballot_sync(0xffffffffu, valid);
     if (!m) return 0;
     const uint32_t leader = __ffs(m) - 1;
     const uint32_t lk = __shfl_sync(0xffffffffu, key, leader);
-    const bool grp = valid && key == lk;
-    const uint32_t same = __ballot_sync(0xffffffffu, grp);
-    uint32_t b = 0;
-    if (lane == leader) b = atomicAdd(ctr + lk, (uint32_t)__popc(same));
-    b = __shfl_sync(0xffffffffu, b, leader);
-    if (grp) return b + __popc(same & ((1u << lane) - 1));
+    if (__all_sync(0xffffffffu, !valid || key == lk)) {
+        uint32_t b = 0;
+        if (lane == leader) b = atomicAdd(ctr + lk, (uint32_t)__popc(m));
+        b = __shfl_sync(0xffffffffu, b, leader);
+        return b + __popc(m & ((1u << lane) - 1));
+    }
     return valid ? atomicAdd(ctr + key, 1u) : 0u;
 }
 
 constexpr uint32_t MSD_ROUNDS = (MSD_TILE + MSD_THREADS - 1) / MSD_THREADS;
-constexpr uint32_t MSD_BATCH = 8;  // keys loaded before they are counted
+constexpr uint32_t MSD_BATCH = 8;  // entries loaded before they are used
 static_assert(MSD_ROUNDS % MSD_BATCH == 0, "tile rounds come in whole load batches");
+constexpr uint32_t MSD_PER = (1u << MSD_MAX_BITS) / MSD_THREADS;  // digits per thread in row scans
 
-// The block's digit counts of its tile into ctr (zeroed by the caller).
-ZK_DEV void msd_count_tile(const uint2* __restrict__ A, const MsdGeom& g, uint32_t shift, uint32_t mask,
-                           uint32_t* __restrict__ ctr) {
+static __global__ void __launch_bounds__(MSD_THREADS) k_msd_count(const uint2* __restrict__ A,
+                                                                 const uint32_t* __restrict__ d_total,
+                                                                 uint32_t shift, uint32_t bits, uint32_t ntiles,
+                                                                 const uint32_t* __restrict__ seg_start,
+                                                                 const uint32_t* __restrict__ seg_tile,
+                                                                 uint32_t nseg, uint32_t* __restrict__ C) {
+    __shared__ uint32_t cnt[1u << MSD_MAX_BITS];
+    const uint32_t nb = 1u << bits, mask = nb - 1;
+    MsdGeom g;
+    if (!msd_geom(blockIdx.x, *d_total, ntiles, seg_start, seg_tile, nseg, nb, g)) return;
+    for (uint32_t i = threadIdx.x; i < nb; i += MSD_THREADS) cnt[i] = 0;
+    __syncthreads();
     const uint32_t len = g.hi - g.lo;
 #pragma unroll 1
     for (uint32_t r0 = 0; r0 < MSD_ROUNDS; r0 += MSD_BATCH) {
@@ -1450,47 +1480,81 @@ ZK_DEV void msd_count_tile(const uint2* __restrict__ A, const MsdGeom& g, uint32
             key[q] = j < len ? (A[(uint64_t)g.lo + j].x >> shift) & mask : 0xffffffffu;
         }
 #pragma unroll
-        for (uint32_t q = 0; q < MSD_BATCH; q++) warp_count(ctr, key[q] != 0xffffffffu, key[q]);
+        for (uint32_t q = 0; q < MSD_BATCH; q++) msd_count_one(cnt, key[q] != 0xffffffffu, key[q]);
     }
+    __syncthreads();
+    uint32_t* row = C + (uint64_t)blockIdx.x * nb;
+    for (uint32_t d = threadIdx.x; d < nb; d += MSD_THREADS) row[d] = cnt[d];
 }
 
-static __global__ void __launch_bounds__(MSD_THREADS) k_msd_count(const uint2* __restrict__ A,
-                                                                 const uint32_t* __restrict__ d_total,
-                                                                 uint32_t shift, uint32_t bits, uint32_t ntiles,
-                                                                 const uint32_t* __restrict__ seg_start,
-                                                                 const uint32_t* __restrict__ seg_tile,
-                                                                 uint32_t nseg, uint32_t* __restrict__ H) {
-    __shared__ uint32_t cnt[1u << MSD_MAX_BITS];
+// Between the row layout R[tile][digit] and the scan layout S (see
+// msd_geom), for the tiles of a pass: to_scan 1 copies R -> S, 0 copies
+// S -> R.  Blocks of 32 tiles x 32 digits go through shared memory so that
+// both sides are read and written along their contiguous dimension.
+constexpr uint32_t MSD_TR = 32;
+static __global__ void __launch_bounds__(MSD_TR * 8) k_msd_transpose(uint32_t* __restrict__ R,
+                                                                    uint32_t* __restrict__ S,
+                                                                    const uint32_t* __restrict__ d_total,
+                                                                    uint32_t bits, uint32_t ntiles,
+                                                                    const uint32_t* __restrict__ seg_start,
+                                                                    const uint32_t* __restrict__ seg_tile,
+                                                                    uint32_t nseg, int to_scan) {
+    __shared__ uint32_t blk[MSD_TR][MSD_TR + 1];
+    __shared__ uint64_t row_base[MSD_TR];  // hbase + k of each tile row (~0: no tile)
+    __shared__ uint32_t row_nt[MSD_TR];
     const uint32_t nb = 1u << bits;
-    MsdGeom g;
-    if (!msd_geom(blockIdx.x, *d_total, ntiles, seg_start, seg_tile, nseg, nb, g)) return;
-    for (uint32_t i = threadIdx.x; i < nb; i += MSD_THREADS) cnt[i] = 0;
+    const uint32_t t0 = blockIdx.x * MSD_TR, d0 = blockIdx.y * MSD_TR;
+    const uint32_t tx = threadIdx.x, ty = threadIdx.y;  // 32 x 8
+    if (ty == 0) {
+        MsdGeom g;
+        const bool ok = msd_geom(t0 + tx, *d_total, ntiles, seg_start, seg_tile, nseg, nb, g);
+        row_base[tx] = ok ? g.hbase + g.k : ~0ull;
+        row_nt[tx] = ok ? g.nt : 0;
+    }
     __syncthreads();
-    msd_count_tile(A, g, shift, nb - 1, cnt);
-    __syncthreads();
-    for (uint32_t d = threadIdx.x; d < nb; d += MSD_THREADS) H[g.hbase + (uint64_t)d * g.nt + g.k] = cnt[d];
+    if (to_scan) {
+        // read rows (contiguous in digits), write the scan layout (contiguous in tiles)
+        for (uint32_t i = ty; i < MSD_TR; i += 8) {
+            const uint32_t t = t0 + i, d = d0 + tx;
+            blk[i][tx] = row_base[i] != ~0ull && d < nb ? R[(uint64_t)t * nb + d] : 0u;
+        }
+        __syncthreads();
+        for (uint32_t j = ty; j < MSD_TR; j += 8) {
+            const uint32_t d = d0 + j;
+            if (row_base[tx] != ~0ull && d < nb) S[row_base[tx] + (uint64_t)d * row_nt[tx]] = blk[tx][j];
+        }
+    } else {
+        for (uint32_t j = ty; j < MSD_TR; j += 8) {
+            const uint32_t d = d0 + j;
+            blk[tx][j] = row_base[tx] != ~0ull && d < nb ? S[row_base[tx] + (uint64_t)d * row_nt[tx]] : 0u;
+        }
+        __syncthreads();
+        for (uint32_t i = ty; i < MSD_TR; i += 8) {
+            const uint32_t t = t0 + i, d = d0 + tx;
+            if (row_base[i] != ~0ull && d < nb) R[(uint64_t)t * nb + d] = blk[i][tx];
+        }
+    }
 }
 
 // Between the passes (one block): seg_start[s] = first output slot of pass-1
 // digit s (the scanned count of (s, tile 0)), seg_start[nseg] = E; seg_tile =
 // exclusive prefix of ceil(segment length / MSD_TILE), nseg + 1 entries.
-static __global__ void __launch_bounds__(MSD_THREADS) k_msd_tiles(const uint32_t* __restrict__ H1s,
+static __global__ void __launch_bounds__(MSD_THREADS) k_msd_tiles(const uint32_t* __restrict__ S1,
                                                                  uint32_t ntiles1, uint32_t nseg,
                                                                  const uint32_t* __restrict__ d_total,
                                                                  uint32_t* __restrict__ seg_start,
                                                                  uint32_t* __restrict__ seg_tile) {
     __shared__ uint32_t sh[MSD_THREADS / 32];
     const uint32_t E = *d_total;
-    constexpr uint32_t PER = (1u << MSD_MAX_BITS) / MSD_THREADS;
-    uint32_t st[PER + 1], nt[PER], sum = 0;
+    uint32_t st[MSD_PER + 1], nt[MSD_PER], sum = 0;
 #pragma unroll
-    for (uint32_t q = 0; q <= PER; q++) {
-        const uint32_t s = threadIdx.x * PER + q;
-        st[q] = s < nseg ? H1s[(uint64_t)s * ntiles1] : E;
+    for (uint32_t q = 0; q <= MSD_PER; q++) {
+        const uint32_t s = threadIdx.x * MSD_PER + q;
+        st[q] = s < nseg ? S1[(uint64_t)s * ntiles1] : E;
     }
 #pragma unroll
-    for (uint32_t q = 0; q < PER; q++) {
-        const uint32_t s = threadIdx.x * PER + q;
+    for (uint32_t q = 0; q < MSD_PER; q++) {
+        const uint32_t s = threadIdx.x * MSD_PER + q;
         const uint32_t len = s < nseg ? st[q + 1] - st[q] : 0;
         nt[q] = (len + MSD_TILE - 1) / MSD_TILE;
         sum += nt[q];
@@ -1498,8 +1562,8 @@ static __global__ void __launch_bounds__(MSD_THREADS) k_msd_tiles(const uint32_t
     uint32_t total;
     uint32_t pre = block_excl_scan_w<MSD_THREADS / 32>(sum, sh, total);
 #pragma unroll
-    for (uint32_t q = 0; q < PER; q++) {
-        const uint32_t s = threadIdx.x * PER + q;
+    for (uint32_t q = 0; q < MSD_PER; q++) {
+        const uint32_t s = threadIdx.x * MSD_PER + q;
         if (s < nseg) {
             seg_start[s] = st[q];
             seg_tile[s] = pre;
@@ -1512,8 +1576,8 @@ static __global__ void __launch_bounds__(MSD_THREADS) k_msd_tiles(const uint32_t
     }
 }
 
-// Dynamic shared memory of k_msd_scatter: the staged tile and two counters
-// per digit.
+// Dynamic shared memory of k_msd_scatter: the staged tile and two words per
+// digit.
 constexpr size_t MSD_SCATTER_SMEM = (size_t)MSD_TILE * sizeof(uint2) + 2 * (1u << MSD_MAX_BITS) * sizeof(uint32_t);
 
 static __global__ void __launch_bounds__(MSD_THREADS) k_msd_scatter(const uint2* __restrict__ A,
@@ -1521,7 +1585,8 @@ static __global__ void __launch_bounds__(MSD_THREADS) k_msd_scatter(const uint2*
                                                                    uint32_t shift, uint32_t bits, uint32_t ntiles,
                                                                    const uint32_t* __restrict__ seg_start,
                                                                    const uint32_t* __restrict__ seg_tile,
-                                                                   uint32_t nseg, const uint32_t* __restrict__ Hs,
+                                                                   uint32_t nseg, const uint32_t* __restrict__ C,
+                                                                   const uint32_t* __restrict__ P,
                                                                    uint2* __restrict__ B) {
     extern __shared__ uint4 msd_smem[];
     uint2* stage = reinterpret_cast<uint2*>(msd_smem);
@@ -1533,25 +1598,22 @@ static __global__ void __launch_bounds__(MSD_THREADS) k_msd_scatter(const uint2*
     if (!msd_geom(blockIdx.x, *d_total, ntiles, seg_start, seg_tile, nseg, nb, g)) return;
     const uint32_t len = g.hi - g.lo;
     if (len == 0) return;
-    for (uint32_t i = threadIdx.x; i < nb; i += MSD_THREADS) cur[i] = 0;
-    __syncthreads();
-    msd_count_tile(A, g, shift, mask, cur);
-    __syncthreads();
-    // local offsets of the digits (exclusive scan of the counts), counters reset
+    const uint32_t* crow = C + (uint64_t)blockIdx.x * nb;
+    const uint32_t* prow = P + (uint64_t)blockIdx.x * nb;
+    // local offsets of the digits: exclusive scan of the tile's counts
     {
-        constexpr uint32_t PER = (1u << MSD_MAX_BITS) / MSD_THREADS;
-        uint32_t c[PER], sum = 0;
+        uint32_t c[MSD_PER], sum = 0;
 #pragma unroll
-        for (uint32_t q = 0; q < PER; q++) {
-            const uint32_t d = threadIdx.x * PER + q;
-            c[q] = d < nb ? cur[d] : 0;
+        for (uint32_t q = 0; q < MSD_PER; q++) {
+            const uint32_t d = threadIdx.x * MSD_PER + q;
+            c[q] = d < nb ? crow[d] : 0;
             sum += c[q];
         }
         uint32_t total;
         uint32_t pre = block_excl_scan_w<MSD_THREADS / 32>(sum, sh, total);
 #pragma unroll
-        for (uint32_t q = 0; q < PER; q++) {
-            const uint32_t d = threadIdx.x * PER + q;
+        for (uint32_t q = 0; q < MSD_PER; q++) {
+            const uint32_t d = threadIdx.x * MSD_PER + q;
             if (d < nb) {
                 off[d] = pre;
                 cur[d] = 0;
@@ -1560,7 +1622,7 @@ static __global__ void __launch_bounds__(MSD_THREADS) k_msd_scatter(const uint2*
         }
     }
     __syncthreads();
-    // place the tile in digit order (the entries are read again, from L2)
+    // place the tile in digit order
 #pragma unroll 1
     for (uint32_t r0 = 0; r0 < MSD_ROUNDS; r0 += MSD_BATCH) {
         uint2 e[MSD_BATCH];
@@ -1574,14 +1636,13 @@ static __global__ void __launch_bounds__(MSD_THREADS) k_msd_scatter(const uint2*
             const uint32_t j = (r0 + q) * MSD_THREADS + threadIdx.x;
             const bool v = j < len;
             const uint32_t d = v ? (e[q].x >> shift) & mask : 0u;
-            const uint32_t slot = warp_claim(cur, v, d);
+            const uint32_t slot = msd_claim_one(cur, v, d);
             if (v) stage[off[d] + slot] = e[q];
         }
     }
     __syncthreads();
-    // global start of each digit's run, less its local offset
-    for (uint32_t d = threadIdx.x; d < nb; d += MSD_THREADS)
-        if (cur[d]) off[d] = Hs[g.hbase + (uint64_t)d * g.nt + g.k] - off[d];
+    // global slot of each digit's run, less its local offset
+    for (uint32_t d = threadIdx.x; d < nb; d += MSD_THREADS) off[d] = prow[d] - off[d];
     __syncthreads();
     for (uint32_t i = threadIdx.x; i < len; i += MSD_THREADS) {
         const uint2 v = stage[i];
