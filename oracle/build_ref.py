@@ -1,13 +1,17 @@
 #!/usr/bin/env python3
 """Build recipe for the reference's own CPU Pippenger (test infrastructure only).
 
-This is the CHECKER, never the product.  It compiles the reference's three C
+This is the CHECKER, never the product.  It compiles the reference's four C
 translation units that hold the MSM path,
 
     Sources/NeonFieldOps/bn254_msm.c       (bn254_pippenger_msm, :1145-1187)
     Sources/NeonFieldOps/bls12_381_ops.c   (bls12_381_g1_pippenger_msm, :1141-1165)
     Sources/NeonFieldOps/bls12_377_ops.c   (bls12_377_g1_pippenger_msm, :1476-1550,
                                             bls12_377_g1_scalar_mul, :1301)
+    Sources/NeonFieldOps/bn254_pairing.c   (bn254_pairing, :1320: the optimal ate
+                                            pairing, used to pin BN254 G2 MSM results
+                                            through bilinearity; the reference has no
+                                            C G2 MSM)
 
 from where they lie in the read-only reference checkout into
 ``oracle/_ref/libzkref.so`` (git-ignored; it travels to the GPU host with the
@@ -39,7 +43,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 OUT = os.path.join(HERE, "_ref")
 LIB = os.path.join(OUT, "libzkref.so")
 SOURCES = ["Sources/NeonFieldOps/bn254_msm.c", "Sources/NeonFieldOps/bls12_381_ops.c",
-           "Sources/NeonFieldOps/bls12_377_ops.c"]
+           "Sources/NeonFieldOps/bls12_377_ops.c", "Sources/NeonFieldOps/bn254_pairing.c"]
 HEADER_DIR = "Sources/NeonFieldOps/include"
 
 

@@ -148,6 +148,9 @@ class RefOracle:
         L.bls12_381_fr_mul.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
         L.bn254_point_scalar_mul.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
         L.bls12_381_g1_scalar_mul.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+        self.has_pairing = hasattr(L, "bn254_pairing")
+        if self.has_pairing:
+            L.bn254_pairing.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
         self._c = None
 
     def _conv(self):
@@ -178,6 +181,16 @@ class RefOracle:
             return out.tobytes()
         # the reference exports no BLS12-381 Jacobian->affine; normalise with the restatement
         return self._conv().jacobian_to_affine(curve, jac)
+
+    def bn254_pairing(self, g1_affine, g2_affine):
+        """The reference's optimal ate pairing e(P, Q) (bn254_pairing,
+        bn254_pairing.c:1320): P affine G1 (64 B), Q affine G2 (128 B: x.c0,
+        x.c1, y.c0, y.c1), both Montgomery; returns the Fp12 value (384 B)."""
+        p = np.frombuffer(g1_affine, dtype=np.uint64).copy()
+        q = np.frombuffer(g2_affine, dtype=np.uint64).copy()
+        out = np.zeros(48, dtype=np.uint64)
+        self.lib.bn254_pairing(p.ctypes.data, q.ctypes.data, out.ctypes.data)
+        return out.tobytes()
 
     def point_scalar_mul(self, curve, point_affine, k_int):
         """k*P (affine bytes) by the reference's own double-and-add

@@ -1,7 +1,9 @@
 """BN254 G2 MSM (GPU) against the Python restatement of the reference's G2
-path (oracle/pyref.py G2Curve; the reference has no C G2 MSM to compile, so
-this parity is pinned to the restatement and to group identities:
-r*G2 = O, linearity, k*G2 known answers)."""
+path (oracle/pyref.py G2Curve) and group identities (r*G2 = O, linearity,
+k*G2 known answers), and against the reference itself through its compiled
+C pairing: the reference has no C G2 MSM, but with bases k_i*G2 an MSM equals
+t*G2 for a known t, and e(G1, MSM) = e(t*G1, G2) under the reference's
+bn254_pairing pins each result (test_g2_msm_pinned_by_reference_pairing)."""
 import ctypes
 import random
 
@@ -124,3 +126,31 @@ def test_g2_table_batches_with_shifts(eng):
             off += c
     finally:
         t.close()
+
+
+@pytest.mark.parametrize("n", [4096, 1 << 16])
+def test_g2_msm_pinned_by_reference_pairing(eng, oracles, n):
+    """The device G2 MSM against the reference itself through its pairing:
+    bases are k_i*G2 from the library's generator (k_i known from the
+    restatement of the generator), so MSM(Q, s) = t*G2 with t = sum s_i k_i,
+    and e(G1, MSM) must equal e(t*G1, G2) with the reference's bn254_pairing
+    and bn254_point_scalar_mul (bn254_pairing.c:1320, bn254_msm.c:1333)."""
+    ref, _ = oracles
+    if ref is None or not ref.has_pairing:
+        pytest.skip("reference C library not built")
+    C = R.BN254
+    L = zl.lib()
+    seed = 977
+    p = torch.empty(n * 128, dtype=torch.uint8, device="cuda")
+    s = torch.empty(n * 32, dtype=torch.uint8, device="cuda")
+    torch.cuda.synchronize()
+    check(L.zkmsm_gen_bases(eng.handle, zl.BN254_G2, seed, 0, n, p.data_ptr()))
+    check(L.zkmsm_gen_scalars(eng.handle, zl.BN254_G2, seed + 1, 0, n, 0, zl.SCALAR_INT, s.data_ptr()))
+    sh = to_host(s)
+    got = aff(eng.msm(to_host(p), sh))
+    sc = [int.from_bytes(sh[32 * i:32 * i + 32], "little") for i in range(n)]
+    t = sum(a * R.base_scalar(G2, seed, i) for i, a in enumerate(sc)) % G2.r
+    G1b = C.enc_affine((C.gx, C.gy))
+    lhs = ref.bn254_pairing(G1b, G2.enc_affine(got))
+    rhs = ref.bn254_pairing(ref.point_scalar_mul("bn254", G1b, t), G2.enc_affine((G2.gx, G2.gy)))
+    assert lhs == rhs

@@ -193,3 +193,29 @@ def test_host_generator_matches_restatement(curve, oracles):
         assert cm.gen_scalars(curve, 77, 40, dist, 1, index0=5).tobytes() == R.pack_scalars_mont(C, sc)
     got = cm.gen_bases(curve, C.enc_affine((C.gx, C.gy)), 77, 24, index0=3).tobytes()
     assert got == R.pack_points(C, [R.scalar_mul(C, (C.gx, C.gy), R.base_scalar(C, 77, i)) for i in range(3, 27)])
+
+
+def test_g2_restatement_pinned_by_reference_pairing(oracles):
+    """The BN254 G2 restatement (the checker of the G2 MSM) against the
+    reference's own optimal ate pairing (bn254_pairing, bn254_pairing.c:1320):
+    with bases Q_i = k_i*G2, MSM(Q, s) = t*G2 for t = sum s_i k_i, so
+    e(G1, MSM) must equal e(t*G1, G2), t*G1 by the reference's
+    bn254_point_scalar_mul.  The reference has no C G2 MSM; bilinearity of its
+    pairing pins the G2 results to it."""
+    ref, _ = oracles
+    if ref is None or not ref.has_pairing:
+        pytest.skip("reference C library not built")
+    C, G2 = R.BN254, R.BN254_G2
+    G1b = C.enc_affine((C.gx, C.gy))
+    Q = (G2.gx, G2.gy)
+    rng = random.Random(23)
+    for n in (1, 3, 17):
+        ks = [R.base_scalar(G2, 55, i) for i in range(n)]
+        pts = [G2.scalar_mul(Q, k) for k in ks]
+        sc = [rng.randrange(G2.r) for _ in range(n)]
+        t = sum(a * b for a, b in zip(sc, ks)) % G2.r
+        msm = G2.naive_msm(pts, sc)
+        lhs = ref.bn254_pairing(G1b, G2.enc_affine(msm))
+        rhs = ref.bn254_pairing(ref.point_scalar_mul("bn254", G1b, t), G2.enc_affine(Q))
+        assert lhs == rhs, n
+    assert ref.bn254_pairing(G1b, G2.enc_affine(G2.scalar_mul(Q, 2))) != ref.bn254_pairing(G1b, G2.enc_affine(Q))
