@@ -785,9 +785,18 @@ static __global__ void __launch_bounds__(256) k_chunk_count(const uint32_t* __re
 // SM at its natural 114 registers; BLS12-381 (158 registers unbounded) is
 // held to 128 registers for two blocks per SM, 8% faster despite a few
 // spilled bytes (measured at 2^22).
+// (ZKMSM_ACC_MIN_BLOCKS_BN254: build-time override of BN254's minimum
+// resident blocks, for occupancy measurements.)
+#ifndef ZKMSM_ACC_MIN_BLOCKS_BN254
+#define ZKMSM_ACC_MIN_BLOCKS_BN254 1
+#endif
 template <class C>
 struct AccLaunch {
     static constexpr int THREADS = 256, MIN_BLOCKS = 1;
+};
+template <>
+struct AccLaunch<Bn254> {
+    static constexpr int THREADS = 256, MIN_BLOCKS = ZKMSM_ACC_MIN_BLOCKS_BN254;
 };
 template <>
 struct AccLaunch<Bls381> {
