@@ -12,7 +12,7 @@ import re
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
-LIB_PATH = os.environ.get("ZKMSM_LIB", os.path.join(HERE, "libzkmsm.so"))
+LIB_PATH = os.environ.get("ZKMSM_LIB") or os.path.join(HERE, "libzkmsm.so")
 HEADER = os.path.join(ROOT, "include", "zkmsm.h")
 
 SUCCESS = 0
