@@ -307,7 +307,7 @@ void zkmsm_pool_destroy(ZkMsmPool pool);
  * c bits, then (c + 1)-bit windows up to the scalar width. */
 ZkMetalStatus zkmsm_engine_set_tuning(ZkMetalMSMEngine engine, int window_bits, int chunk, int glv);
 /* NEW: window layout from a sample of the scalars (on by default).  For a
- * single MSM of at least 2^20 points on a GLV curve, with no window width
+ * single MSM of at least 2^21 points on a GLV curve, with no window width
  * forced or autotuned for its size, the engine first profiles 4096 of the
  * scalars on the device (bit lengths of their prepared halves) and picks the
  * window layout that minimises sorted entries plus bucket-reduction work for

@@ -400,11 +400,11 @@ def test_dropin_pinned_buffers_overlap(eng, curve, n):
 @pytest.mark.parametrize("dist", ["uniform", "witness"])
 def test_sampled_layout_same_result(eng, dist):
     """The window layout chosen from a sample of the scalars (on by default
-    from 2^20 points) changes the schedule, never the result: device calls
+    from 2^21 points) changes the schedule, never the result: device calls
     (synchronous and on a stream) and a drop-in host call with sampling on
     equal the call with sampling off."""
     e = eng["bn254"]
-    n = (1 << 20) + 123
+    n = (1 << 21) + 123
     p, s = gen_inputs(e, "bn254", 881, n, dist, zl.SCALAR_MONT)
     L = zl.lib()
     check(L.zkmsm_engine_set_sampling(e.handle, 0))

@@ -530,11 +530,14 @@ class Engine {
     std::vector<std::vector<cudaEvent_t>> prof_pending;
     double phase_ms[NPHASE] = {0, 0, 0, 0, 0};
     uint64_t phase_calls = 0;
-    // Sample the scalars of MSMs of at least 2^20 points and choose their
+    // Sample the scalars of MSMs of at least 2^21 points and choose their
     // window layout from the sample (k_scalar_profile); 0 = layout from n
-    // alone.  Sampling waits for the stream the call runs on.
+    // alone.  Sampling waits for the stream the call runs on.  (At 2^20
+    // BN254 points it did not pay: witness-like scalars 2.93 -> 2.97 ms,
+    // uniform 5.21 -> 5.30 ms for the wait; at 2^21 witness-like 4.35 ->
+    // 4.04 ms, at 2^24 17.3 -> 14.6 ms.)
     int scalar_sampling = 1;
-    static constexpr uint64_t SAMPLE_MIN_POINTS = 1ull << 20;
+    static constexpr uint64_t SAMPLE_MIN_POINTS = 1ull << 21;
     std::vector<cudaEvent_t> prof_begin() {
         std::vector<cudaEvent_t> ev;
         if (!profile) return ev;

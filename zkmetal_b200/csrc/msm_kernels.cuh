@@ -785,18 +785,9 @@ static __global__ void __launch_bounds__(256) k_chunk_count(const uint32_t* __re
 // SM at its natural 114 registers; BLS12-381 (158 registers unbounded) is
 // held to 128 registers for two blocks per SM, 8% faster despite a few
 // spilled bytes (measured at 2^22).
-// (ZKMSM_ACC_MIN_BLOCKS_BN254: build-time override of BN254's minimum
-// resident blocks, for occupancy measurements.)
-#ifndef ZKMSM_ACC_MIN_BLOCKS_BN254
-#define ZKMSM_ACC_MIN_BLOCKS_BN254 1
-#endif
 template <class C>
 struct AccLaunch {
     static constexpr int THREADS = 256, MIN_BLOCKS = 1;
-};
-template <>
-struct AccLaunch<Bn254> {
-    static constexpr int THREADS = 256, MIN_BLOCKS = ZKMSM_ACC_MIN_BLOCKS_BN254;
 };
 template <>
 struct AccLaunch<Bls381> {
@@ -1466,9 +1457,6 @@ constexpr uint32_t MSD_ROUNDS = (MSD_TILE + MSD_THREADS - 1) / MSD_THREADS;
 constexpr uint32_t MSD_BATCH = 8;  // entries loaded before they are used
 static_assert(MSD_ROUNDS % MSD_BATCH == 0, "tile rounds come in whole load batches");
 constexpr uint32_t MSD_PER = (1u << MSD_MAX_BITS) / MSD_THREADS;  // digits per thread in row scans
-#ifndef ZKMSM_MSD_INDEX_STAGE
-#define ZKMSM_MSD_INDEX_STAGE 0
-#endif
 
 static __global__ void __launch_bounds__(MSD_THREADS) k_msd_count(const uint2* __restrict__ A,
                                                                  const uint32_t* __restrict__ d_total,
@@ -1588,80 +1576,6 @@ static __global__ void __launch_bounds__(MSD_THREADS) k_msd_tiles(const uint32_t
     }
 }
 
-#if ZKMSM_MSD_INDEX_STAGE
-// Variant (build-time switch, for measurement): the tile is staged as 16-bit
-// local indices (48 KB instead of 192 KB, two blocks per SM); the write-out
-// gathers each entry again from L2, where the tile still is.
-constexpr size_t MSD_SCATTER_SMEM = (size_t)MSD_TILE * sizeof(uint16_t) + 2 * (1u << MSD_MAX_BITS) * sizeof(uint32_t);
-static_assert(MSD_TILE <= 65536, "16-bit local indices");
-
-static __global__ void __launch_bounds__(MSD_THREADS, 2) k_msd_scatter(const uint2* __restrict__ A,
-                                                                      const uint32_t* __restrict__ d_total,
-                                                                      uint32_t shift, uint32_t bits, uint32_t ntiles,
-                                                                      const uint32_t* __restrict__ seg_start,
-                                                                      const uint32_t* __restrict__ seg_tile,
-                                                                      uint32_t nseg, const uint32_t* __restrict__ C,
-                                                                      const uint32_t* __restrict__ P,
-                                                                      uint2* __restrict__ B) {
-    extern __shared__ uint4 msd_smem[];
-    uint32_t* cur = reinterpret_cast<uint32_t*>(msd_smem);
-    uint32_t* off = cur + (1u << MSD_MAX_BITS);
-    uint16_t* stage = reinterpret_cast<uint16_t*>(off + (1u << MSD_MAX_BITS));
-    __shared__ uint32_t sh[MSD_THREADS / 32];
-    const uint32_t nb = 1u << bits, mask = nb - 1;
-    MsdGeom g;
-    if (!msd_geom(blockIdx.x, *d_total, ntiles, seg_start, seg_tile, nseg, nb, g)) return;
-    const uint32_t len = g.hi - g.lo;
-    if (len == 0) return;
-    const uint32_t* crow = C + (uint64_t)blockIdx.x * nb;
-    const uint32_t* prow = P + (uint64_t)blockIdx.x * nb;
-    {
-        uint32_t c[MSD_PER], sum = 0;
-#pragma unroll
-        for (uint32_t q = 0; q < MSD_PER; q++) {
-            const uint32_t d = threadIdx.x * MSD_PER + q;
-            c[q] = d < nb ? crow[d] : 0;
-            sum += c[q];
-        }
-        uint32_t total;
-        uint32_t pre = block_excl_scan_w<MSD_THREADS / 32>(sum, sh, total);
-#pragma unroll
-        for (uint32_t q = 0; q < MSD_PER; q++) {
-            const uint32_t d = threadIdx.x * MSD_PER + q;
-            if (d < nb) {
-                off[d] = pre;
-                cur[d] = 0;
-            }
-            pre += c[q];
-        }
-    }
-    __syncthreads();
-#pragma unroll 1
-    for (uint32_t r0 = 0; r0 < MSD_ROUNDS; r0 += MSD_BATCH) {
-        uint32_t key[MSD_BATCH];
-#pragma unroll
-        for (uint32_t q = 0; q < MSD_BATCH; q++) {
-            const uint32_t j = (r0 + q) * MSD_THREADS + threadIdx.x;
-            key[q] = j < len ? A[(uint64_t)g.lo + j].x : 0u;
-        }
-#pragma unroll
-        for (uint32_t q = 0; q < MSD_BATCH; q++) {
-            const uint32_t j = (r0 + q) * MSD_THREADS + threadIdx.x;
-            const bool v = j < len;
-            const uint32_t d = (key[q] >> shift) & mask;
-            const uint32_t slot = msd_claim_one(cur, v, d);
-            if (v) stage[off[d] + slot] = (uint16_t)j;
-        }
-    }
-    __syncthreads();
-    for (uint32_t d = threadIdx.x; d < nb; d += MSD_THREADS) off[d] = prow[d] - off[d];
-    __syncthreads();
-    for (uint32_t i = threadIdx.x; i < len; i += MSD_THREADS) {
-        const uint2 v = A[(uint64_t)g.lo + stage[i]];
-        B[(uint64_t)off[(v.x >> shift) & mask] + i] = v;
-    }
-}
-#else
 // Dynamic shared memory of k_msd_scatter: the staged tile and two words per
 // digit.
 constexpr size_t MSD_SCATTER_SMEM = (size_t)MSD_TILE * sizeof(uint2) + 2 * (1u << MSD_MAX_BITS) * sizeof(uint32_t);
@@ -1735,8 +1649,6 @@ static __global__ void __launch_bounds__(MSD_THREADS) k_msd_scatter(const uint2*
         B[(uint64_t)off[(v.x >> shift) & mask] + i] = v;
     }
 }
-
-#endif  // ZKMSM_MSD_INDEX_STAGE
 
 // ------------------------------------------------------------ synthetic inputs
 // Counter-based generator shared with the Python restatement in the oracle:
