@@ -1631,13 +1631,42 @@ static __global__ void __launch_bounds__(MSD_THREADS) k_msd_scatter(const uint2*
             const uint32_t j = (r0 + q) * MSD_THREADS + threadIdx.x;
             e[q] = j < len ? A[(uint64_t)g.lo + j] : make_uint2(0, 0);
         }
+        // the batch's claims in three sweeps, so that its eight shared-memory
+        // atomics are in flight together rather than one after another:
+        // digits and the all-lanes-one-key test, the atomics, the slots
+        const uint32_t lane = threadIdx.x & 31;
+        uint32_t d[MSD_BATCH], m[MSD_BATCH], lk[MSD_BATCH], b[MSD_BATCH];
+        bool one[MSD_BATCH];
 #pragma unroll
         for (uint32_t q = 0; q < MSD_BATCH; q++) {
             const uint32_t j = (r0 + q) * MSD_THREADS + threadIdx.x;
             const bool v = j < len;
-            const uint32_t d = v ? (e[q].x >> shift) & mask : 0u;
-            const uint32_t slot = msd_claim_one(cur, v, d);
-            if (v) stage[off[d] + slot] = e[q];
+            d[q] = v ? (e[q].x >> shift) & mask : 0u;
+            m[q] = __ballot_sync(0xffffffffu, v);
+            const uint32_t leader = m[q] ? __ffs(m[q]) - 1 : 0;
+            lk[q] = __shfl_sync(0xffffffffu, d[q], leader);
+            one[q] = __all_sync(0xffffffffu, !v || d[q] == lk[q]);
+        }
+#pragma unroll
+        for (uint32_t q = 0; q < MSD_BATCH; q++) {
+            const bool v = (m[q] >> lane) & 1u;
+            const uint32_t leader = m[q] ? __ffs(m[q]) - 1 : 0;
+            b[q] = 0;
+            if (one[q]) {
+                if (lane == leader && m[q]) b[q] = atomicAdd(cur + lk[q], (uint32_t)__popc(m[q]));
+            } else if (v) {
+                b[q] = atomicAdd(cur + d[q], 1u);
+            }
+        }
+#pragma unroll
+        for (uint32_t q = 0; q < MSD_BATCH; q++) {
+            const bool v = (m[q] >> lane) & 1u;
+            uint32_t slot = b[q];
+            if (one[q]) {
+                const uint32_t leader = m[q] ? __ffs(m[q]) - 1 : 0;
+                slot = __shfl_sync(0xffffffffu, b[q], leader) + __popc(m[q] & ((1u << lane) - 1));
+            }
+            if (v) stage[off[d[q]] + slot] = e[q];
         }
     }
     __syncthreads();
