@@ -134,12 +134,15 @@ def sort_bytes(n, entries, plan):
     pass the entries read by the count kernel and read and written by the
     scatter (24 B per entry), or per LSD pass read and written by the scatter
     and read by every histogram pass after the first; and the per-tile
-    histograms written once and read and written by their scans."""
+    histograms (MSD: count rows written once and read once, the groups' scan
+    layout written, scanned and read; LSD: written once and read and written
+    by their scans)."""
     msd = plan.get("msd", [0])
     if msd[0]:
-        passes, b1, b2, t1, t2 = msd
-        hist = (1 << b1) * t1 * 4 + ((1 << b2) * t2 * 4 if passes == 2 else 0)
-        return 32 * n + 8 * entries + passes * 24 * entries + 5 * hist
+        passes, b1, b2, t1, t2, g1, ch2 = msd
+        rows = (1 << b1) * t1 * 4 + ((1 << b2) * t2 * 4 if passes == 2 else 0)
+        scan = (1 << b1) * g1 * 2 * 4 + ((1 << b2) * ch2 * 4 if passes == 2 else 0)
+        return 32 * n + 8 * entries + passes * 24 * entries + 2 * rows + 4 * scan
     passes, bits, tiles = plan["sort"][2], plan["sort"][3], plan["sort"][4]
     hist = (1 << bits) * tiles * 4
     return 32 * n + 8 * entries + passes * 16 * entries + max(0, passes - 1) * 8 * entries + passes * 3 * hist

@@ -1,21 +1,25 @@
 """The MSD radix sort of the sorted-entry stage, replayed on the CPU (no GPU).
 
-k_msd_count / k_msd_transpose / k_msd_tiles / k_msd_scatter (msm_kernels.cuh)
-are restated here index for index: tile geometry (pass 1 over [0, E); pass 2
-over the pass-1 segments through the tile table), the count rows, the
-[segment][digit][tile] scan layout and its exclusive scan, the slot rows, and
-each tile's placement (local digit offsets from its count row plus the slot
-of its run).  On random key sets -- uniform,
-skewed (one bucket holding a fifth of the entries, like witness scalars
-equal to 1), with fewer entries than the plan's bound, and empty -- every
-index stays inside its buffer, no output slot is written twice and the
-result is ordered by bucket id.  Plans (digit widths, tile bounds) come from
-the real C++ planner through zkmsm_plan_describe.
+k_msd_count / k_msd_prefix / k_msd_tiles / k_msd_scatter (msm_kernels.cuh)
+are restated here index for index: group geometry (pass 1: the tiles of
+[0, E) split evenly over the plan's groups, each counted in MSD_COUNT_PARTS
+parts; pass 2: chunks of at most MSD_CHUNK_TILES tiles of each pass-1
+segment through the tile and chunk tables), the count rows, the group
+totals written straight into the [segment][digit][group] scan layout and
+its exclusive scan, the slot rows of k_msd_prefix, and each tile's
+placement (local digit offsets from its count row plus the slot of its
+run).  On random key sets -- uniform, skewed (one bucket holding a fifth of
+the entries, like witness scalars equal to 1), with fewer entries than the
+plan's bound, and empty -- every index stays inside its buffer, no output
+slot is written twice and the result is ordered by bucket id.  Plans (digit
+widths, tile and group bounds) come from the real C++ planner through
+zkmsm_plan_describe.
 """
 import ctypes
 import json
 import os
 import re
+import zlib
 
 import numpy as np
 import pytest
@@ -33,6 +37,8 @@ def _const(name):
 
 TILE = _const("MSD_TILE")
 MAX_BITS = _const("MSD_MAX_BITS")
+PARTS = _const("MSD_COUNT_PARTS")
+CHUNK = _const("MSD_CHUNK_TILES")
 
 
 def plan(counts, curve=0):
@@ -48,12 +54,53 @@ def excl_scan(h):
     return out
 
 
-def geom(t, E, ntiles, seg_start, seg_tile, nb):
-    if seg_tile is None:
-        if t >= ntiles:
+def group(u, E, ng, sub, whole, seg_start, seg_tile, seg_chunk, nb):
+    """msd_group: (lo, hi, row0, sidx, sstride) of unit u, or None."""
+    if seg_chunk is None:
+        grp, part = (u, 0) if whole else (u // sub, u % sub)
+        if grp >= ng:
             return None
-        lo = min(t * TILE, E)
-        return lo, min(lo + TILE, E), t, ntiles, 0
+        nt = (E + TILE - 1) // TILE
+        K = (nt + ng - 1) // ng
+        Ks = (K + sub - 1) // sub
+        gend = (grp + 1) * K
+        t0, t1 = grp * K, gend
+        if not whole:
+            t0 += part * Ks
+            t1 = min(t0 + Ks, gend)
+        t1 = min(t1, nt)
+        t0 = min(t0, t1)
+        return min(t0 * TILE, E), min(t1 * TILE, E), t0, grp * sub + part, ng * sub
+    nseg = len(seg_chunk) - 1
+    if u >= seg_chunk[nseg]:
+        return None
+    a, b = 0, nseg - 1
+    while a < b:
+        mid = (a + b + 1) >> 1
+        if seg_chunk[mid] <= u:
+            a = mid
+        else:
+            b = mid - 1
+    k = u - seg_chunk[a]
+    lo = seg_start[a] + k * CHUNK * TILE
+    end = seg_start[a + 1]
+    assert lo < end, "chunk starts past its segment"
+    hi = min(end, lo + CHUNK * TILE)
+    row0 = seg_tile[a] + k * CHUNK
+    assert row0 + (hi - lo + TILE - 1) // TILE <= seg_tile[a + 1], "chunk rows spill into the next segment"
+    return lo, hi, row0, seg_chunk[a] * nb + k, seg_chunk[a + 1] - seg_chunk[a]
+
+
+def tiles_of(g):
+    lo, hi, row0 = g[0], g[1], g[2]
+    return [(t0, min(t0 + TILE, hi), row0 + j) for j, t0 in enumerate(range(lo, hi, TILE))]
+
+
+def tile_range(t, E, seg):
+    """msd_tile: (lo, hi) of tile t, or None past the pass-2 tiles."""
+    if seg is None:
+        return min(t * TILE, E), min(t * TILE + TILE, E)
+    seg_start, seg_tile, _ = seg
     nseg = len(seg_tile) - 1
     if t >= seg_tile[nseg]:
         return None
@@ -64,55 +111,61 @@ def geom(t, E, ntiles, seg_start, seg_tile, nb):
             a = mid
         else:
             b = mid - 1
-    k = t - seg_tile[a]
-    nt = seg_tile[a + 1] - seg_tile[a]
-    lo = seg_start[a] + k * TILE
+    lo = seg_start[a] + (t - seg_tile[a]) * TILE
     assert lo < seg_start[a + 1], "tile starts past its segment"
-    return lo, min(seg_start[a + 1], lo + TILE), k, nt, seg_tile[a] * nb
+    return lo, min(seg_start[a + 1], lo + TILE)
 
 
-def msd_pass(keys, vals, E, shift, bits, ntiles, seg_start, seg_tile, hsize, grid):
-    """One pass as the device runs it: k_msd_count (rows C[tile][digit]),
-    k_msd_transpose to the scan layout S, the exclusive scan, the transpose
-    back to slot rows P, k_msd_scatter (local offsets from the tile's C row,
-    run slots from its P row)."""
+def msd_pass(keys, vals, E, shift, bits, ng, sub, ntiles, seg, rows_size, scan_size):
+    """One pass as the device runs it: k_msd_count over ng*sub units (count
+    rows C[tile][digit], unit totals into the scan layout S), the exclusive
+    scan of S over its bound, k_msd_prefix over ng groups (slot rows
+    P[tile][digit]), k_msd_scatter over the `ntiles` tile bound (local
+    offsets from the tile's C row, run slots from its P row)."""
     nb = 1 << bits
-    C = np.full(hsize, 5, dtype=np.int64)  # stale contents everywhere
-    S = np.full(hsize, 7, dtype=np.int64)
-    P = np.full(hsize, 9, dtype=np.int64)
-    geoms = [geom(t, E, ntiles, seg_start, seg_tile, nb) for t in range(grid)]
-    for t, g in enumerate(geoms):  # k_msd_count
+    seg_start, seg_tile, seg_chunk = seg if seg else (None, None, None)
+    C = np.full(rows_size, 5, dtype=np.int64)  # stale contents everywhere
+    P = np.full(rows_size, 9, dtype=np.int64)
+    S = np.full(scan_size, 7, dtype=np.int64)
+    used = np.zeros(scan_size, dtype=bool)
+    rows_seen = {}
+    for u in range(ng * sub):  # k_msd_count
+        g = group(u, E, ng, sub, False, seg_start, seg_tile, seg_chunk, nb)
         if g is None:
             continue
-        lo, hi, k, nt, hb = g
-        assert (t + 1) * nb <= hsize
-        C[t * nb:(t + 1) * nb] = np.bincount((keys[lo:hi] >> shift) & (nb - 1), minlength=nb)
-    used = np.zeros(hsize, dtype=bool)
-    for t, g in enumerate(geoms):  # k_msd_transpose, rows -> scan layout
-        if g is None:
-            continue
-        lo, hi, k, nt, hb = g
-        idx = hb + np.arange(nb) * nt + k
-        assert idx.max() < hsize and not used[idx].any()
+        tot = np.zeros(nb, dtype=np.int64)
+        for lo, hi, row in tiles_of(g):
+            assert (row + 1) * nb <= rows_size and row not in rows_seen
+            rows_seen[row] = (lo, hi)
+            C[row * nb:(row + 1) * nb] = np.bincount((keys[lo:hi] >> shift) & (nb - 1), minlength=nb)
+            tot += C[row * nb:(row + 1) * nb]
+        idx = g[3] + np.arange(nb) * g[4]
+        assert idx.max() < scan_size and not used[idx].any()
         used[idx] = True
-        S[idx] = C[t * nb:(t + 1) * nb]
+        S[idx] = tot
     n_used = int(used.sum())
-    assert used[:n_used].all(), "pass counts are not a prefix of the scan layout"
-    S[:grid * nb] = excl_scan(S[:grid * nb])  # the scan runs over the bound
-    for t, g in enumerate(geoms):  # k_msd_transpose back, scan layout -> slot rows
+    assert used[:n_used].all(), "group totals are not a prefix of the scan layout"
+    S[:nb * ng * sub] = excl_scan(S[:nb * ng * sub])  # the scan runs over the bound
+    for u in range(ng):  # k_msd_prefix
+        g = group(u, E, ng, sub, True, seg_start, seg_tile, seg_chunk, nb)
         if g is None:
             continue
-        lo, hi, k, nt, hb = g
-        P[t * nb:(t + 1) * nb] = S[hb + np.arange(nb) * nt + k]
+        run = S[g[3] + np.arange(nb) * g[4]].copy()
+        for lo, hi, row in tiles_of(g):
+            P[row * nb:(row + 1) * nb] = run
+            run = run + C[row * nb:(row + 1) * nb]
     outk = np.full(E, -1, dtype=np.int64)
     outv = np.full(E, -1, dtype=np.int64)
-    for t, g in enumerate(geoms):  # k_msd_scatter
-        if g is None or g[0] == g[1]:
+    for t in range(ntiles):  # k_msd_scatter
+        r = tile_range(t, E, seg)
+        if r is None or r[0] == r[1]:
             continue
-        lo, hi, k, nt, hb = g
+        lo, hi = r
+        assert rows_seen.get(t) == (lo, hi), "rows of tile %d were written for another range" % t
         d = (keys[lo:hi] >> shift) & (nb - 1)
-        off = excl_scan(C[t * nb:(t + 1) * nb])
-        perm = np.random.default_rng(t).permutation(hi - lo)  # any order inside a digit
+        cnt = C[t * nb:(t + 1) * nb]
+        off = excl_scan(cnt)
+        perm = np.random.default_rng(lo).permutation(hi - lo)  # any order inside a digit
         order = perm[np.argsort(d[perm], kind="stable")]
         dd = d[order]
         dst = P[t * nb + dd] - off[dd] + np.arange(hi - lo)
@@ -124,37 +177,43 @@ def msd_pass(keys, vals, E, shift, bits, ntiles, seg_start, seg_tile, hsize, gri
     return outk, outv, S
 
 
-def msd_tiles(Hs, ntiles1, nseg, E):
-    seg_start = [int(Hs[s * ntiles1]) for s in range(nseg)] + [E]
+def msd_tiles(S1, stride1, nseg, E):
+    seg_start = [int(S1[s * stride1]) for s in range(nseg)] + [E]
     nt = [(seg_start[s + 1] - seg_start[s] + TILE - 1) // TILE for s in range(nseg)]
-    seg_tile = [0] + list(np.cumsum(nt))
-    return seg_start, [int(x) for x in seg_tile]
+    nc = [(t + CHUNK - 1) // CHUNK for t in nt]
+    seg_tile = [0] + [int(x) for x in np.cumsum(nt)]
+    seg_chunk = [0] + [int(x) for x in np.cumsum(nc)]
+    return seg_start, seg_tile, seg_chunk
 
 
 def run_msd(pl, keys):
-    passes, b1, b2, t1, t2 = pl["msd"]
+    passes, b1, b2, t1, t2, g1, ch2 = pl["msd"]
     E = len(keys)
     assert E <= pl["entry_bound"]
     vals = np.arange(E, dtype=np.int64)
-    hsize = max((1 << b1) * t1, (1 << b2) * t2 if passes == 2 else 0)
+    rows = max((1 << b1) * t1, (1 << b2) * t2 if passes == 2 else 0)
+    scan = max((1 << b1) * g1 * PARTS, (1 << b2) * ch2 if passes == 2 else 0)
     shift1 = b2 if passes == 2 else 0
-    k1, v1, Hs = msd_pass(keys, vals, E, shift1, b1, t1, None, None, hsize, t1)
+    k1, v1, S1 = msd_pass(keys, vals, E, shift1, b1, g1, PARTS, t1, None, rows, scan)
     if passes == 1:
         return k1, v1
-    seg_start, seg_tile = msd_tiles(Hs, t1, 1 << b1, E)
-    assert seg_tile[-1] <= t2, "pass-2 tiles exceed the bound the grid is launched for"
-    return msd_pass(k1, v1, E, 0, b2, 0, seg_start, seg_tile, hsize, t2)[:2]
+    seg = msd_tiles(S1, g1 * PARTS, 1 << b1, E)
+    assert seg[1][-1] <= t2, "pass-2 tiles exceed the count rows"
+    assert seg[2][-1] <= ch2, "pass-2 chunks exceed the bound the grid is launched for"
+    return msd_pass(k1, v1, E, 0, b2, ch2, 1, t2, seg, rows, scan)[:2]
 
 
 @pytest.mark.parametrize("counts", [[1 << 20], [1 << 24], [(1 << 21) + 77], [4096, 1 << 20, 333, 1 << 19]])
 def test_plans_choose_msd_within_limits(counts):
     pl = plan(counts)
-    passes, b1, b2, t1, t2 = pl["msd"]
+    passes, b1, b2, t1, t2, g1, ch2 = pl["msd"]
     kb = max(1, (pl["nbuckets"] - 1).bit_length())
     assert passes in (1, 2) and b1 + b2 == kb and max(b1, b2) <= MAX_BITS
     assert t1 * TILE >= pl["entry_bound"]
+    assert 1 <= g1 <= min(t1, 148)
     if passes == 2:
         assert t2 == t1 + (1 << b1)
+        assert ch2 == (t2 + CHUNK - 1) // CHUNK + (1 << b1)
 
 
 @pytest.mark.parametrize("case", ["uniform", "hot", "sparse", "empty"])
@@ -162,7 +221,7 @@ def test_msd_sort_replay(case):
     pl = plan([1 << 19])  # a real two-pass plan (18-bit bucket ids)
     assert pl["msd"][0] == 2
     G = pl["nbuckets"]
-    rng = np.random.default_rng(hash(case) & 0xFFFF)
+    rng = np.random.default_rng(zlib.crc32(case.encode()))
     bound = pl["entry_bound"]
     if case == "uniform":
         E = bound - 12345

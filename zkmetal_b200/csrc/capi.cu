@@ -1028,7 +1028,8 @@ static ZkMetalStatus plan_json(int curve, const uint32_t* counts, uint32_t n_msm
              std::to_string(pl.sort_passes) + "," + std::to_string(pl.sort_bits) + "," +
              std::to_string(pl.sort_tiles) + "],\"msd\":[" + std::to_string(pl.msd_passes) + "," +
              std::to_string(pl.msd_bits1) + "," + std::to_string(pl.msd_bits2) + "," + std::to_string(pl.msd_tiles1) +
-             "," + std::to_string(pl.msd_tiles2) + "],\"acc\":[";
+             "," + std::to_string(pl.msd_tiles2) + "," + std::to_string(pl.msd_groups1) + "," +
+             std::to_string(pl.msd_chunks2) + "],\"acc\":[";
         for (size_t l = 0; l < pl.acc_K.size(); l++)
             s += (l ? "," : "") + std::string("[") + std::to_string(pl.acc_K[l]) + "," + std::to_string(pl.acc_T[l]) +
                  "," + std::to_string(pl.acc_Mbound[l]) + "]";

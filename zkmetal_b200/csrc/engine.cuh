@@ -239,6 +239,8 @@ struct Tuning {
     // threads of the level-1 accumulation kernel resident at once on the
     // device, per curve (0: unknown; then chunks are not wave-aligned)
     uint32_t acc_wave[NCURVES] = {};
+    // SMs of the device (the MSD sort's first pass runs one group per SM)
+    uint32_t sms = 148;
 };
 
 // Host description of one batch run.
@@ -255,8 +257,10 @@ struct Plan {
     uint32_t sort_maxd = 0, sort_spb = 0, sort_passes = 0, sort_bits = 0, sort_tiles = 0;
     // MSD sort instead (msd_passes 1 or 2; 0: the LSD passes above): digit
     // widths of the passes (the first takes the top bits), tile-count
-    // bounds of the passes (pass 2: one partial tile more per segment)
+    // bounds of the passes (pass 2: one partial tile more per segment), the
+    // scatter groups of pass 1 and the chunk-count bound of pass 2
     uint32_t msd_passes = 0, msd_bits1 = 0, msd_bits2 = 0, msd_tiles1 = 0, msd_tiles2 = 0;
+    uint32_t msd_groups1 = 0, msd_chunks2 = 0;
     // segmented-sum levels: chunk length and chunk-count bound per level
     std::vector<uint32_t> acc_K, acc_T;
     std::vector<uint64_t> acc_Mbound;
@@ -278,6 +282,7 @@ struct Plan {
         nbuckets = nwin_total = 0;
         sort_maxd = sort_spb = sort_passes = sort_bits = sort_tiles = 0;
         msd_passes = msd_bits1 = msd_bits2 = msd_tiles1 = msd_tiles2 = 0;
+        msd_groups1 = msd_chunks2 = 0;
         red_L = 8;
         red_log2L = 3;
         acc_threads = 0;
@@ -290,6 +295,18 @@ struct Plan {
         graph_misses = 0;
     }
 };
+
+// Words of the MSD sort's count rows (one row per tile, the larger pass; the
+// slot rows are as large) and of its scan layout (one word per digit and group: pass-1 groups in
+// MSD_COUNT_PARTS parts, pass-2 chunks).
+inline uint64_t msd_rows_words(const Plan& pl) {
+    return std::max<uint64_t>((uint64_t)(1u << pl.msd_bits1) * pl.msd_tiles1,
+                              pl.msd_passes == 2 ? (uint64_t)(1u << pl.msd_bits2) * pl.msd_tiles2 : 0);
+}
+inline uint64_t msd_scan_words(const Plan& pl) {
+    return std::max<uint64_t>((uint64_t)(1u << pl.msd_bits1) * pl.msd_groups1 * MSD_COUNT_PARTS,
+                              pl.msd_passes == 2 ? (uint64_t)(1u << pl.msd_bits2) * pl.msd_chunks2 : 0);
+}
 
 // Nearest power-of-two exponent of n (n >= 1).
 inline int nearest_log2(uint64_t n) {
@@ -597,6 +614,10 @@ class Engine {
 
     Engine() {
         ZK_CUDA(cudaGetDevice(&device));
+        int sms = 0;
+        if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) == cudaSuccess && sms > 0)
+            tuning.sms = (uint32_t)sms;
+        cudaGetLastError();
         ZK_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
         bind_workspace_stream();
         tuning.acc_wave[0] = acc_resident_threads<Bn254>();
@@ -771,6 +792,11 @@ class Engine {
                 pl.msd_bits2 = kb - (pl.msd_passes == 1 ? kb : pl.msd_bits1);
                 pl.msd_tiles1 = (uint32_t)((pl.entry_bound + MSD_TILE - 1) / MSD_TILE);
                 pl.msd_tiles2 = pl.msd_passes == 2 ? pl.msd_tiles1 + (1u << pl.msd_bits1) : 0;
+                pl.msd_groups1 = std::max<uint32_t>(1, std::min<uint32_t>(tuning.sms, pl.msd_tiles1));
+                // sum over segments of ceil(tiles / chunk) <= tiles / chunk + segments
+                pl.msd_chunks2 = pl.msd_passes == 2
+                                         ? (pl.msd_tiles2 + MSD_CHUNK_TILES - 1) / MSD_CHUNK_TILES + (1u << pl.msd_bits1)
+                                         : 0;
             }
         }
         // autotuned schedule of the plan's largest MSM, if any
@@ -949,12 +975,11 @@ class Engine {
         grew |= w_ents.ensure(pl.entry_bound * 8 + 16);
         uint64_t hsz = (uint64_t)(1u << pl.sort_bits) * pl.sort_tiles;
         if (pl.msd_passes) {
-            hsz = std::max<uint64_t>((uint64_t)(1u << pl.msd_bits1) * pl.msd_tiles1,
-                                     pl.msd_passes == 2 ? (uint64_t)(1u << pl.msd_bits2) * pl.msd_tiles2 : 0);
-            grew |= w_seg.ensure(((size_t)2 << pl.msd_bits1) * 4 + 64);
+            // count and slot rows of every tile, then the scan layout of the groups
+            hsz = 2 * msd_rows_words(pl) + msd_scan_words(pl);
+            grew |= w_seg.ensure(((size_t)3 << pl.msd_bits1) * 4 + 64);
         }
-        // the MSD sort keeps three histogram-sized arrays (rows, scan layout, slots)
-        const uint64_t hwords = pl.msd_passes ? 3 * hsz : hsz;
+        const uint64_t hwords = hsz;
         grew |= w_ents2.ensure(pl.entry_bound * 8 + 16);
         grew |= w_thist.ensure(hwords * 4 + 16);
         grew |= w_buckets.ensure((size_t)pl.nbuckets * xs + xs);

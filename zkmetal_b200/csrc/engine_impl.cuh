@@ -30,8 +30,9 @@ static void scan_u32(Engine& e, uint32_t* d_in_out, uint32_t n, uint32_t* d_tota
 
 
 // MSD sort of the entries in A by bucket id (tot[0] entries): one or two
-// passes, each k_msd_count, an exclusive scan of the tile counts and
-// k_msd_scatter; after two passes the result is back in A, after one in B.
+// passes, each k_msd_count, an exclusive scan of the group totals,
+// k_msd_prefix and k_msd_scatter; after two passes the result is back in A,
+// after one in B.
 static void msd_scatter_attr(int device) {
     // the staged tile needs more than the default 48 KB of dynamic shared
     // memory; set once per device for this unit's copy of the kernel
@@ -46,40 +47,41 @@ static void msd_scatter_attr(int device) {
 template <class C>
 void Engine::msd_sort(const Plan& pl, uint2* A, uint2* B, uint32_t* tot) {
     msd_scatter_attr(device);
-    const uint32_t b1 = pl.msd_bits1, b2 = pl.msd_bits2, t1 = pl.msd_tiles1, t2 = pl.msd_tiles2;
-    // three arrays of the larger pass's histogram size: counts as rows (C),
-    // the scan layout (S), the scanned slots as rows (P)
-    const uint64_t hsz = std::max<uint64_t>((uint64_t)(1u << b1) * t1, pl.msd_passes == 2 ? (uint64_t)(1u << b2) * t2 : 0);
+    const uint32_t b1 = pl.msd_bits1, b2 = pl.msd_bits2, G = pl.msd_groups1, CH = pl.msd_chunks2;
+    // count rows (C) and slot rows (P) of every tile, then the scan layout
+    // of the groups (S)
     uint32_t* Cr = w_thist.as<uint32_t>();
-    uint32_t* S = Cr + hsz;
-    uint32_t* P = S + hsz;
+    uint32_t* P = Cr + msd_rows_words(pl);
+    uint32_t* S = P + msd_rows_words(pl);
     const uint32_t nseg = 1u << b1;
     uint32_t* seg_start = w_seg.as<uint32_t>();
     uint32_t* seg_tile = seg_start + nseg + 1;
-    auto pass = [&](const uint2* src, uint2* dst, uint32_t shift, uint32_t bits, uint32_t grid, uint32_t ntiles,
-                    const uint32_t* ss, const uint32_t* st, uint32_t ns) {
+    uint32_t* seg_chunk = seg_tile + nseg + 1;
+    // pass 1: G groups of MSD_COUNT_PARTS count parts over the tile bound;
+    // pass 2: the chunk and tile bounds (blocks past the real chunks and
+    // tiles return at once)
+    auto pass = [&](const uint2* src, uint2* dst, uint32_t shift, uint32_t bits, uint32_t ng, uint32_t sub,
+                    uint32_t ntiles, const uint32_t* ss, const uint32_t* st, const uint32_t* sc, uint32_t ns) {
         const uint32_t nb = 1u << bits;
-        const dim3 tg((grid + MSD_TR - 1) / MSD_TR, (nb + MSD_TR - 1) / MSD_TR), tb(MSD_TR, 8);
-        k_msd_count<<<grid, MSD_THREADS, 0, stream>>>(src, tot + 0, shift, bits, ntiles, ss, st, ns, Cr);
-        k_msd_transpose<<<tg, tb, 0, stream>>>(Cr, S, tot + 0, bits, ntiles, ss, st, ns, 1);
-        launches += 2;
+        k_msd_count<<<ng * sub, MSD_THREADS, 0, stream>>>(src, tot + 0, shift, bits, ng, sub, ss, st, sc, ns, Cr, S);
+        launches++;
         ZK_CUDA(cudaGetLastError());
-        // pass-2 counts fill a prefix of S (tiles in segment order); the scan
-        // runs over the bound, and whatever lies past the prefix only shifts
-        // slots past it
-        scan_u32(*this, S, nb * grid, tot + 63, nullptr);
-        k_msd_transpose<<<tg, tb, 0, stream>>>(P, S, tot + 0, bits, ntiles, ss, st, ns, 0);
-        k_msd_scatter<<<grid, MSD_THREADS, MSD_SCATTER_SMEM, stream>>>(src, tot + 0, shift, bits, ntiles, ss, st,
-                                                                      ns, Cr, P, dst);
+        // pass-2 totals fill a prefix of S (chunks in segment order); the
+        // scan runs over the bound, and whatever lies past the prefix only
+        // shifts slots past it
+        scan_u32(*this, S, (uint64_t)nb * ng * sub, tot + 63, nullptr);
+        k_msd_prefix<<<ng, MSD_THREADS, 0, stream>>>(tot + 0, bits, ng, sub, ss, st, sc, ns, Cr, S, P);
+        k_msd_scatter<<<ntiles, MSD_THREADS, MSD_SCATTER_SMEM, stream>>>(src, tot + 0, shift, bits, ntiles, ss, st,
+                                                                        ns, Cr, P, dst);
         launches += 2;
         ZK_CUDA(cudaGetLastError());
     };
-    pass(A, B, pl.msd_passes == 2 ? b2 : 0, b1, t1, t1, nullptr, nullptr, 0);
+    pass(A, B, pl.msd_passes == 2 ? b2 : 0, b1, G, MSD_COUNT_PARTS, pl.msd_tiles1, nullptr, nullptr, nullptr, 0);
     if (pl.msd_passes < 2) return;
-    k_msd_tiles<<<1, MSD_THREADS, 0, stream>>>(S, t1, nseg, tot + 0, seg_start, seg_tile);
+    k_msd_tiles<<<1, MSD_THREADS, 0, stream>>>(S, G * MSD_COUNT_PARTS, nseg, tot + 0, seg_start, seg_tile, seg_chunk);
     launches++;
     ZK_CUDA(cudaGetLastError());
-    pass(B, A, 0, b2, t2, 0, seg_start, seg_tile, nseg);
+    pass(B, A, 0, b2, CH, 1, pl.msd_tiles2, seg_start, seg_tile, seg_chunk, nseg);
 }
 
 // ------------------------------------------------------------ pipeline

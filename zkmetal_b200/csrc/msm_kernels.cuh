@@ -1332,65 +1332,91 @@ static __global__ void __launch_bounds__(SCAN_THREADS) k_scan_add(uint32_t* __re
 // stability -- entries of one bucket may come out in any order, since bucket
 // sums do not depend on it -- so a tile ranks its entries by digit with
 // shared-memory atomics instead of the per-bit ballots a stable LSD pass
-// needs.  Per pass, over tiles of at most MSD_TILE entries that never
+// needs.  A pass runs over tiles of at most MSD_TILE entries that never
 // straddle a segment (pass 1: the whole array is one segment; pass 2: one
-// segment per pass-1 digit):
-//  k_msd_count      each tile's digit counts, one contiguous row per tile:
-//                   C[tile][digit];
-//  k_msd_transpose  (to the scan layout) segment by segment, digit-major
-//                   inside a segment: S[seg][digit][tile of seg], the output
-//                   order, so that an exclusive scan of S gives each
-//                   (seg, digit, tile) its first output slot;
+// segment per pass-1 digit), and the tiles come in groups of consecutive
+// tiles of one segment (pass 1: the tiles split evenly over `ng` groups,
+// about one per SM; pass 2: chunks of at most MSD_CHUNK_TILES tiles of a
+// segment).  Output order inside a segment: digit, then group, then tile.
+//  k_msd_count      each tile's digit counts as a contiguous row C[tile][digit],
+//                   and the group's digit totals straight into the scan
+//                   layout S[seg][digit][group of seg], so that an exclusive
+//                   scan of S gives each (seg, digit, group) the first output
+//                   slot of its run (pass 1 counts each group in `sub` parts,
+//                   S[digit][group][part], so that two count blocks share an
+//                   SM);
 //  scan;
-//  k_msd_transpose  (back) the slots as rows again: P[tile][digit];
+//  k_msd_prefix     per group: the slot rows P[tile][digit], the group's
+//                   scanned slot plus the counts of its earlier tiles;
 //  k_msd_tiles      (between the passes) the segment starts, read from the
-//                   pass-1 scan, and the pass-2 tile table;
-//  k_msd_scatter    reads its tile's two rows (counts -> local offsets, and
-//                   slots), places the tile in digit order in shared memory
-//                   and writes it out as one run per digit.
-// Rows keep every per-tile read and write contiguous; the transposes move
-// 32 x 32 blocks through shared memory.
+//                   pass-1 scan, and the pass-2 tile and chunk tables;
+//  k_msd_scatter    one block per tile: reads its count row (local offsets)
+//                   and slot row, places the tile in digit order in shared
+//                   memory and writes it out as one run per digit.
+// The scan layout holds one word per group and digit (pass 1: 2.4 MB at any
+// size), not one per tile, so the tile rows never need transposing; the
+// scatter keeps one block per tile because blocks placing neighbouring
+// tiles at the same time write their runs of a digit side by side (one block
+// placing a whole group wrote 148 x 4096 separate fronts at 2^24 points and
+// took 2.10 ms against 1.28 ms for pass 1).
 // Replaces the reference's CPU counting sort per window (MSMEngine.swift:595-661).
 
-// Tile t of a pass.  Pass 1 (seg_tile == nullptr): [t*MSD_TILE, ...) of
-// [0, E) in the scan layout of one segment of `ntiles` tiles (tiles past E
-// are empty and count zeros).  Pass 2: the segment owning t in the tile
-// table seg_tile (exclusive prefix of tiles per segment, nseg + 1 entries)
-// with segment starts seg_start (nseg + 1 entries, the last one E).  hbase,
-// nt and k place the tile's counts in the scan layout: S[hbase + digit*nt +
-// k].  False past the last tile.
-struct MsdGeom {
-    uint32_t lo, hi, k, nt;
-    uint64_t hbase;
+// Group (or, for the count kernel of pass 1, part of a group) u of a pass.
+// Pass 1 (seg_chunk == nullptr): the ceil(E / MSD_TILE) tiles of [0, E) are
+// split into `ng` groups of K = ceil(tiles / ng) tiles, each counted in
+// `sub` parts of ceil(K / sub) tiles; the count kernel runs ng*sub units
+// (u = group*sub + part), the scatter ng (u = group, whole groups, part 0's
+// scan slot).  Every unit exists (groups past the last tile are empty and
+// count zeros).  Pass 2: chunk u of the chunk table seg_chunk (exclusive
+// prefix of chunks per segment, nseg + 1 entries), with the tile table
+// seg_tile and segment starts seg_start (nseg + 1 entries each, the last
+// start E); false past the last chunk.  lo..hi: the entries; row0: the
+// count row of the first tile; S[sidx + digit*sstride]: the unit's slot in
+// the scan layout.
+struct MsdGroup {
+    uint32_t lo, hi, row0, sstride;
+    uint64_t sidx;
 };
 
-ZK_DEV bool msd_geom(uint32_t t, uint32_t E, uint32_t ntiles, const uint32_t* __restrict__ seg_start,
-                     const uint32_t* __restrict__ seg_tile, uint32_t nseg, uint32_t nb, MsdGeom& g) {
-    if (!seg_tile) {
-        if (t >= ntiles) return false;
-        const uint64_t lo = (uint64_t)t * MSD_TILE;
-        g.lo = (uint32_t)(lo < E ? lo : E);
-        g.hi = (uint32_t)(lo + MSD_TILE < E ? lo + MSD_TILE : E);
-        g.k = t;
-        g.nt = ntiles;
-        g.hbase = 0;
+ZK_DEV bool msd_group(uint32_t u, uint32_t E, uint32_t ng, uint32_t sub, bool whole,
+                      const uint32_t* __restrict__ seg_start, const uint32_t* __restrict__ seg_tile,
+                      const uint32_t* __restrict__ seg_chunk, uint32_t nseg, uint32_t nb, MsdGroup& g) {
+    if (!seg_chunk) {
+        const uint32_t grp = whole ? u : u / sub, part = whole ? 0 : u % sub;
+        if (grp >= ng) return false;
+        const uint32_t nt = (uint32_t)(((uint64_t)E + MSD_TILE - 1) / MSD_TILE);
+        const uint32_t K = (nt + ng - 1) / ng, Ks = (K + sub - 1) / sub;
+        const uint64_t gend = (uint64_t)(grp + 1) * K;
+        uint64_t t0 = (uint64_t)grp * K, t1 = gend;
+        if (!whole) {
+            t0 += (uint64_t)part * Ks;
+            t1 = t0 + Ks < gend ? t0 + Ks : gend;
+        }
+        if (t1 > nt) t1 = nt;
+        if (t0 > t1) t0 = t1;
+        g.row0 = (uint32_t)t0;
+        g.lo = (uint32_t)(t0 * MSD_TILE < E ? t0 * MSD_TILE : E);
+        g.hi = (uint32_t)(t1 * MSD_TILE < E ? t1 * MSD_TILE : E);
+        g.sidx = (uint64_t)grp * sub + part;
+        g.sstride = ng * sub;
         return true;
     }
-    if (t >= seg_tile[nseg]) return false;
-    // the last segment whose first tile is at or below t (empty segments
-    // before it share its first-tile index and are skipped)
+    if (u >= seg_chunk[nseg]) return false;
+    // the last segment whose first chunk is at or below u (empty segments
+    // before it share its first-chunk index and are skipped)
     uint32_t a = 0, b = nseg - 1;
     while (a < b) {
         const uint32_t mid = (a + b + 1) >> 1;
-        if (seg_tile[mid] <= t) a = mid;
+        if (seg_chunk[mid] <= u) a = mid;
         else b = mid - 1;
     }
-    g.k = t - seg_tile[a];
-    g.nt = seg_tile[a + 1] - seg_tile[a];
-    g.hbase = (uint64_t)seg_tile[a] * nb;
-    g.lo = seg_start[a] + g.k * MSD_TILE;
+    const uint32_t k = u - seg_chunk[a];
+    g.row0 = seg_tile[a] + k * MSD_CHUNK_TILES;
+    g.lo = seg_start[a] + k * (MSD_CHUNK_TILES * MSD_TILE);
     const uint32_t end = seg_start[a + 1];
-    g.hi = g.lo + MSD_TILE < end ? g.lo + MSD_TILE : end;
+    g.hi = end - g.lo > MSD_CHUNK_TILES * MSD_TILE ? g.lo + MSD_CHUNK_TILES * MSD_TILE : end;
+    g.sidx = (uint64_t)seg_chunk[a] * nb + k;
+    g.sstride = seg_chunk[a + 1] - seg_chunk[a];
     return true;
 }
 
@@ -1460,126 +1486,180 @@ constexpr uint32_t MSD_PER = (1u << MSD_MAX_BITS) / MSD_THREADS;  // digits per 
 
 static __global__ void __launch_bounds__(MSD_THREADS) k_msd_count(const uint2* __restrict__ A,
                                                                  const uint32_t* __restrict__ d_total,
-                                                                 uint32_t shift, uint32_t bits, uint32_t ntiles,
+                                                                 uint32_t shift, uint32_t bits, uint32_t ng,
+                                                                 uint32_t sub,
                                                                  const uint32_t* __restrict__ seg_start,
                                                                  const uint32_t* __restrict__ seg_tile,
-                                                                 uint32_t nseg, uint32_t* __restrict__ C) {
+                                                                 const uint32_t* __restrict__ seg_chunk,
+                                                                 uint32_t nseg, uint32_t* __restrict__ C,
+                                                                 uint32_t* __restrict__ S) {
     __shared__ uint32_t cnt[1u << MSD_MAX_BITS];
     const uint32_t nb = 1u << bits, mask = nb - 1;
-    MsdGeom g;
-    if (!msd_geom(blockIdx.x, *d_total, ntiles, seg_start, seg_tile, nseg, nb, g)) return;
+    MsdGroup g;
+    if (!msd_group(blockIdx.x, *d_total, ng, sub, false, seg_start, seg_tile, seg_chunk, nseg, nb, g)) return;
     for (uint32_t i = threadIdx.x; i < nb; i += MSD_THREADS) cnt[i] = 0;
     __syncthreads();
-    const uint32_t len = g.hi - g.lo;
+    uint32_t tot[MSD_PER];
+#pragma unroll
+    for (uint32_t q = 0; q < MSD_PER; q++) tot[q] = 0;
+    uint32_t row = g.row0;
 #pragma unroll 1
-    for (uint32_t r0 = 0; r0 < MSD_ROUNDS; r0 += MSD_BATCH) {
-        uint32_t key[MSD_BATCH];
+    for (uint32_t t0 = g.lo; t0 < g.hi; t0 += MSD_TILE, row++) {
+        const uint32_t len = g.hi - t0 < MSD_TILE ? g.hi - t0 : MSD_TILE;
+#pragma unroll 1
+        for (uint32_t r0 = 0; r0 * MSD_THREADS < len; r0 += MSD_BATCH) {
+            uint32_t key[MSD_BATCH];
 #pragma unroll
-        for (uint32_t q = 0; q < MSD_BATCH; q++) {
-            const uint32_t j = (r0 + q) * MSD_THREADS + threadIdx.x;
-            key[q] = j < len ? (A[(uint64_t)g.lo + j].x >> shift) & mask : 0xffffffffu;
-        }
+            for (uint32_t q = 0; q < MSD_BATCH; q++) {
+                const uint32_t j = (r0 + q) * MSD_THREADS + threadIdx.x;
+                key[q] = j < len ? (A[(uint64_t)t0 + j].x >> shift) & mask : 0xffffffffu;
+            }
 #pragma unroll
-        for (uint32_t q = 0; q < MSD_BATCH; q++) msd_count_one(cnt, key[q] != 0xffffffffu, key[q]);
-    }
-    __syncthreads();
-    uint32_t* row = C + (uint64_t)blockIdx.x * nb;
-    for (uint32_t d = threadIdx.x; d < nb; d += MSD_THREADS) row[d] = cnt[d];
-}
-
-// Between the row layout R[tile][digit] and the scan layout S (see
-// msd_geom), for the tiles of a pass: to_scan 1 copies R -> S, 0 copies
-// S -> R.  Blocks of 32 tiles x 32 digits go through shared memory so that
-// both sides are read and written along their contiguous dimension.
-constexpr uint32_t MSD_TR = 32;
-static __global__ void __launch_bounds__(MSD_TR * 8) k_msd_transpose(uint32_t* __restrict__ R,
-                                                                    uint32_t* __restrict__ S,
-                                                                    const uint32_t* __restrict__ d_total,
-                                                                    uint32_t bits, uint32_t ntiles,
-                                                                    const uint32_t* __restrict__ seg_start,
-                                                                    const uint32_t* __restrict__ seg_tile,
-                                                                    uint32_t nseg, int to_scan) {
-    __shared__ uint32_t blk[MSD_TR][MSD_TR + 1];
-    __shared__ uint64_t row_base[MSD_TR];  // hbase + k of each tile row (~0: no tile)
-    __shared__ uint32_t row_nt[MSD_TR];
-    const uint32_t nb = 1u << bits;
-    const uint32_t t0 = blockIdx.x * MSD_TR, d0 = blockIdx.y * MSD_TR;
-    const uint32_t tx = threadIdx.x, ty = threadIdx.y;  // 32 x 8
-    if (ty == 0) {
-        MsdGeom g;
-        const bool ok = msd_geom(t0 + tx, *d_total, ntiles, seg_start, seg_tile, nseg, nb, g);
-        row_base[tx] = ok ? g.hbase + g.k : ~0ull;
-        row_nt[tx] = ok ? g.nt : 0;
-    }
-    __syncthreads();
-    if (to_scan) {
-        // read rows (contiguous in digits), write the scan layout (contiguous in tiles)
-        for (uint32_t i = ty; i < MSD_TR; i += 8) {
-            const uint32_t t = t0 + i, d = d0 + tx;
-            blk[i][tx] = row_base[i] != ~0ull && d < nb ? R[(uint64_t)t * nb + d] : 0u;
+            for (uint32_t q = 0; q < MSD_BATCH; q++) msd_count_one(cnt, key[q] != 0xffffffffu, key[q]);
         }
         __syncthreads();
-        for (uint32_t j = ty; j < MSD_TR; j += 8) {
-            const uint32_t d = d0 + j;
-            if (row_base[tx] != ~0ull && d < nb) S[row_base[tx] + (uint64_t)d * row_nt[tx]] = blk[tx][j];
-        }
-    } else {
-        for (uint32_t j = ty; j < MSD_TR; j += 8) {
-            const uint32_t d = d0 + j;
-            blk[tx][j] = row_base[tx] != ~0ull && d < nb ? S[row_base[tx] + (uint64_t)d * row_nt[tx]] : 0u;
+        // the tile's row; the counters are cleared for the next tile
+        uint32_t* crow = C + (uint64_t)row * nb;
+#pragma unroll
+        for (uint32_t q = 0; q < MSD_PER; q++) {
+            const uint32_t d = threadIdx.x * MSD_PER + q;
+            if (d < nb) {
+                const uint32_t v = cnt[d];
+                crow[d] = v;
+                tot[q] += v;
+                cnt[d] = 0;
+            }
         }
         __syncthreads();
-        for (uint32_t i = ty; i < MSD_TR; i += 8) {
-            const uint32_t t = t0 + i, d = d0 + tx;
-            if (row_base[i] != ~0ull && d < nb) R[(uint64_t)t * nb + d] = blk[i][tx];
-        }
+    }
+#pragma unroll
+    for (uint32_t q = 0; q < MSD_PER; q++) {
+        const uint32_t d = threadIdx.x * MSD_PER + q;
+        if (d < nb) S[g.sidx + (uint64_t)d * g.sstride] = tot[q];
     }
 }
 
 // Between the passes (one block): seg_start[s] = first output slot of pass-1
-// digit s (the scanned count of (s, tile 0)), seg_start[nseg] = E; seg_tile =
-// exclusive prefix of ceil(segment length / MSD_TILE), nseg + 1 entries.
+// digit s (the scanned slot of (digit s, group 0, part 0), at s * stride1),
+// seg_start[nseg] = E; seg_tile and seg_chunk = exclusive prefixes of the
+// segments' tiles (ceil(length / MSD_TILE)) and chunks (ceil(tiles /
+// MSD_CHUNK_TILES)), nseg + 1 entries each.
 static __global__ void __launch_bounds__(MSD_THREADS) k_msd_tiles(const uint32_t* __restrict__ S1,
-                                                                 uint32_t ntiles1, uint32_t nseg,
+                                                                 uint32_t stride1, uint32_t nseg,
                                                                  const uint32_t* __restrict__ d_total,
                                                                  uint32_t* __restrict__ seg_start,
-                                                                 uint32_t* __restrict__ seg_tile) {
+                                                                 uint32_t* __restrict__ seg_tile,
+                                                                 uint32_t* __restrict__ seg_chunk) {
     __shared__ uint32_t sh[MSD_THREADS / 32];
     const uint32_t E = *d_total;
-    uint32_t st[MSD_PER + 1], nt[MSD_PER], sum = 0;
+    uint32_t st[MSD_PER + 1], nt[MSD_PER], nc[MSD_PER], sum = 0, csum = 0;
 #pragma unroll
     for (uint32_t q = 0; q <= MSD_PER; q++) {
         const uint32_t s = threadIdx.x * MSD_PER + q;
-        st[q] = s < nseg ? S1[(uint64_t)s * ntiles1] : E;
+        st[q] = s < nseg ? S1[(uint64_t)s * stride1] : E;
     }
 #pragma unroll
     for (uint32_t q = 0; q < MSD_PER; q++) {
         const uint32_t s = threadIdx.x * MSD_PER + q;
         const uint32_t len = s < nseg ? st[q + 1] - st[q] : 0;
         nt[q] = (len + MSD_TILE - 1) / MSD_TILE;
+        nc[q] = (nt[q] + MSD_CHUNK_TILES - 1) / MSD_CHUNK_TILES;
         sum += nt[q];
+        csum += nc[q];
     }
-    uint32_t total;
+    uint32_t total, ctotal;
     uint32_t pre = block_excl_scan_w<MSD_THREADS / 32>(sum, sh, total);
+    uint32_t cpre = block_excl_scan_w<MSD_THREADS / 32>(csum, sh, ctotal);
 #pragma unroll
     for (uint32_t q = 0; q < MSD_PER; q++) {
         const uint32_t s = threadIdx.x * MSD_PER + q;
         if (s < nseg) {
             seg_start[s] = st[q];
             seg_tile[s] = pre;
+            seg_chunk[s] = cpre;
         }
         pre += nt[q];
+        cpre += nc[q];
     }
     if (threadIdx.x == 0) {
         seg_start[nseg] = E;
         seg_tile[nseg] = total;
+        seg_chunk[nseg] = ctotal;
     }
 }
 
-// Dynamic shared memory of k_msd_scatter: the staged tile and two words per
-// digit.
-constexpr size_t MSD_SCATTER_SMEM = (size_t)MSD_TILE * sizeof(uint2) + 2 * (1u << MSD_MAX_BITS) * sizeof(uint32_t);
+// The slot rows: P[tile][digit] = the first output slot of the tile's run of
+// each digit, from the group's scanned slot (part 0's) plus the counts of
+// the group's earlier tiles.  One block per group (pass 1) or chunk (pass 2).
+static __global__ void __launch_bounds__(MSD_THREADS) k_msd_prefix(const uint32_t* __restrict__ d_total,
+                                                                  uint32_t bits, uint32_t ng, uint32_t sub,
+                                                                  const uint32_t* __restrict__ seg_start,
+                                                                  const uint32_t* __restrict__ seg_tile,
+                                                                  const uint32_t* __restrict__ seg_chunk,
+                                                                  uint32_t nseg, const uint32_t* __restrict__ C,
+                                                                  const uint32_t* __restrict__ S,
+                                                                  uint32_t* __restrict__ P) {
+    const uint32_t nb = 1u << bits;
+    MsdGroup g;
+    if (!msd_group(blockIdx.x, *d_total, ng, sub, true, seg_start, seg_tile, seg_chunk, nseg, nb, g)) return;
+    const uint32_t ntl = (g.hi - g.lo + MSD_TILE - 1) / MSD_TILE;
+#pragma unroll
+    for (uint32_t q = 0; q < MSD_PER; q++) {
+        const uint32_t d = threadIdx.x * MSD_PER + q;
+        if (d >= nb) continue;
+        uint32_t run = S[g.sidx + (uint64_t)d * g.sstride];
+        // the count loads of a few rows go out together
+        uint32_t j = 0;
+#pragma unroll 1
+        for (; j + 4 <= ntl; j += 4) {
+            uint32_t c[4];
+#pragma unroll
+            for (uint32_t k = 0; k < 4; k++) c[k] = C[(uint64_t)(g.row0 + j + k) * nb + d];
+#pragma unroll
+            for (uint32_t k = 0; k < 4; k++) {
+                P[(uint64_t)(g.row0 + j + k) * nb + d] = run;
+                run += c[k];
+            }
+        }
+#pragma unroll 1
+        for (; j < ntl; j++) {
+            const uint32_t c = C[(uint64_t)(g.row0 + j) * nb + d];
+            P[(uint64_t)(g.row0 + j) * nb + d] = run;
+            run += c;
+        }
+    }
+}
 
+// Tile t of a pass: pass 1 (seg_tile == nullptr): [t*MSD_TILE, ...) of
+// [0, E), past E empty; pass 2: tile t of the tile table seg_tile inside its
+// segment (false past the last tile).  Its count and slot rows are row t.
+ZK_DEV bool msd_tile(uint32_t t, uint32_t E, const uint32_t* __restrict__ seg_start,
+                     const uint32_t* __restrict__ seg_tile, uint32_t nseg, uint32_t& lo, uint32_t& hi) {
+    if (!seg_tile) {
+        const uint64_t l = (uint64_t)t * MSD_TILE;
+        lo = (uint32_t)(l < E ? l : E);
+        hi = (uint32_t)(l + MSD_TILE < E ? l + MSD_TILE : E);
+        return true;
+    }
+    if (t >= seg_tile[nseg]) return false;
+    uint32_t a = 0, b = nseg - 1;
+    while (a < b) {
+        const uint32_t mid = (a + b + 1) >> 1;
+        if (seg_tile[mid] <= t) a = mid;
+        else b = mid - 1;
+    }
+    lo = seg_start[a] + (t - seg_tile[a]) * MSD_TILE;
+    const uint32_t end = seg_start[a + 1];
+    hi = end - lo > MSD_TILE ? lo + MSD_TILE : end;
+    return true;
+}
+
+// Dynamic shared memory of k_msd_scatter: the staged tile and one word per
+// digit (claim cursors, then each run's output slot less its local offset).
+constexpr size_t MSD_SCATTER_SMEM = (size_t)MSD_TILE * sizeof(uint2) + (1u << MSD_MAX_BITS) * sizeof(uint32_t);
+
+// One block per tile: the tiles placed at once are neighbours, so their runs
+// of one digit land side by side in the output.
 static __global__ void __launch_bounds__(MSD_THREADS) k_msd_scatter(const uint2* __restrict__ A,
                                                                    const uint32_t* __restrict__ d_total,
                                                                    uint32_t shift, uint32_t bits, uint32_t ntiles,
@@ -1591,22 +1671,26 @@ static __global__ void __launch_bounds__(MSD_THREADS) k_msd_scatter(const uint2*
     extern __shared__ uint4 msd_smem[];
     uint2* stage = reinterpret_cast<uint2*>(msd_smem);
     uint32_t* cur = reinterpret_cast<uint32_t*>(stage + MSD_TILE);
-    uint32_t* off = cur + (1u << MSD_MAX_BITS);
     __shared__ uint32_t sh[MSD_THREADS / 32];
     const uint32_t nb = 1u << bits, mask = nb - 1;
-    MsdGeom g;
-    if (!msd_geom(blockIdx.x, *d_total, ntiles, seg_start, seg_tile, nseg, nb, g)) return;
-    const uint32_t len = g.hi - g.lo;
-    if (len == 0) return;
-    const uint32_t* crow = C + (uint64_t)blockIdx.x * nb;
-    const uint32_t* prow = P + (uint64_t)blockIdx.x * nb;
-    // local offsets of the digits: exclusive scan of the tile's counts
+    const uint32_t lane = threadIdx.x & 31;
+    const uint32_t t = blockIdx.x;
+    if (!seg_tile && t >= ntiles) return;
+    uint32_t lo, hi;
+    if (!msd_tile(t, *d_total, seg_start, seg_tile, nseg, lo, hi) || lo == hi) return;
+    const uint32_t len = hi - lo;
+    const uint32_t* crow = C + (uint64_t)t * nb;
+    const uint32_t* prow = P + (uint64_t)t * nb;
+    // local offsets of the digits: exclusive scan of the tile's counts; the
+    // claim cursors start there
+    uint32_t loff[MSD_PER], slot0[MSD_PER], sum = 0;
     {
-        uint32_t c[MSD_PER], sum = 0;
+        uint32_t c[MSD_PER];
 #pragma unroll
         for (uint32_t q = 0; q < MSD_PER; q++) {
             const uint32_t d = threadIdx.x * MSD_PER + q;
             c[q] = d < nb ? crow[d] : 0;
+            slot0[q] = d < nb ? prow[d] : 0;
             sum += c[q];
         }
         uint32_t total;
@@ -1614,27 +1698,25 @@ static __global__ void __launch_bounds__(MSD_THREADS) k_msd_scatter(const uint2*
 #pragma unroll
         for (uint32_t q = 0; q < MSD_PER; q++) {
             const uint32_t d = threadIdx.x * MSD_PER + q;
-            if (d < nb) {
-                off[d] = pre;
-                cur[d] = 0;
-            }
+            loff[q] = pre;
+            if (d < nb) cur[d] = pre;
             pre += c[q];
         }
     }
     __syncthreads();
     // place the tile in digit order
 #pragma unroll 1
-    for (uint32_t r0 = 0; r0 < MSD_ROUNDS; r0 += MSD_BATCH) {
+    for (uint32_t r0 = 0; r0 * MSD_THREADS < len; r0 += MSD_BATCH) {
         uint2 e[MSD_BATCH];
 #pragma unroll
         for (uint32_t q = 0; q < MSD_BATCH; q++) {
             const uint32_t j = (r0 + q) * MSD_THREADS + threadIdx.x;
-            e[q] = j < len ? A[(uint64_t)g.lo + j] : make_uint2(0, 0);
+            e[q] = j < len ? A[(uint64_t)lo + j] : make_uint2(0, 0);
         }
         // the batch's claims in three sweeps, so that its eight shared-memory
         // atomics are in flight together rather than one after another:
-        // digits and the all-lanes-one-key test, the atomics, the slots
-        const uint32_t lane = threadIdx.x & 31;
+        // digits and the all-lanes-one-key test, the atomics (a cursor
+        // returns the stage slot itself), the slots
         uint32_t d[MSD_BATCH], m[MSD_BATCH], lk[MSD_BATCH], b[MSD_BATCH];
         bool one[MSD_BATCH];
 #pragma unroll
@@ -1666,16 +1748,20 @@ static __global__ void __launch_bounds__(MSD_THREADS) k_msd_scatter(const uint2*
                 const uint32_t leader = m[q] ? __ffs(m[q]) - 1 : 0;
                 slot = __shfl_sync(0xffffffffu, b[q], leader) + __popc(m[q] & ((1u << lane) - 1));
             }
-            if (v) stage[off[d[q]] + slot] = e[q];
+            if (v) stage[slot] = e[q];
         }
     }
     __syncthreads();
-    // global slot of each digit's run, less its local offset
-    for (uint32_t d = threadIdx.x; d < nb; d += MSD_THREADS) off[d] = prow[d] - off[d];
+    // each run's output slot less its local offset
+#pragma unroll
+    for (uint32_t q = 0; q < MSD_PER; q++) {
+        const uint32_t d = threadIdx.x * MSD_PER + q;
+        if (d < nb) cur[d] = slot0[q] - loff[q];
+    }
     __syncthreads();
     for (uint32_t i = threadIdx.x; i < len; i += MSD_THREADS) {
         const uint2 v = stage[i];
-        B[(uint64_t)off[(v.x >> shift) & mask] + i] = v;
+        B[(uint64_t)cur[(v.x >> shift) & mask] + i] = v;
     }
 }
 

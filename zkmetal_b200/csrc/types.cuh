@@ -77,6 +77,11 @@ constexpr uint32_t MSD_TILE = 24576;
 constexpr uint32_t MSD_THREADS = 1024;
 constexpr uint32_t MSD_MAX_BITS = 12;
 constexpr uint64_t MSD_MIN_ENTRIES = 1ull << 21;
+// Tiles per scatter group: pass 1 splits its tiles over one group per SM,
+// each counted in MSD_COUNT_PARTS parts (two count blocks fit an SM); pass 2
+// cuts each segment into chunks of at most MSD_CHUNK_TILES tiles.
+constexpr uint32_t MSD_COUNT_PARTS = 2;
+constexpr uint32_t MSD_CHUNK_TILES = 8;
 
 // Scalar profile for the window-layout choice (k_scalar_profile): bins of
 // the bit length (0..288) of a prepared scalar half, and sampled scalars.
