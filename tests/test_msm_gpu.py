@@ -122,6 +122,44 @@ def test_edge_cases(eng, curve):
         check(L.zkmsm_engine_set_tuning(eng[curve].handle, 0, 0, -1))
 
 
+def glv_boundary_scalars(C):
+    """Scalars where the GLV split is most fragile: within one of a Babai
+    rounding boundary s*G_j / 2^256 = k + 1/2 (c_j flips there), around
+    lambda and its multiples, the extremes of [0, r) and the half-width
+    powers of two."""
+    g = C.glv
+    out = set()
+    for gj in (g["g1"], g["g2"]):
+        top = (C.r * gj) >> 256
+        for k in [0, 1, 2, 3, 1000, top // 3, top // 2, top - 2, top - 1, top]:
+            for d in (-1, 0, 1):
+                s = (((2 * k + 1) << 255) // gj) + d
+                if 0 <= s < C.r:
+                    out.add(s)
+    for s in (0, 1, 2, C.lam - 1, C.lam, C.lam + 1, 2 * C.lam % C.r, C.r - C.lam, C.r - 1, C.r - 2,
+              (C.r - 1) // 2, (C.r + 1) // 2, (1 << 127) - 1, 1 << 127, (1 << 128) - 1, 1 << 128):
+        out.add(s % C.r)
+    return sorted(out)
+
+
+@pytest.mark.parametrize("curve", CURVES3)
+def test_glv_rounding_boundaries(eng, curve):
+    """Every boundary scalar of the GLV split, as integer and as Montgomery
+    input, against the naive sum (one MSM of all of them, and each alone so
+    that one wrong split cannot hide behind another)."""
+    C = R.CURVES[curve]
+    e = eng[curve]
+    sc = glv_boundary_scalars(C)
+    pts = R.make_bases(C, 77, len(sc))
+    want = C.enc_affine(R.naive_msm(C, pts, sc))
+    assert aff(C, e.msm(R.pack_points(C, pts), R.pack_scalars_int(sc))) == want
+    assert aff(C, e.msmFr(R.pack_points(C, pts), R.pack_scalars_mont(C, sc))) == want
+    G = (C.gx, C.gy)
+    for s in sc:
+        one = C.enc_affine(R.naive_msm(C, [G], [s]))
+        assert aff(C, e.msmFr(R.pack_points(C, [G]), R.pack_scalars_mont(C, [s]))) == one, hex(s)
+
+
 def test_invalid_inputs(eng):
     e = eng["bn254"]
     with pytest.raises(MSMError) as ei:

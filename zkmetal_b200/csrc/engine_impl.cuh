@@ -60,10 +60,14 @@ void Engine::msd_sort(const Plan& pl, uint2* A, uint2* B, uint32_t* tot) {
     // pass 1: G groups of MSD_COUNT_PARTS count parts over the tile bound;
     // pass 2: the chunk and tile bounds (blocks past the real chunks and
     // tiles return at once)
+    // pass 1 counts the digit array the digit kernel wrote (w_dig), pass 2
+    // the entries' keys
     auto pass = [&](const uint2* src, uint2* dst, uint32_t shift, uint32_t bits, uint32_t ng, uint32_t sub,
-                    uint32_t ntiles, const uint32_t* ss, const uint32_t* st, const uint32_t* sc, uint32_t ns) {
+                    uint32_t ntiles, const uint32_t* ss, const uint32_t* st, const uint32_t* sc, uint32_t ns,
+                    const uint16_t* D) {
         const uint32_t nb = 1u << bits;
-        k_msd_count<<<ng * sub, MSD_THREADS, 0, stream>>>(src, tot + 0, shift, bits, ng, sub, ss, st, sc, ns, Cr, S);
+        k_msd_count<<<ng * sub, MSD_THREADS, 0, stream>>>(D, src, shift, tot + 0, bits, ng, sub, ss, st, sc, ns, Cr,
+                                                          S);
         launches++;
         ZK_CUDA(cudaGetLastError());
         // pass-2 totals fill a prefix of S (chunks in segment order); the
@@ -76,12 +80,14 @@ void Engine::msd_sort(const Plan& pl, uint2* A, uint2* B, uint32_t* tot) {
         launches += 2;
         ZK_CUDA(cudaGetLastError());
     };
-    pass(A, B, pl.msd_passes == 2 ? b2 : 0, b1, G, MSD_COUNT_PARTS, pl.msd_tiles1, nullptr, nullptr, nullptr, 0);
-    if (pl.msd_passes < 2) return;
+    const bool two = pl.msd_passes == 2;
+    pass(A, B, two ? b2 : 0, b1, G, MSD_COUNT_PARTS, pl.msd_tiles1, nullptr, nullptr, nullptr, 0,
+         w_dig.as<uint16_t>());
+    if (!two) return;
     k_msd_tiles<<<1, MSD_THREADS, 0, stream>>>(S, G * MSD_COUNT_PARTS, nseg, tot + 0, seg_start, seg_tile, seg_chunk);
     launches++;
     ZK_CUDA(cudaGetLastError());
-    pass(B, A, 0, b2, CH, 1, pl.msd_tiles2, seg_start, seg_tile, seg_chunk, nseg);
+    pass(B, A, 0, b2, CH, 1, pl.msd_tiles2, seg_start, seg_tile, seg_chunk, nseg, nullptr);
 }
 
 // ------------------------------------------------------------ pipeline
@@ -110,9 +116,21 @@ void Engine::enqueue(const Plan& pl, const uint32_t* d_bases, const uint32_t* d_
     if (hist0) ZK_CUDA(cudaMemsetAsync(w_thist.p, 0, (size_t)(1u << pl.sort_bits) * pl.sort_tiles * 4, stream));
     if (pl.total_scalars) {
         const uint64_t g = (pl.total_scalars + pl.sort_spb - 1) / pl.sort_spb;
-        k_radix_digits<C><<<(unsigned)g, SORT_DTHREADS, 0, stream>>>(
-                d_scalars, dd, nd, pl.total_scalars, pl.sort_spb, bufA, tot + 0,
-                hist0 ? w_thist.as<uint32_t>() : nullptr, pl.sort_bits, pl.sort_tiles);
+        // five-limb halves when every MSM splits with GLV
+        bool all_glv = true;
+        for (const auto& d : pl.descs) all_glv = all_glv && d.glv;
+        // MSD sorts: the first pass's digit of each entry beside it
+        uint16_t* D = pl.msd_passes ? w_dig.as<uint16_t>() : nullptr;
+        const uint32_t dshift = pl.msd_passes == 2 ? pl.msd_bits2 : 0u;
+        const uint32_t dmask = pl.msd_passes ? (1u << pl.msd_bits1) - 1 : 0u;
+        if (all_glv)
+            k_radix_digits<C, 5><<<(unsigned)g, SORT_DTHREADS, 0, stream>>>(
+                    d_scalars, dd, nd, pl.total_scalars, pl.sort_spb, bufA, tot + 0,
+                    hist0 ? w_thist.as<uint32_t>() : nullptr, pl.sort_bits, pl.sort_tiles, D, dshift, dmask);
+        else
+            k_radix_digits<C, 9><<<(unsigned)g, SORT_DTHREADS, 0, stream>>>(
+                    d_scalars, dd, nd, pl.total_scalars, pl.sort_spb, bufA, tot + 0,
+                    hist0 ? w_thist.as<uint32_t>() : nullptr, pl.sort_bits, pl.sort_tiles, D, dshift, dmask);
         launches++;
         ZK_CUDA(cudaGetLastError());
     }

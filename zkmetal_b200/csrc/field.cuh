@@ -311,13 +311,39 @@ ZK_DEV void fe_to_mont(Fe<P>& r, const Fe<P>& a) {
     fe_mul(r, a, r2);
 }
 
-// Montgomery form -> integer
+// Montgomery form -> integer: a * R^-1 mod p by N reduction rounds alone
+// (the product with 1 that a Montgomery multiplication would form is
+// skipped).  Each round adds m*p with m = t0 * (-p^-1 mod 2^32), clearing the
+// low limb, and drops it.  For any a < 2^(32N) and p < 2^(32N-1) the sum
+// stays inside N+1 limbs and the result is below 2p, so one conditional
+// subtraction leaves it below p.
 template <class P>
 ZK_DEV void fe_from_mont(Fe<P>& r, const Fe<P>& a) {
-    Fe<P> one;
-    fe_set_zero(one);
-    one.v[0] = 1;
-    fe_mul(r, a, one);
+    constexpr int N = P::N;
+    uint32_t t[N + 1];
+#pragma unroll
+    for (int i = 0; i < N; i++) t[i] = a.v[i];
+    t[N] = 0;
+#pragma unroll
+    for (int i = 0; i < N; i++) {
+        const uint32_t m = t[0] * P::N0R();
+        asm volatile("mad.lo.cc.u32 %0, %1, %2, %0;" : "+r"(t[0]) : "r"(m), "r"(P::P(0)));
+#pragma unroll
+        for (int j = 1; j < N; j++) asm volatile("madc.lo.cc.u32 %0, %1, %2, %0;" : "+r"(t[j]) : "r"(m), "r"(P::P(j)));
+        asm volatile("addc.u32 %0, %0, 0;" : "+r"(t[N]));
+        asm volatile("mad.hi.cc.u32 %0, %1, %2, %0;" : "+r"(t[1]) : "r"(m), "r"(P::P(0)));
+#pragma unroll
+        for (int j = 1; j < N - 1; j++)
+            asm volatile("madc.hi.cc.u32 %0, %1, %2, %0;" : "+r"(t[j + 1]) : "r"(m), "r"(P::P(j)));
+        asm volatile("madc.hi.u32 %0, %1, %2, %0;" : "+r"(t[N]) : "r"(m), "r"(P::P(N - 1)));
+#pragma unroll
+        for (int j = 0; j < N; j++) t[j] = t[j + 1];
+        t[N] = 0;
+    }
+    Fe<P> x;
+#pragma unroll
+    for (int i = 0; i < N; i++) x.v[i] = t[i];
+    fe_reduce_once(r, x);
 }
 
 // ------------------------------------------------------------ inversion

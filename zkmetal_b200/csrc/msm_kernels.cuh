@@ -43,19 +43,108 @@ struct Halves {
 
 // ------------------------------------------------------------ scalar prep
 
-template <class C>
-ZK_DEV void prepare_scalar(Halves& h, const uint32_t* __restrict__ s8, uint32_t fmt, uint32_t glv) {
+// Constants of a curve's GLV split by name (W: 0 = G1, 1 = G2, 2 = A1,
+// 3 = A2, 4 = B1, 5 = B2), their nonzero limbs and bit length.
+template <class G, int W>
+struct GlvK {
+    __host__ __device__ static constexpr uint32_t limb(int i) {
+        return W == 0 ? G::G1(i) : W == 1 ? G::G2(i) : W == 2 ? G::A1(i) : W == 3 ? G::A2(i) : W == 4 ? G::B1(i)
+                                                                                                      : G::B2(i);
+    }
+    __host__ __device__ static constexpr int limbs() {
+        return limb(4) ? 5 : limb(3) ? 4 : limb(2) ? 3 : limb(1) ? 2 : limb(0) ? 1 : 0;
+    }
+    __host__ __device__ static constexpr int bits() {
+        int b = 0;
+        for (uint32_t t = limbs() ? limb(limbs() - 1) : 0u; t; t >>= 1) b++;
+        return limbs() ? 32 * (limbs() - 1) + b : 0;
+    }
+};
+
+// Babai rounding c = (s * G + 2^255) >> 256 for an 8-limb s below 2^BITS and
+// a constant G of K::limbs() nonzero limbs; c has `LC` limbs.  One row per
+// limb of G: the 8 low halves (carry into the row's top limb, still zero),
+// then the 8 high halves.
+template <class K, int LC>
+ZK_DEV void babai_round(uint32_t (&c)[5], const uint32_t (&s)[8]) {
+    constexpr int NG = K::limbs();
+    uint32_t p[8 + NG];
+#pragma unroll
+    for (int i = 0; i < 8 + NG; i++) p[i] = 0;
+#pragma unroll
+    for (int l = 0; l < NG; l++) {
+        const uint32_t g = K::limb(l);
+        asm volatile("mad.lo.cc.u32 %0, %1, %2, %0;" : "+r"(p[l]) : "r"(s[0]), "r"(g));
+#pragma unroll
+        for (int i = 1; i < 8; i++) asm volatile("madc.lo.cc.u32 %0, %1, %2, %0;" : "+r"(p[l + i]) : "r"(s[i]), "r"(g));
+        asm volatile("addc.u32 %0, %0, 0;" : "+r"(p[l + 8]));
+        asm volatile("mad.hi.cc.u32 %0, %1, %2, %0;" : "+r"(p[l + 1]) : "r"(s[0]), "r"(g));
+#pragma unroll
+        for (int i = 1; i < 7; i++) asm volatile("madc.hi.cc.u32 %0, %1, %2, %0;" : "+r"(p[l + 1 + i]) : "r"(s[i]), "r"(g));
+        asm volatile("madc.hi.u32 %0, %1, %2, %0;" : "+r"(p[l + 8]) : "r"(s[7]), "r"(g));
+    }
+    asm volatile("add.cc.u32 %0, %0, %1;" : "+r"(p[7]) : "r"(0x80000000u));
+#pragma unroll
+    for (int i = 8; i < 8 + NG - 1; i++) asm volatile("addc.cc.u32 %0, %0, 0;" : "+r"(p[i]));
+    asm volatile("addc.u32 %0, %0, 0;" : "+r"(p[8 + NG - 1]));
+#pragma unroll
+    for (int i = 0; i < 5; i++) c[i] = i < NG && i < LC ? p[8 + i] : 0u;
+}
+
+// acc -= c * K (SUB) or acc += c * K, mod 2^160; c has LC limbs, the
+// lattice constant K its nonzero limbs.
+template <class K, int LC, bool SUB>
+ZK_DEV void lattice_mac(uint32_t (&acc)[5], const uint32_t (&c)[5]) {
+    constexpr int LK = K::limbs();
+    uint32_t p[5] = {0, 0, 0, 0, 0};
+#pragma unroll
+    for (int i = 0; i < LC && i < 5; i++) {
+        uint32_t carry = 0;
+#pragma unroll
+        for (int l = 0; l < LK && i + l < 5; l++) {
+            const uint64_t t = (uint64_t)c[i] * K::limb(l) + p[i + l] + carry;
+            p[i + l] = (uint32_t)t;
+            carry = (uint32_t)(t >> 32);
+        }
+        if (i + LK < 5) p[i + LK] = carry;
+    }
+    if (SUB) {
+        asm volatile("sub.cc.u32 %0, %0, %1;" : "+r"(acc[0]) : "r"(p[0]));
+#pragma unroll
+        for (int i = 1; i < 4; i++) asm volatile("subc.cc.u32 %0, %0, %1;" : "+r"(acc[i]) : "r"(p[i]));
+        asm volatile("subc.u32 %0, %0, %1;" : "+r"(acc[4]) : "r"(p[4]));
+    } else {
+        asm volatile("add.cc.u32 %0, %0, %1;" : "+r"(acc[0]) : "r"(p[0]));
+#pragma unroll
+        for (int i = 1; i < 4; i++) asm volatile("addc.cc.u32 %0, %0, %1;" : "+r"(acc[i]) : "r"(p[i]));
+        asm volatile("addc.u32 %0, %0, %1;" : "+r"(acc[4]) : "r"(p[4]));
+    }
+}
+
+// Scalar preparation into registers: the integer scalar (Montgomery
+// reduction for Fr input, bn254_msm.c:1537-1552; subtractions of r for
+// integer input, MSMEngine.swift:182-200), then for GLV the split
+// k = k1 + k2*lambda with k1 = s - c1*a1 - c2*a2, k2 = -c1*b1 - c2*b2 and the
+// Babai roundings c_j = round(s*G_j / 2^256) (GLV.swift:8-33,
+// glv_kernels.metal:172-256).  x[j] holds |k_j| (NL limbs; 5 suffice for
+// GLV halves, 9 for a whole 256-bit scalar plus the guard limb of the top
+// window's carry), neg[j] its sign; count = 2 with GLV, else 1 (x[0] the
+// scalar).  All indexing is static, so everything stays in registers.
+template <class C, int NL>
+ZK_DEV void prep_scalar(uint32_t (&x)[2][NL], uint32_t (&neg)[2], int& count, const uint32_t* __restrict__ s8,
+                        uint32_t fmt, uint32_t glv) {
     using Fr = typename C::Fr;
     using G = typename C::Glv;
+    static_assert(NL >= 5, "a GLV half needs five limbs");
     Fe<Fr> s;
     const uint4* p4 = reinterpret_cast<const uint4*>(s8);
-    uint4 a = __ldg(p4), b = __ldg(p4 + 1);
+    const uint4 a = __ldg(p4), b = __ldg(p4 + 1);
     s.v[0] = a.x; s.v[1] = a.y; s.v[2] = a.z; s.v[3] = a.w;
     s.v[4] = b.x; s.v[5] = b.y; s.v[6] = b.z; s.v[7] = b.w;
     if (fmt == 1) {
-        fe_from_mont(s, s);  // s * R^-1 mod r  (bn254_msm.c:1537-1552)
+        fe_from_mont(s, s);
     } else {
-        // integer form may exceed r: subtract r until below (MSMEngine.swift:182-200);
+        // integer form may exceed r: subtract r until below;
         // REDUCE_PASSES = floor((2^256 - 1) / r) passes always suffice (5 for
         // BN254, 2 for BLS12-381, 13 for BLS12-377)
         Fe<Fr> r;
@@ -64,95 +153,61 @@ ZK_DEV void prepare_scalar(Halves& h, const uint32_t* __restrict__ s8, uint32_t 
 #pragma unroll 1
         for (int it = 0; it < Fr::REDUCE_PASSES && fe_geq_int(s, r); it++) fe_sub_int(s, s, r);
     }
-    if (!glv) {
-#pragma unroll
-        for (int i = 0; i < 8; i++) h.k[0][i] = s.v[i];
-        h.k[0][8] = 0;
-        h.neg[0] = 0;
-        h.count = 1;
-        return;
-    }
-    // c_j = (s * G_j + 2^255) >> 256, 5 limbs each
-    uint32_t c[2][5];
 #pragma unroll
     for (int j = 0; j < 2; j++) {
-        uint32_t prod[13];
+        neg[j] = 0;
 #pragma unroll
-        for (int i = 0; i < 13; i++) prod[i] = 0;
-#pragma unroll
-        for (int i = 0; i < 8; i++) {
-            uint64_t carry = 0;
-#pragma unroll
-            for (int l = 0; l < 5; l++) {
-                uint32_t g = j == 0 ? G::G1(l) : G::G2(l);
-                uint64_t t = (uint64_t)s.v[i] * g + prod[i + l] + carry;
-                prod[i + l] = (uint32_t)t;
-                carry = t >> 32;
-            }
-            prod[i + 5] = (uint32_t)carry;
-        }
-        // + 2^255 (bit 31 of limb 7)
-        uint64_t t = (uint64_t)prod[7] + 0x80000000u;
-        prod[7] = (uint32_t)t;
-        uint32_t cy = (uint32_t)(t >> 32);
-#pragma unroll
-        for (int i = 8; i < 13; i++) {
-            uint64_t u = (uint64_t)prod[i] + cy;
-            prod[i] = (uint32_t)u;
-            cy = (uint32_t)(u >> 32);
-        }
-#pragma unroll
-        for (int i = 0; i < 5; i++) c[j][i] = prod[8 + i];
+        for (int i = 0; i < NL; i++) x[j][i] = 0;
     }
+    if (!glv) {
+        if (NL >= 9) {
+#pragma unroll
+            for (int i = 0; i < 8 && i < NL; i++) x[0][i] = s.v[i];
+        }
+        count = NL >= 9 ? 1 : 0;  // a five-limb kernel is never launched without GLV
+        return;
+    }
+    using KG1 = GlvK<G, 0>;
+    using KG2 = GlvK<G, 1>;
+    // c_j < 2^(BITS + bits(G_j) - 256) + 1/2
+    constexpr int LC1 = (Fr::BITS + KG1::bits() - 256 + 1 + 31) / 32 < 5 ? (Fr::BITS + KG1::bits() - 256 + 1 + 31) / 32 : 5;
+    constexpr int LC2 = (Fr::BITS + KG2::bits() - 256 + 1 + 31) / 32 < 5 ? (Fr::BITS + KG2::bits() - 256 + 1 + 31) / 32 : 5;
+    uint32_t c1[5], c2[5];
+    babai_round<KG1, LC1>(c1, s.v);
+    babai_round<KG2, LC2>(c2, s.v);
     // k1 = s - c1*a1 - c2*a2, k2 = -c1*b1 - c2*b2   (mod 2^160, signed)
-    uint32_t k1[5], k2[5];
-#pragma unroll
-    for (int i = 0; i < 5; i++) { k1[i] = s.v[i]; k2[i] = 0; }
-    auto mac = [](uint32_t* acc, const uint32_t* x, int which, bool subtract) {
-        // acc -/+= x * K  where K is the lattice constant selected by `which`
-        uint32_t prod[5] = {0, 0, 0, 0, 0};
-#pragma unroll
-        for (int i = 0; i < 5; i++) {
-            uint64_t carry = 0;
-#pragma unroll
-            for (int l = 0; l + i < 5; l++) {
-                uint32_t kv = which == 0 ? G::A1(l) : which == 1 ? G::A2(l) : which == 2 ? G::B1(l) : G::B2(l);
-                uint64_t t = (uint64_t)x[i] * kv + prod[i + l] + carry;
-                prod[i + l] = (uint32_t)t;
-                carry = t >> 32;
-            }
-        }
-        uint64_t cy = subtract ? 1 : 0;  // two's complement: acc + ~prod + 1
-#pragma unroll
-        for (int i = 0; i < 5; i++) {
-            uint64_t t = (uint64_t)acc[i] + (subtract ? (uint32_t)~prod[i] : prod[i]) + cy;
-            acc[i] = (uint32_t)t;
-            cy = t >> 32;
-        }
-    };
-    mac(k1, c[0], 0, !G::A1_NEG);
-    mac(k1, c[1], 1, !G::A2_NEG);
-    mac(k2, c[0], 2, !G::B1_NEG);
-    mac(k2, c[1], 3, !G::B2_NEG);
+    uint32_t k1[5] = {s.v[0], s.v[1], s.v[2], s.v[3], s.v[4]};
+    uint32_t k2[5] = {0, 0, 0, 0, 0};
+    lattice_mac<GlvK<G, 2>, LC1, !G::A1_NEG>(k1, c1);
+    lattice_mac<GlvK<G, 3>, LC2, !G::A2_NEG>(k1, c2);
+    lattice_mac<GlvK<G, 4>, LC1, !G::B1_NEG>(k2, c1);
+    lattice_mac<GlvK<G, 5>, LC2, !G::B2_NEG>(k2, c2);
     uint32_t* ks[2] = {k1, k2};
 #pragma unroll
     for (int j = 0; j < 2; j++) {
         uint32_t* k = ks[j];
-        uint32_t neg = k[4] >> 31;
-        if (neg) {  // magnitude = -k
-            uint64_t cy = 1;
+        const uint32_t ng = k[4] >> 31;
+        // magnitude = ng ? -k : k  (two's complement under a mask)
+        const uint32_t m = 0u - ng;
+        asm volatile("add.cc.u32 %0, %1, %2;" : "=r"(x[j][0]) : "r"(k[0] ^ m), "r"(ng));
 #pragma unroll
-            for (int i = 0; i < 5; i++) {
-                uint64_t t = (uint64_t)(~k[i]) + cy;
-                k[i] = (uint32_t)t;
-                cy = t >> 32;
-            }
-        }
-#pragma unroll
-        for (int i = 0; i < 9; i++) h.k[j][i] = i < 5 ? k[i] : 0;
-        h.neg[j] = neg;
+        for (int i = 1; i < 4; i++) asm volatile("addc.cc.u32 %0, %1, 0;" : "=r"(x[j][i]) : "r"(k[i] ^ m));
+        asm volatile("addc.u32 %0, %1, 0;" : "=r"(x[j][4]) : "r"(k[4] ^ m));
+        neg[j] = ng;
     }
-    h.count = 2;
+    count = 2;
+}
+
+template <class C>
+ZK_DEV void prepare_scalar(Halves& h, const uint32_t* __restrict__ s8, uint32_t fmt, uint32_t glv) {
+    uint32_t x[2][9], neg[2];
+    prep_scalar<C, 9>(x, neg, h.count, s8, fmt, glv);
+#pragma unroll
+    for (int j = 0; j < 2; j++) {
+#pragma unroll
+        for (int i = 0; i < 9; i++) h.k[j][i] = x[j][i];
+        h.neg[j] = neg[j];
+    }
 }
 
 // c-bit field of a multi-limb magnitude starting at bit `off` (c <= 31, off + c <= 288)
@@ -385,61 +440,104 @@ ZK_DEV void warp_count(uint32_t* __restrict__ ctr, bool valid, uint32_t key) {
     else if (valid && !grp) atomicAdd(ctr + key, 1u);
 }
 
+// Signed digit of the current window of a prepared half held in registers
+// (NL limbs, shifted right window by window: the low bits are always the
+// current window).  v = field + carry; v > 2^(cw-1) gives digit v - 2^cw
+// (negative: dn = 1, carry 1), otherwise v (carry 0); digits lie in
+// [-2^(cw-1), 2^(cw-1)].  Returns the digit's magnitude.
+
+template <int NL>
+ZK_DEV uint32_t take_window(uint32_t (&x)[NL], uint32_t cw, uint32_t& carry, uint32_t& dn) {
+    const uint32_t v = (x[0] & ((1u << cw) - 1u)) + carry;
+    const bool hi = v > (1u << (cw - 1));
+    dn = hi ? 1u : 0u;
+    carry = dn;
+#pragma unroll
+    for (int i = 0; i < NL - 1; i++) x[i] = __funnelshift_r(x[i], x[i + 1], cw);
+    x[NL - 1] >>= cw;
+    return hi ? (1u << cw) - v : v;
+}
+
 // hist0 (optional, zeroed before the launch): the first radix pass's
 // digit-major per-tile counts of the low h0bits bits of the bucket ids, for
 // tiles of SORT_ETILE entries of A ([digit][tile], ntiles tiles), added here
-// so that the first pass needs no histogram kernel.
+// so that the first LSD pass needs no histogram kernel.  D (optional): the
+// first MSD pass's digit of each entry, (key >> dshift) & dmask, beside A, so
+// that its count kernel reads 2 bytes per entry instead of 8.
+//
+// Each thread prepares one scalar per round into registers; the warp then
+// walks (half, window) in step: each lane takes its digit, a ballot ranks
+// the nonzero ones, one shared-memory claim per warp and window reserves
+// their slots in the block buffer.  The buffer (every digit of the block's
+// scalars_per_block scalars) goes to A in one run claimed by one atomic.
+// NL = 5 when every MSM of the launch splits with GLV, else 9.
 static_assert(SORT_DBUF <= SORT_ETILE, "a digit block's range spans at most two sort tiles");
-template <class C>
+template <class C, int NL>
 __global__ void __launch_bounds__(SORT_DTHREADS) k_radix_digits(const uint32_t* __restrict__ scalars,
                                                                 const MsmDesc* __restrict__ descs, int nd,
                                                                 uint64_t total, uint32_t scalars_per_block,
                                                                 uint2* __restrict__ A,
                                                                 uint32_t* __restrict__ d_count,
                                                                 uint32_t* __restrict__ hist0, uint32_t h0bits,
-                                                                uint32_t ntiles) {
+                                                                uint32_t ntiles, uint16_t* __restrict__ D,
+                                                                uint32_t dshift, uint32_t dmask) {
     __shared__ uint2 buf[SORT_DBUF];
     __shared__ uint32_t cur, base_s;
     const uint32_t tid = threadIdx.x, lane = tid & 31;
+    const uint32_t lt = (1u << lane) - 1u;
     if (tid == 0) cur = 0;
     __syncthreads();
 #pragma unroll 1
     for (uint32_t k = 0; k < scalars_per_block; k += SORT_DTHREADS) {
         const uint64_t gi = (uint64_t)blockIdx.x * scalars_per_block + k + tid;
-        Halves h;
-        h.count = 0;
+        uint32_t x[2][NL], neg[2] = {0, 0};
+        int cnt = 0;
         MsmDesc d{};
         d.c = 2;
         uint32_t idx = 0;
-        DigitGen g{0, 0, 0};
         if (k + tid < scalars_per_block && gi < total) {
             d = descs[find_msm(descs, nd, gi)];
-            prepare_scalar<C>(h, scalars + gi * 8, d.fmt, d.glv);
+            prep_scalar<C, NL>(x, neg, cnt, scalars + gi * 8, d.fmt, d.glv);
             idx = d.base_off + (uint32_t)(gi - d.scalar_off);
-            if (d.nwin == 0) g.j = (uint32_t)h.count;
+            if (d.nwin == 0) cnt = 0;
+        } else {
+#pragma unroll
+            for (int j = 0; j < 2; j++)
+#pragma unroll
+                for (int i = 0; i < NL; i++) x[j][i] = 0;
         }
-        bool valid[DBATCH];
-        uint32_t gb[DBATCH], val[DBATCH];
+        // warp-uniform walk: the most halves and windows of any lane
+        const uint32_t jm = __reduce_max_sync(0xffffffffu, (uint32_t)cnt);
+        const uint32_t wm = __reduce_max_sync(0xffffffffu, cnt ? d.nwin : 0u);
+#pragma unroll
+        for (uint32_t j = 0; j < 2; j++) {
+            if (j >= jm) break;
+            uint32_t carry = 0, wb = 0;
 #pragma unroll 1
-        while (__any_sync(0xffffffffu, g.j < (uint32_t)h.count)) {
-            next_digits(g, h, d, idx, valid, gb, val);
-            uint32_t nv = 0;
-#pragma unroll
-            for (int s = 0; s < DBATCH; s++) nv += valid[s] ? 1u : 0u;
-            uint32_t incl = nv;
-#pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
-                if (lane >= (uint32_t)o) incl += t;
+            for (uint32_t w = 0; w < wm; w++) {
+                const uint32_t cw = d.c + (w >= d.nlo ? 1u : 0u);
+                uint32_t dn;
+                const uint32_t a = take_window<NL>(x[j], cw, carry, dn);
+                const bool ok = j < (uint32_t)cnt && w < d.nwin && a != 0;
+                const uint32_t m = __ballot_sync(0xffffffffu, ok);
+                if (m) {
+                    uint32_t base = 0;
+                    if (lane == __ffs(m) - 1) base = atomicAdd(&cur, (uint32_t)__popc(m));
+                    base = __shfl_sync(0xffffffffu, base, __ffs(m) - 1);
+                    if (ok) {
+                        uint2 e;
+                        if (d.wstep) {  // shift table: window w's base is 2^(c*w)*P, one bucket set
+                            e.x = d.bucket_off + (a - 1);
+                            e.y = (idx + w * d.wstep) | ((neg[j] ^ dn) << 31);
+                        } else {
+                            e.x = d.bucket_off + wb + (a - 1);
+                            e.y = idx | (j << 30) | ((neg[j] ^ dn) << 31);
+                        }
+                        buf[base + __popc(m & lt)] = e;
+                    }
+                }
+                wb += 1u << (cw - 1);
             }
-            uint32_t base = 0;
-            if (lane == 31 && incl) base = atomicAdd(&cur, incl);
-            base = __shfl_sync(0xffffffffu, base, 31) + incl - nv;
-            // valid slots form a prefix of the batch; the buffer holds every
-            // digit of the block's scalars (scalars_per_block * max digits)
-#pragma unroll
-            for (int s = 0; s < DBATCH; s++)
-                if (valid[s]) buf[base + s] = make_uint2(gb[s], val[s]);
         }
     }
     __syncthreads();
@@ -447,7 +545,11 @@ __global__ void __launch_bounds__(SORT_DTHREADS) k_radix_digits(const uint32_t* 
     if (tid == 0) base_s = cnt ? atomicAdd(d_count, cnt) : 0;
     __syncthreads();
     const uint32_t base = base_s;
-    for (uint32_t i = tid; i < cnt; i += SORT_DTHREADS) A[(size_t)base + i] = buf[i];
+    for (uint32_t i = tid; i < cnt; i += SORT_DTHREADS) {
+        const uint2 e = buf[i];
+        A[(size_t)base + i] = e;
+        if (D) D[(size_t)base + i] = (uint16_t)((e.x >> dshift) & dmask);
+    }
     if (hist0) {
         // counts of the range [base, base + cnt) per tile (the tile of base,
         // and the next one from entry `split` on) and digit, then one
@@ -1338,8 +1440,11 @@ static __global__ void __launch_bounds__(SCAN_THREADS) k_scan_add(uint32_t* __re
 // tiles of one segment (pass 1: the tiles split evenly over `ng` groups,
 // about one per SM; pass 2: chunks of at most MSD_CHUNK_TILES tiles of a
 // segment).  Output order inside a segment: digit, then group, then tile.
-//  k_msd_count      each tile's digit counts as a contiguous row C[tile][digit],
-//                   and the group's digit totals straight into the scan
+//  k_msd_count      each tile's digit counts as a contiguous row C[tile][digit]
+//                   (pass 1 from the 2-byte digit array the digit kernel
+//                   writes beside the entries, pass 2 from the entries'
+//                   keys), and the group's digit totals straight into the
+//                   scan
 //                   layout S[seg][digit][group of seg], so that an exclusive
 //                   scan of S gives each (seg, digit, group) the first output
 //                   slot of its run (pass 1 counts each group in `sub` parts,
@@ -1484,9 +1589,10 @@ constexpr uint32_t MSD_BATCH = 8;  // entries loaded before they are used
 static_assert(MSD_ROUNDS % MSD_BATCH == 0, "tile rounds come in whole load batches");
 constexpr uint32_t MSD_PER = (1u << MSD_MAX_BITS) / MSD_THREADS;  // digits per thread in row scans
 
-static __global__ void __launch_bounds__(MSD_THREADS) k_msd_count(const uint2* __restrict__ A,
+static __global__ void __launch_bounds__(MSD_THREADS) k_msd_count(const uint16_t* __restrict__ D,
+                                                                 const uint2* __restrict__ A, uint32_t shift,
                                                                  const uint32_t* __restrict__ d_total,
-                                                                 uint32_t shift, uint32_t bits, uint32_t ng,
+                                                                 uint32_t bits, uint32_t ng,
                                                                  uint32_t sub,
                                                                  const uint32_t* __restrict__ seg_start,
                                                                  const uint32_t* __restrict__ seg_tile,
@@ -1512,7 +1618,9 @@ static __global__ void __launch_bounds__(MSD_THREADS) k_msd_count(const uint2* _
 #pragma unroll
             for (uint32_t q = 0; q < MSD_BATCH; q++) {
                 const uint32_t j = (r0 + q) * MSD_THREADS + threadIdx.x;
-                key[q] = j < len ? (A[(uint64_t)t0 + j].x >> shift) & mask : 0xffffffffu;
+                key[q] = j >= len ? 0xffffffffu
+                         : D      ? (uint32_t)D[(uint64_t)t0 + j]
+                                  : (A[(uint64_t)t0 + j].x >> shift) & mask;
             }
 #pragma unroll
             for (uint32_t q = 0; q < MSD_BATCH; q++) msd_count_one(cnt, key[q] != 0xffffffffu, key[q]);
@@ -1659,7 +1767,9 @@ ZK_DEV bool msd_tile(uint32_t t, uint32_t E, const uint32_t* __restrict__ seg_st
 constexpr size_t MSD_SCATTER_SMEM = (size_t)MSD_TILE * sizeof(uint2) + (1u << MSD_MAX_BITS) * sizeof(uint32_t);
 
 // One block per tile: the tiles placed at once are neighbours, so their runs
-// of one digit land side by side in the output.
+// of one digit land side by side in the output.  (Writing the next pass's
+// digit beside each placed entry, 2 bytes at scattered slots, cost more in
+// partial-sector writes than the pass-2 count saved.)
 static __global__ void __launch_bounds__(MSD_THREADS) k_msd_scatter(const uint2* __restrict__ A,
                                                                    const uint32_t* __restrict__ d_total,
                                                                    uint32_t shift, uint32_t bits, uint32_t ntiles,
