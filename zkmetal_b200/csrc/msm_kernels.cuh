@@ -1707,34 +1707,36 @@ static __global__ void __launch_bounds__(MSD_THREADS) k_msd_prefix(const uint32_
                                                                   uint32_t nseg, const uint32_t* __restrict__ C,
                                                                   const uint32_t* __restrict__ S,
                                                                   uint32_t* __restrict__ P) {
+    constexpr uint32_t ROWS = 4;  // count rows loaded before any is used
     const uint32_t nb = 1u << bits;
     MsdGroup g;
     if (!msd_group(blockIdx.x, *d_total, ng, sub, true, seg_start, seg_tile, seg_chunk, nseg, nb, g)) return;
     const uint32_t ntl = (g.hi - g.lo + MSD_TILE - 1) / MSD_TILE;
+    // digits threadIdx.x + q * MSD_THREADS: each row access is coalesced
+    uint32_t run[MSD_PER];
 #pragma unroll
     for (uint32_t q = 0; q < MSD_PER; q++) {
-        const uint32_t d = threadIdx.x * MSD_PER + q;
-        if (d >= nb) continue;
-        uint32_t run = S[g.sidx + (uint64_t)d * g.sstride];
-        // the count loads of a few rows go out together
-        uint32_t j = 0;
+        const uint32_t d = threadIdx.x + q * MSD_THREADS;
+        run[q] = d < nb ? S[g.sidx + (uint64_t)d * g.sstride] : 0u;
+    }
 #pragma unroll 1
-        for (; j + 4 <= ntl; j += 4) {
-            uint32_t c[4];
+    for (uint32_t j = 0; j < ntl; j += ROWS) {
+        uint32_t c[ROWS][MSD_PER];
 #pragma unroll
-            for (uint32_t k = 0; k < 4; k++) c[k] = C[(uint64_t)(g.row0 + j + k) * nb + d];
+        for (uint32_t k = 0; k < ROWS; k++)
 #pragma unroll
-            for (uint32_t k = 0; k < 4; k++) {
-                P[(uint64_t)(g.row0 + j + k) * nb + d] = run;
-                run += c[k];
+            for (uint32_t q = 0; q < MSD_PER; q++) {
+                const uint32_t d = threadIdx.x + q * MSD_THREADS;
+                c[k][q] = j + k < ntl && d < nb ? C[(uint64_t)(g.row0 + j + k) * nb + d] : 0u;
             }
-        }
-#pragma unroll 1
-        for (; j < ntl; j++) {
-            const uint32_t c = C[(uint64_t)(g.row0 + j) * nb + d];
-            P[(uint64_t)(g.row0 + j) * nb + d] = run;
-            run += c;
-        }
+#pragma unroll
+        for (uint32_t k = 0; k < ROWS; k++)
+#pragma unroll
+            for (uint32_t q = 0; q < MSD_PER; q++) {
+                const uint32_t d = threadIdx.x + q * MSD_THREADS;
+                if (j + k < ntl && d < nb) P[(uint64_t)(g.row0 + j + k) * nb + d] = run[q];
+                run[q] += c[k][q];
+            }
     }
 }
 
