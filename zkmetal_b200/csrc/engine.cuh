@@ -585,7 +585,7 @@ class Engine {
 
     // workspace
     DevBuf w_points, w_phi, w_scalars, w_counts, w_offsets, w_cursor, w_ents, w_buckets;
-    DevBuf w_ents2, w_thist, w_stripe_buckets, w_seg, w_dig;
+    DevBuf w_ents2, w_thist, w_stripe_buckets, w_seg;
     DevBuf w_cnt, w_pos, w_tiles, w_totals, w_pkeys[2], w_pvals[2], w_redS[2], w_redW[2];
     DevBuf w_results, w_comb, w_profile;
     uint32_t* h_profile = nullptr;  // pinned, PROFILE_BINS words
@@ -598,7 +598,7 @@ class Engine {
     // setting, e.g. a server's reservation, is left as it is).
     void bind_workspace_stream() {
         DevBuf* bufs[] = {&w_points, &w_phi, &w_scalars, &w_counts, &w_offsets, &w_cursor, &w_ents, &w_buckets,
-                          &w_ents2, &w_thist, &w_stripe_buckets, &w_seg, &w_dig, &w_cnt, &w_pos, &w_tiles, &w_totals,
+                          &w_ents2, &w_thist, &w_stripe_buckets, &w_seg, &w_cnt, &w_pos, &w_tiles, &w_totals,
                           &w_pkeys[0], &w_pkeys[1], &w_pvals[0], &w_pvals[1], &w_redS[0], &w_redS[1],
                           &w_redW[0], &w_redW[1], &w_results, &w_comb, &w_profile, &transient.d_descs,
                           &transient.d_tasks};
@@ -978,8 +978,6 @@ class Engine {
             // count and slot rows of every tile, then the scan layout of the groups
             hsz = 2 * msd_rows_words(pl) + msd_scan_words(pl);
             grew |= w_seg.ensure(((size_t)3 << pl.msd_bits1) * 4 + 64);
-            // each entry's digit of the first MSD pass (2 bytes)
-            grew |= w_dig.ensure(pl.entry_bound * 2 + 16);
         }
         const uint64_t hwords = hsz;
         grew |= w_ents2.ensure(pl.entry_bound * 8 + 16);

@@ -60,8 +60,9 @@ void Engine::msd_sort(const Plan& pl, uint2* A, uint2* B, uint32_t* tot) {
     // pass 1: G groups of MSD_COUNT_PARTS count parts over the tile bound;
     // pass 2: the chunk and tile bounds (blocks past the real chunks and
     // tiles return at once)
-    // pass 1 counts the digit array the digit kernel wrote (w_dig), pass 2
-    // the entries' keys
+    // pass 1 counts the digit array the digit kernel wrote at the front of
+    // B (the pass-1 scatter overwrites it only after the count), pass 2 the
+    // entries' keys
     auto pass = [&](const uint2* src, uint2* dst, uint32_t shift, uint32_t bits, uint32_t ng, uint32_t sub,
                     uint32_t ntiles, const uint32_t* ss, const uint32_t* st, const uint32_t* sc, uint32_t ns,
                     const uint16_t* D) {
@@ -82,7 +83,7 @@ void Engine::msd_sort(const Plan& pl, uint2* A, uint2* B, uint32_t* tot) {
     };
     const bool two = pl.msd_passes == 2;
     pass(A, B, two ? b2 : 0, b1, G, MSD_COUNT_PARTS, pl.msd_tiles1, nullptr, nullptr, nullptr, 0,
-         w_dig.as<uint16_t>());
+         reinterpret_cast<const uint16_t*>(B));
     if (!two) return;
     k_msd_tiles<<<1, MSD_THREADS, 0, stream>>>(S, G * MSD_COUNT_PARTS, nseg, tot + 0, seg_start, seg_tile, seg_chunk);
     launches++;
@@ -119,8 +120,9 @@ void Engine::enqueue(const Plan& pl, const uint32_t* d_bases, const uint32_t* d_
         // five-limb halves when every MSM splits with GLV
         bool all_glv = true;
         for (const auto& d : pl.descs) all_glv = all_glv && d.glv;
-        // MSD sorts: the first pass's digit of each entry beside it
-        uint16_t* D = pl.msd_passes ? w_dig.as<uint16_t>() : nullptr;
+        // MSD sorts: the first pass's digit of each entry, 2 bytes, at the
+        // front of the other entry buffer (free until the pass-1 scatter)
+        uint16_t* D = pl.msd_passes ? reinterpret_cast<uint16_t*>(bufB) : nullptr;
         const uint32_t dshift = pl.msd_passes == 2 ? pl.msd_bits2 : 0u;
         const uint32_t dmask = pl.msd_passes ? (1u << pl.msd_bits1) - 1 : 0u;
         if (all_glv)

@@ -201,7 +201,7 @@ struct Server {
                     const DevBuf* ws[] = {&eng->w_counts, &eng->w_cursor, &eng->w_ents, &eng->w_ents2,
                                           &eng->w_thist, &eng->w_buckets, &eng->w_cnt, &eng->w_pkeys[0],
                                           &eng->w_pkeys[1], &eng->w_pvals[0], &eng->w_pvals[1], &eng->w_redS[0],
-                                          &eng->w_redS[1], &eng->w_redW[0], &eng->w_redW[1], &eng->w_tiles, &eng->w_dig};
+                                          &eng->w_redS[1], &eng->w_redW[0], &eng->w_redW[1], &eng->w_tiles};
                     uint64_t wsb = d_cap;
                     for (const DevBuf* b : ws) wsb += b->cap;
                     uint64_t pool_res = 0, pool_used = 0;
