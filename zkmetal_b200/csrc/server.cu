@@ -93,6 +93,42 @@ struct Server {
         }
         uint32_t* d_scalars = nullptr;
         size_t d_cap = 0;
+        // Size the workspace now for the batch shapes that set its high-water
+        // marks (full-table requests up to the batch limit; sizes doubling
+        // from 2^10 points to the table size, repeated up to the limit), so
+        // that serving rarely has to grow it: a growth while the other
+        // workers' batches ran has held up every batch on the device, once
+        // for 3.5 s.
+        try {
+            for (int c = 0; c < 2; c++) {
+                if (!has_table[c]) continue;
+                const TableView& tv = tables[c];
+                const uint64_t T = std::min<uint64_t>(tv.n, max_batch_points), M = max_batch_points;
+                std::vector<std::vector<uint32_t>> shapes(2);
+                for (uint64_t s = 0; T && s + T <= M; s += T) shapes[0].push_back((uint32_t)T);
+                for (uint64_t s = 0, added = 1; added && T;) {
+                    added = 0;
+                    for (uint64_t n = std::min<uint64_t>(1024, T); n <= T && s + n <= M; n *= 2, added++) {
+                        shapes[1].push_back((uint32_t)n);
+                        s += n;
+                    }
+                }
+                for (auto& counts : shapes) {
+                    if (counts.empty()) continue;
+                    std::vector<uint32_t> boffs(counts.size(), 0);
+                    if (c == 0)
+                        eng->ensure_workspace<Bn254>(eng->transient_plan<Bn254>(counts, boffs, 1, tv.shifts));
+                    else
+                        eng->ensure_workspace<Bls381>(eng->transient_plan<Bls381>(counts, boffs, 1, tv.shifts));
+                }
+            }
+            const uint64_t want = max_batch_points * 36;
+            if (cudaMallocAsync(reinterpret_cast<void**>(&d_scalars), want, eng->stream) == cudaSuccess) d_cap = want;
+            else d_scalars = nullptr;
+            cudaStreamSynchronize(eng->stream);
+        } catch (...) {
+        }
+        cudaGetLastError();
         // small batches run on a high-priority stream: their blocks get SMs
         // as soon as blocks of other workers' large batches finish, instead
         // of queueing behind whole kernels
