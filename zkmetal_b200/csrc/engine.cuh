@@ -785,10 +785,14 @@ class Engine {
             pl.sort_bits = passes ? (kb + passes - 1) / passes : 0;
             pl.sort_tiles = (uint32_t)std::max<uint64_t>((pl.entry_bound + SORT_ETILE - 1) / SORT_ETILE, 1);
             // large entry sets: MSD passes of up to 12 bits (two cover bucket
-            // ids of up to 24 bits), the first pass over the top bits
+            // ids of up to 24 bits), the first pass over the top bits.  An odd
+            // width gives the first pass the narrower digit: its scatter writes
+            // runs all over the output, where fewer, longer runs pay (BN254
+            // 2^24: 11 + 12 bits, prep+sort 4.25 ms, against 4.35 with 12 + 11),
+            // while the second writes inside one segment
             if (pl.entry_bound >= MSD_MIN_ENTRIES && kb >= 1 && kb <= 2 * MSD_MAX_BITS) {
                 pl.msd_passes = kb <= MSD_MAX_BITS ? 1 : 2;
-                pl.msd_bits1 = pl.msd_passes == 1 ? kb : (kb + 1) / 2;
+                pl.msd_bits1 = pl.msd_passes == 1 ? kb : kb / 2;
                 pl.msd_bits2 = kb - (pl.msd_passes == 1 ? kb : pl.msd_bits1);
                 pl.msd_tiles1 = (uint32_t)((pl.entry_bound + MSD_TILE - 1) / MSD_TILE);
                 pl.msd_tiles2 = pl.msd_passes == 2 ? pl.msd_tiles1 + (1u << pl.msd_bits1) : 0;
