@@ -774,8 +774,13 @@ class Engine {
         {
             uint32_t maxd = 1;
             for (auto& d : pl.descs) maxd = std::max(maxd, (d.glv ? 2u : 1u) * d.nwin);
-            uint32_t spb = SORT_DBUF / maxd;
-            if (spb >= SORT_DTHREADS) spb -= spb % SORT_DTHREADS;
+            // scalars per digit block: each warp owns a buffer slice of
+            // SORT_DBUF / 8 entries; rounds of 256 scalars while a lane's
+            // digits of all rounds fit its share of the slice, else fewer
+            // lanes per warp (k_radix_digits)
+            const uint32_t wslice = SORT_DBUF / (SORT_DTHREADS / 32);
+            const uint32_t spb = maxd * 32 <= wslice ? SORT_DTHREADS * (wslice / (32 * maxd))
+                                                     : (SORT_DTHREADS / 32) * std::max<uint32_t>(1, wslice / maxd);
             uint32_t kb = 0;
             while (kb < 32 && (1ull << kb) < (uint64_t)boff) kb++;
             uint32_t passes = (kb + 7) / 8;

@@ -466,11 +466,17 @@ ZK_DEV uint32_t take_window(uint32_t (&x)[NL], uint32_t cw, uint32_t& carry, uin
 // that its count kernel reads 2 bytes per entry instead of 8.
 //
 // Each thread prepares one scalar per round into registers; the warp then
-// walks (half, window) in step: each lane takes its digit, a ballot ranks
-// the nonzero ones, one shared-memory claim per warp and window reserves
-// their slots in the block buffer.  The buffer (every digit of the block's
-// scalars_per_block scalars) goes to A in one run claimed by one atomic.
-// NL = 5 when every MSM of the launch splits with GLV, else 9.
+// walks (half, window) in step: each lane takes its digit and a ballot ranks
+// the nonzero ones inside the warp's own slice of the block buffer, behind a
+// running count the whole warp holds (no atomics, no shuffles).  A slice
+// takes SORT_DBUF / 8 entries: with maxd digits per scalar at most, a block
+// runs min(32, spb / 8) lanes per warp and rounds of 8 * lanes scalars, so
+// that a slice never overflows (spb from the plan: 256 * floor(16 / maxd)
+// scalars when maxd <= 16, else 8 * floor(512 / maxd)).  The slices go to A
+// in one run claimed by one atomic per block.  NL = 5 when every MSM of the
+// launch splits with GLV, else 9.
+constexpr uint32_t SORT_DWARPS = SORT_DTHREADS / 32;
+constexpr uint32_t SORT_DSLICE = SORT_DBUF / SORT_DWARPS;
 static_assert(SORT_DBUF <= SORT_ETILE, "a digit block's range spans at most two sort tiles");
 template <class C, int NL>
 __global__ void __launch_bounds__(SORT_DTHREADS) k_radix_digits(const uint32_t* __restrict__ scalars,
@@ -482,20 +488,23 @@ __global__ void __launch_bounds__(SORT_DTHREADS) k_radix_digits(const uint32_t* 
                                                                 uint32_t ntiles, uint16_t* __restrict__ D,
                                                                 uint32_t dshift, uint32_t dmask) {
     __shared__ uint2 buf[SORT_DBUF];
-    __shared__ uint32_t cur, base_s;
-    const uint32_t tid = threadIdx.x, lane = tid & 31;
+    __shared__ uint32_t wpre[SORT_DWARPS + 1];
+    __shared__ uint32_t base_s;
+    const uint32_t tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
     const uint32_t lt = (1u << lane) - 1u;
-    if (tid == 0) cur = 0;
-    __syncthreads();
+    const uint32_t lanes = scalars_per_block / SORT_DWARPS < 32 ? scalars_per_block / SORT_DWARPS : 32u;
+    uint2* slice = buf + wid * SORT_DSLICE;
+    uint32_t wc = 0;  // entries in the warp's slice (the same in every lane)
 #pragma unroll 1
-    for (uint32_t k = 0; k < scalars_per_block; k += SORT_DTHREADS) {
-        const uint64_t gi = (uint64_t)blockIdx.x * scalars_per_block + k + tid;
+    for (uint32_t k = 0; k < scalars_per_block; k += SORT_DWARPS * lanes) {
+        const uint32_t r = k + wid * lanes + lane;  // scalar of the block
+        const uint64_t gi = (uint64_t)blockIdx.x * scalars_per_block + r;
         uint32_t x[2][NL], neg[2] = {0, 0};
         int cnt = 0;
         MsmDesc d{};
         d.c = 2;
         uint32_t idx = 0;
-        if (k + tid < scalars_per_block && gi < total) {
+        if (lane < lanes && r < scalars_per_block && gi < total) {
             d = descs[find_msm(descs, nd, gi)];
             prep_scalar<C, NL>(x, neg, cnt, scalars + gi * 8, d.fmt, d.glv);
             idx = d.base_off + (uint32_t)(gi - d.scalar_off);
@@ -520,35 +529,41 @@ __global__ void __launch_bounds__(SORT_DTHREADS) k_radix_digits(const uint32_t* 
                 const uint32_t a = take_window<NL>(x[j], cw, carry, dn);
                 const bool ok = j < (uint32_t)cnt && w < d.nwin && a != 0;
                 const uint32_t m = __ballot_sync(0xffffffffu, ok);
-                if (m) {
-                    uint32_t base = 0;
-                    if (lane == __ffs(m) - 1) base = atomicAdd(&cur, (uint32_t)__popc(m));
-                    base = __shfl_sync(0xffffffffu, base, __ffs(m) - 1);
-                    if (ok) {
-                        uint2 e;
-                        if (d.wstep) {  // shift table: window w's base is 2^(c*w)*P, one bucket set
-                            e.x = d.bucket_off + (a - 1);
-                            e.y = (idx + w * d.wstep) | ((neg[j] ^ dn) << 31);
-                        } else {
-                            e.x = d.bucket_off + wb + (a - 1);
-                            e.y = idx | (j << 30) | ((neg[j] ^ dn) << 31);
-                        }
-                        buf[base + __popc(m & lt)] = e;
+                if (ok) {
+                    uint2 e;
+                    if (d.wstep) {  // shift table: window w's base is 2^(c*w)*P, one bucket set
+                        e.x = d.bucket_off + (a - 1);
+                        e.y = (idx + w * d.wstep) | ((neg[j] ^ dn) << 31);
+                    } else {
+                        e.x = d.bucket_off + wb + (a - 1);
+                        e.y = idx | (j << 30) | ((neg[j] ^ dn) << 31);
                     }
+                    slice[wc + __popc(m & lt)] = e;
                 }
+                wc += __popc(m);
                 wb += 1u << (cw - 1);
             }
         }
     }
+    // slices -> one dense run of A
+    if (lane == 0) wpre[wid] = wc;
     __syncthreads();
-    const uint32_t cnt = cur;
-    if (tid == 0) base_s = cnt ? atomicAdd(d_count, cnt) : 0;
+    if (tid == 0) {
+        uint32_t run = 0;
+        for (uint32_t w = 0; w < SORT_DWARPS; w++) {
+            const uint32_t c = wpre[w];
+            wpre[w] = run;
+            run += c;
+        }
+        wpre[SORT_DWARPS] = run;
+        base_s = run ? atomicAdd(d_count, run) : 0;
+    }
     __syncthreads();
-    const uint32_t base = base_s;
-    for (uint32_t i = tid; i < cnt; i += SORT_DTHREADS) {
-        const uint2 e = buf[i];
-        A[(size_t)base + i] = e;
-        if (D) D[(size_t)base + i] = (uint16_t)((e.x >> dshift) & dmask);
+    const uint32_t base = base_s, wbase = wpre[wid];
+    for (uint32_t i = lane; i < wc; i += 32) {
+        const uint2 e = slice[i];
+        A[(size_t)base + wbase + i] = e;
+        if (D) D[(size_t)base + wbase + i] = (uint16_t)((e.x >> dshift) & dmask);
     }
     if (hist0) {
         // counts of the range [base, base + cnt) per tile (the tile of base,
@@ -559,11 +574,11 @@ __global__ void __launch_bounds__(SORT_DTHREADS) k_radix_digits(const uint32_t* 
         __syncthreads();
         const uint32_t mask = (1u << h0bits) - 1;
         const uint32_t split = SORT_ETILE - base % SORT_ETILE;
-        for (uint32_t i0 = 0; i0 < cnt; i0 += SORT_DTHREADS) {
-            const uint32_t i = i0 + tid;
-            const bool v = i < cnt;
-            const uint32_t key = v ? (i < split ? 0u : SORT_MAX_BINS) + (buf[i].x & mask) : 0u;
-            warp_count(hc, v, key);
+        for (uint32_t i0 = 0; i0 < SORT_DSLICE; i0 += 32) {
+            const uint32_t i = i0 + lane;
+            const bool v = i < wc;
+            const uint32_t key = v ? (wbase + i < split ? 0u : SORT_MAX_BINS) + (slice[i].x & mask) : 0u;
+            if (__any_sync(0xffffffffu, v)) warp_count(hc, v, key);
         }
         __syncthreads();
         const uint32_t t0 = base / SORT_ETILE;
