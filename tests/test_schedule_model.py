@@ -366,3 +366,33 @@ def test_two_width_layout_covers_scalar(curve, n):
     widths = [win_width(c, nlo, w) for w in range(nwin)]
     assert max(widths) - min(widths) <= 1 and widths == sorted(widths)
     assert sum(widths) - widths[-1] < 128 <= sum(widths)
+
+
+def _types_const(name):
+    import os
+    import re
+    text = open(os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "zkmetal_b200", "csrc",
+                             "types.cuh")).read()
+    m = re.search(r"constexpr\s+\w+\s+%s\s*=\s*([^;]+);" % name, text)
+    return int(m.group(1))
+
+
+@pytest.mark.parametrize("curve,counts,window,glv", [
+    (0, [1 << 24], 0, -1), (0, [1 << 20], 0, -1), (0, [1 << 12], 0, -1), (0, [3000], 6, -1), (0, [5000], 2, 0),
+    (1, [1 << 22], 0, -1), (2, [1 << 16], 0, -1), (3, [1 << 14], 0, -1), (0, [4096, 1 << 20, 333, 1 << 18], 0, -1),
+    (0, [1 << 10] * 64, 0, 0), (0, [100], 3 | 1 << 16, -1)])
+def test_digit_block_slices_fit(curve, counts, window, glv):
+    """k_radix_digits gives each warp a slice of SORT_DBUF / 8 entries and runs
+    min(32, spb / 8) lanes per warp in rounds of 8 * lanes scalars: for the
+    plan's scalars per block (spb) and digits per scalar (maxd), a warp's
+    digits of all its rounds must fit its slice."""
+    dbuf, threads = _types_const("SORT_DBUF"), _types_const("SORT_DTHREADS")
+    warps = threads // 32
+    pl = plan(curve, counts, window=window, glv=glv)
+    maxd, spb = pl["sort"][0], pl["sort"][1]
+    assert maxd >= 1 and spb >= warps
+    lanes = min(32, spb // warps)
+    rounds = -(-spb // (warps * lanes))
+    assert lanes >= 1 and rounds * lanes * maxd <= dbuf // warps, (maxd, spb, lanes, rounds)
+    # the same number of scalars per block as the kernel's rounds cover
+    assert spb <= rounds * warps * lanes
