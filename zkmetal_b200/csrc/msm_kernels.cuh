@@ -1459,8 +1459,7 @@ static __global__ void __launch_bounds__(SCAN_THREADS) k_scan_add(uint32_t* __re
 //                   (pass 1 from the 2-byte digit array the digit kernel
 //                   writes beside the entries, pass 2 from the entries'
 //                   keys), and the group's digit totals straight into the
-//                   scan
-//                   layout S[seg][digit][group of seg], so that an exclusive
+//                   scan layout S[seg][digit][group of seg], so that an exclusive
 //                   scan of S gives each (seg, digit, group) the first output
 //                   slot of its run (pass 1 counts each group in `sub` parts,
 //                   S[digit][group][part], so that two count blocks share an
@@ -1473,8 +1472,8 @@ static __global__ void __launch_bounds__(SCAN_THREADS) k_scan_add(uint32_t* __re
 //  k_msd_scatter    one block per tile: reads its count row (local offsets)
 //                   and slot row, places the tile in digit order in shared
 //                   memory and writes it out as one run per digit.
-// The scan layout holds one word per group and digit (pass 1: 2.4 MB at any
-// size), not one per tile, so the tile rows never need transposing; the
+// The scan layout holds one word per group and digit (pass 1: at most 4.8 MB
+// at any size), not one per tile, so the tile rows never need transposing; the
 // scatter keeps one block per tile because blocks placing neighbouring
 // tiles at the same time write their runs of a digit side by side (one block
 // placing a whole group wrote 148 x 4096 separate fronts at 2^24 points and
@@ -1485,8 +1484,8 @@ static __global__ void __launch_bounds__(SCAN_THREADS) k_scan_add(uint32_t* __re
 // Pass 1 (seg_chunk == nullptr): the ceil(E / MSD_TILE) tiles of [0, E) are
 // split into `ng` groups of K = ceil(tiles / ng) tiles, each counted in
 // `sub` parts of ceil(K / sub) tiles; the count kernel runs ng*sub units
-// (u = group*sub + part), the scatter ng (u = group, whole groups, part 0's
-// scan slot).  Every unit exists (groups past the last tile are empty and
+// (u = group*sub + part), the slot-row kernel ng (u = group, whole groups,
+// part 0's scan slot).  Every unit exists (groups past the last tile are empty and
 // count zeros).  Pass 2: chunk u of the chunk table seg_chunk (exclusive
 // prefix of chunks per segment, nseg + 1 entries), with the tile table
 // seg_tile and segment starts seg_start (nseg + 1 entries each, the last
